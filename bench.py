@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""FP64 cell-updates/s of the GenASiS Fluid_P_I finite-volume step on B200.
+
+Workload (default): 3-D sine-wave advection on the 256^3 periodic unit cube,
+FP64, gamma = 1.4, rho = 1 + 0.5 sin(2 pi (x+y+z)), v = (1,1,1), p = 1,
+PLM (generalized minmod, theta 1.4) + HLLC, RK2, CFL 0.8.  One step = one
+integrator cycle: CFL time step + RK2 step (two fused stages, features,
+ghost refresh), device-resident, replayed from a CUDA graph.  Synthetic
+seeded inputs with the benchmark's shape; the 845 MB state exceeds L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the benchmark fixes one GPU per domain;
+the path has no data exchange between replicas), one rank per GPU.
+--impl reference times the reference's CPU step (the C restatement in
+oracle/, the reference itself being Fortran + MPI that cannot be compiled
+here) on the host cores, with all host threads.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 cell-updates/s"
+UNIT = "cell-updates/s"
+# Algorithmic bytes per cell of each fused stage (6 FP64 conserved fields):
+# stage 1 reads U^n and writes Y; stage 2 reads Y and U^n and writes U^n+1.
+STAGE_BYTES = {"stage1": 96.0, "stage2": 144.0}
+STEP_BYTES = 240.0
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="cells per axis of the sine wave")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:  # noqa: BLE001
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_init():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_step_rate(n, steps, warmup=1):
+    """The CPU oracle on an n^3 sine-wave brick: cell-updates/s over `steps`
+    RK2 steps (after `warmup` untimed ones), all host threads."""
+    from genasis_b200 import problems
+    from oracle.oracle import Oracle
+
+    cfg, prim = problems.sine_wave(n)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    i = 0
+    for _ in range(warmup):
+        o.step(o.timestep(i))
+        i += 1
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(o.timestep(i))
+        i += 1
+    el = time.perf_counter() - t0
+    return n ** 3 * steps / el, el, Oracle.n_threads()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # a bounded sample of the workload per step: the largest cube whose step
+    # keeps the whole run within a few minutes (calibrated on one step)
+    rate, _, cores = cpu_step_rate(64, 1, warmup=0)
+    budget_s = 150.0
+    n = args.n
+    while n > 32 and (n ** 3) * (args.steps + args.warmup) / rate > budget_s:
+        n //= 2
+    value, el, cores = cpu_step_rate(n, args.steps, warmup=args.warmup)
+    sample = ("%d RK2 steps (after %d warm-up) of a %d^3 brick of the sine-wave workload "
+              "(HLLC, periodic), per-cell cost independent of brick size" %
+              (args.steps, args.warmup, n))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "sine_wave_%d" % args.n, "sample_cells": n ** 3,
+                   "riemann": "HLLC", "boundary": "periodic", "cfl": 0.8},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def traffic_per_launch(kernel, cells):
+    """DRAM bytes per launch of the stage kernel from the committed ncu summary
+    (bytes per cell measured on a smaller case, scaled by the cells)."""
+    path = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    try:
+        with open(path) as f:
+            per_cell = json.load(f)[kernel]["dram_bytes_per_cell"]
+        return per_cell * cells
+    except Exception:  # noqa: BLE001
+        return None
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_init()
+    from genasis_b200 import problems
+    from genasis_b200.fluid import FluidBox
+
+    cfg, prim = problems.sine_wave(args.n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
+    cells = cfg.n_proper
+    box = FluidBox(cfg, device="cuda:%d" % local)
+    box.compute_from_primitive(prim)
+    del prim
+    stream = torch.cuda.current_stream()
+    # warm-up cycles (also captures the cycle graph)
+    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(args.warmup, 3))
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = box.kernel_launches()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    launches = box.kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    steps_done = cyc2 - cyc
+    value = world * cells * steps_done / (ms_max / 1000.0)
+
+    # per-kernel device times of the fused stages (CUDA events per launch)
+    dt = box.compute_time_step(cyc2)
+    per = {"features": [], "stage1": [], "stage2": [], "ghosts": []}
+    for _ in range(min(args.steps, 10)):
+        f, s1, s2, gh = box.step_timed(dt)
+        per["features"].append(f)
+        per["stage1"].append(s1)
+        per["stage2"].append(s2)
+        per["ghosts"].append(gh)
+    avg = {k: sum(v) / len(v) for k, v in per.items()}
+    dom = max(("stage1", "stage2"), key=lambda k: avg[k])
+    peak, peak_kind = peaks()
+    achieved = STAGE_BYTES[dom] * cells / (avg[dom] / 1000.0) / 1e9
+    traffic = traffic_per_launch(dom, cells)
+    roofline = {"bound": "hbm", "kernel": "stage_kernel (%s)" % dom, "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_kind,
+                "algorithmic_bytes_per_cell": STAGE_BYTES[dom],
+                "avg_launch_ms": avg[dom],
+                "kernel_ms": avg,
+                "step_hbm_frac": STEP_BYTES * value / world / 1e9 / peak}
+
+    # L1 density error against the exact translated profile at the final time
+    prim_t, _ = box.compute_from_conserved(primitive=True)
+    exact = problems.sine_density(cfg, t_sim)
+    l1 = problems.l1_error(prim_t[0].cpu().numpy(), exact, cfg)
+    del prim_t
+
+    # end to end: H2D of the state from pinned host memory, the step, D2H
+    e2e = None
+    if not args.no_e2e:
+        host = box.U.detach().cpu().pin_memory()
+        nbytes = host.numel() * host.element_size()
+        n_e = max(3, min(args.steps, 20))
+        box.step_host(host, dt)
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(n_e):
+            box.step_host(host, dt)
+        el = time.perf_counter() - t0
+        el = max_over_ranks(el, world)
+        e2e = {"value": world * cells * n_e / el, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": n_e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, el, cores = cpu_step_rate(args.n, 2, warmup=1)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "2 RK2 steps (after 1 warm-up) of the %d^3 sine-wave workload on the "
+                         "CPU oracle, %.1f s" % (args.n, el)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": steps_done, "warmup": args.warmup, "ms_per_step": ms_max / steps_done,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "sine_wave_%d" % args.n, "cells": cells, "riemann": "HLLC",
+                       "reconstruction": "PLM theta 1.4", "boundary": "periodic",
+                       "cfl": 0.8, "rk": 2, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state %.0f MB)" % (
+                           6 * box.n_values * 8 / 1e6),
+                       "l1_density_error": l1, "sim_time": t_sim},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    box.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,322 @@
+// aux_kernels.cuh -- the small kernels around the fused stages: state
+// conversion over every value, shock features, ghost refresh, CFL reduction
+// and the device-side time-step bookkeeping.
+#pragma once
+
+#include "stage_kernel.cuh"
+
+namespace gfx {
+
+struct Box {
+  int n[3], m[3], bc[3][2];
+  long long nV, nP;
+};
+
+__device__ __forceinline__ bool periodic_reachable(const Box& b, int i, int j, int k, int& si,
+                                                   int& sj, int& sk) {
+  // A ghost value is written by the single-brick exchange (faces and edges,
+  // Chart_SLD__Form.f90:131-201) when every axis on which it is a ghost is
+  // periodic and it is not a corner.
+  const int t[3] = {i, j, k};
+  int s[3], nghost = 0;
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int p = t[d] - 2;
+    const bool ghost = (p < 0 || p >= b.n[d]);
+    nghost += ghost;
+    if (ghost && b.bc[d][0] != BC_PERIODIC) ok = false;
+    s[d] = ghost ? ((p % b.n[d] + b.n[d]) % b.n[d]) + 2 : t[d];
+  }
+  si = s[0];
+  sj = s[1];
+  sk = s[2];
+  return ok && nghost > 0 && nghost < 3;
+}
+
+// Fluid_P_I % ComputeFromPrimitive on every value after the periodic
+// exchange of the primitives (Integrator_C_PS__Form.f90:194-203); keeps the
+// primitives of the proper cells (with N clipped at 0 as Compute_D_S_G does)
+// as the next step's state.
+__global__ void from_primitive_kernel(Box b, Phys ph, const double* __restrict__ prim,
+                                      double* __restrict__ U, double* __restrict__ Pst) {
+  const long long nV = b.nV;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(v % b.m[0]);
+    const int j = (int)((v / b.m[0]) % b.m[1]);
+    const int k = (int)(v / ((long long)b.m[0] * b.m[1]));
+    int si, sj, sk;
+    long long src = v;
+    if (periodic_reachable(b, i, j, k, si, sj, sk))
+      src = si + (long long)b.m[0] * (sj + (long long)b.m[1] * sk);
+    FaceState s;
+    face_state<6>(prim[src], prim[nV + src], prim[2 * nV + src], prim[3 * nV + src],
+                  prim[4 * nV + src], ph, s);
+    U[v] = s.D;
+    U[nV + v] = s.S1;
+    U[2 * nV + v] = s.S2;
+    U[3 * nV + v] = s.S3;
+    U[4 * nV + v] = s.G;
+    U[5 * nV + v] = s.DS;
+    const int pi = i - 2, pj = j - 2, pk = k - 2;
+    if (pi >= 0 && pj >= 0 && pk >= 0 && pi < b.n[0] && pj < b.n[1] && pk < b.n[2]) {
+      const long long c = pi + (long long)b.n[0] * (pj + (long long)b.n[1] * pk);
+      Pst[c] = s.N;
+      Pst[b.nP + c] = s.V1;
+      Pst[2 * b.nP + c] = s.V2;
+      Pst[3 * b.nP + c] = s.V3;
+      Pst[4 * b.nP + c] = s.E;
+    }
+  }
+}
+
+// Fluid_P_I % ComputeFromConserved on every value: floors written back to U,
+// DS recomputed, optional primitives and (P, CS, SB).
+__global__ void to_primitive_kernel(Box b, Phys ph, double* __restrict__ U,
+                                    double* __restrict__ prim, double* __restrict__ aux) {
+  const long long nV = b.nV;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
+       v += (long long)gridDim.x * blockDim.x) {
+    Cons u{U[v], U[nV + v], U[2 * nV + v], U[3 * nV + v], U[4 * nV + v]};
+    Prim w;
+    cons_to_prim(u, w, ph.nmin);
+    double P, CS, SB;
+    eos_cell(w.N, w.E, ph, P, CS, &SB);
+    U[v] = u.D;
+    U[nV + v] = u.S1;
+    U[2 * nV + v] = u.S2;
+    U[3 * nV + v] = u.S3;
+    U[4 * nV + v] = u.G;
+    U[5 * nV + v] = SB * w.N;
+    if (prim) {
+      prim[v] = w.N;
+      prim[nV + v] = w.V1;
+      prim[2 * nV + v] = w.V2;
+      prim[3 * nV + v] = w.V3;
+      prim[4 * nV + v] = w.E;
+    }
+    if (aux) {
+      aux[v] = P;
+      aux[nV + v] = CS;
+      aux[2 * nV + v] = SB;
+    }
+  }
+}
+
+// Ghost values at the end of a step: exchange-reachable periodic ghosts take
+// their image (the reference adds the image's exchanged increments to an
+// image copy); every other ghost keeps its conserved values through the
+// floors of ComputeFromConserved, which also recompute its DS.
+__global__ void ghost_refresh_kernel(Box b, Phys ph, double* __restrict__ U) {
+  const long long nV = b.nV;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(v % b.m[0]);
+    const int j = (int)((v / b.m[0]) % b.m[1]);
+    const int k = (int)(v / ((long long)b.m[0] * b.m[1]));
+    const bool ghost = i < 2 || j < 2 || k < 2 || i >= b.n[0] + 2 || j >= b.n[1] + 2 ||
+                       k >= b.n[2] + 2;
+    if (!ghost) continue;
+    int si, sj, sk;
+    if (periodic_reachable(b, i, j, k, si, sj, sk)) {
+      const long long s = si + (long long)b.m[0] * (sj + (long long)b.m[1] * sk);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) U[f * nV + v] = U[f * nV + s];
+    } else {
+      Cons u{U[v], U[nV + v], U[2 * nV + v], U[3 * nV + v], U[4 * nV + v]};
+      Prim w;
+      cons_to_prim(u, w, ph.nmin);
+      double P, CS, SB;
+      eos_cell(w.N, w.E, ph, P, CS, &SB);
+      U[v] = u.D;
+      U[nV + v] = u.S1;
+      U[2 * nV + v] = u.S2;
+      U[3 * nV + v] = u.S3;
+      U[4 * nV + v] = u.G;
+      U[5 * nV + v] = SB * w.N;
+    }
+  }
+}
+
+// Pressure and normal velocity of proper cell (i, j, k) of the state.
+__device__ __forceinline__ void cell_p_v(const Box& b, const Phys& ph, const double* U,
+                                         const double* Pst, int i, int j, int k, double& P,
+                                         double v[3]) {
+  Prim w;
+  if (Pst) {
+    const long long c = i + (long long)b.n[0] * (j + (long long)b.n[1] * k);
+    w.N = Pst[c];
+    w.V1 = Pst[b.nP + c];
+    w.V2 = Pst[2 * b.nP + c];
+    w.V3 = Pst[3 * b.nP + c];
+    w.E = Pst[4 * b.nP + c];
+  } else {
+    const long long o = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
+    Cons u{U[o], U[b.nV + o], U[2 * b.nV + o], U[3 * b.nV + o], U[4 * b.nV + o]};
+    cons_to_prim(u, w, ph.nmin);
+  }
+  P = ph.gm1 * w.E;
+  v[0] = w.V1;
+  v[1] = w.V2;
+  v[2] = w.V3;
+}
+
+// DetectShocks_CSL_Kernel (FluidFeatures_P__Kernel.f90:12-186) for the proper
+// cells: bit e of sb[c] = shock along e at c (compared with c - e_e).
+__global__ void detect_shock_kernel(Box b, Phys ph, const double* __restrict__ U,
+                                    const double* __restrict__ Pst, uint8_t* __restrict__ sb) {
+  const long long nP = b.nP;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % b.n[0]);
+    const int j = (int)((c / b.n[0]) % b.n[1]);
+    const int k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    double P0, v0[3];
+    cell_p_v(b, ph, U, Pst, i, j, k, P0, v0);
+    uint8_t bits = 0;
+    const int t[3] = {i, j, k};
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      if (t[e] < 1) continue;
+      double P1, v1[3];
+      cell_p_v(b, ph, U, Pst, i - (e == 0), j - (e == 1), k - (e == 2), P1, v1);
+      const double dP = fabs(P0 - P1);
+      const double pmin = (P0 < P1) ? P0 : P1;  // Fortran MIN: ties give either
+      const double dLnP = dP / fmax2(pmin, kSqrtTiny);
+      const double dV = v0[e] - v1[e];
+      if (dLnP > ph.shock_threshold && dV <= 0.0) bits |= (uint8_t)(1u << e);
+    }
+    sb[c] = bits;
+  }
+}
+
+// DIFFUSIVE_FLUX_I flags after ClearBoundary_CSL_Kernel (FluidFeatures_P__Kernel.f90:
+// 189-313) on a single brick: only cells at least two cells inside every face
+// keep flags, and DF_d(x) is set by a shock along e != d at x, x + e_e, x - e_d
+// or x + e_e - e_d (the positions DetectShocks_CSL_Kernel writes).
+__global__ void detect_flags_kernel(Box b, const uint8_t* __restrict__ sb,
+                                    uint8_t* __restrict__ df) {
+  const long long nP = b.nP;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int t[3] = {(int)(c % b.n[0]), (int)((c / b.n[0]) % b.n[1]),
+                      (int)(c / ((long long)b.n[0] * b.n[1]))};
+    uint8_t bits = 0;
+    bool interior = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (t[d] < 1 || t[d] > b.n[d] - 2) interior = false;
+    if (interior) {
+      const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          if (e == d) continue;
+          const uint8_t m = (uint8_t)(1u << e);
+          if ((sb[c] & m) || (sb[c + st[e]] & m) || (sb[c - st[d]] & m) ||
+              (sb[c + st[e] - st[d]] & m))
+            bits |= (uint8_t)(1u << d);
+        }
+      }
+    }
+    df[c] = bits;
+  }
+}
+
+// Per-cell inverse CFL time of the state, reduced to one maximum
+// (ComputeTimeStepKernel_CSL, Integrator_C_PS__Kernel.f90:97-142).
+__global__ void inverse_timestep_kernel(Box b, Phys ph, const double* __restrict__ U,
+                                        const double* __restrict__ Pst,
+                                        const double* __restrict__ W0,
+                                        const double* __restrict__ W1,
+                                        const double* __restrict__ W2,
+                                        unsigned long long* __restrict__ tsi_bits) {
+  __shared__ double s_red[32];
+  const long long nP = b.nP;
+  double m = -DBL_MAX;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % b.n[0]);
+    const int j = (int)((c / b.n[0]) % b.n[1]);
+    const int k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    Prim w;
+    if (Pst) {
+      w.N = Pst[c];
+      w.V1 = Pst[nP + c];
+      w.V2 = Pst[2 * nP + c];
+      w.V3 = Pst[3 * nP + c];
+      w.E = Pst[4 * nP + c];
+    } else {
+      const long long o = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
+      Cons u{U[o], U[b.nV + o], U[2 * b.nV + o], U[3 * b.nV + o], U[4 * b.nV + o]};
+      cons_to_prim(u, w, ph.nmin);
+    }
+    double P, CS;
+    eos_cell(w.N, w.E, ph, P, CS, nullptr);
+    m = fmax2(m, inverse_cfl_time(w, CS, W0[i + 2], W1[j + 2], W2[k + 2]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax2(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = s_red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = fmax2(r, s_red[w]);
+    atomicMax(tsi_bits, ordered_bits(r));
+  }
+}
+
+// Device-side integrator state of one brick (evolve loop).
+struct Clock {
+  double dt;       // step to take
+  double time;     // current time
+  double finish;   // FinishTime
+  int cycle;       // iCycle
+  int max_cycle;   // FinishCycle
+  int done;        // nonzero: the loop has ended, kernels skip
+  int pad;
+};
+
+// Integrator ComputeTimeStep (Integrator_Template.f90:896-939 and
+// Integrator_C_PS__Form.f90:419) from the reduced inverse CFL time, plus the
+// CheckpointTimeExact cut of ComputeNewTime (:842-893) at the finish time.
+__global__ void finalize_dt_kernel(Phys ph, const unsigned long long* __restrict__ tsi_bits,
+                                   Clock* __restrict__ clk, int n, int clip_to_finish) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Clock& c = clk[b];
+  if (c.done) return;
+  double tsi = from_ordered_bits_dev(tsi_bits[b]);
+  tsi = fmax2(kTiny, tsi);
+  double dt = DBL_MAX;
+  const double cand = 1.0 / tsi;
+  if (cand < dt) dt = cand;
+  dt = ph.courant * dt;
+  double ramp = (double)(c.cycle + 1) / (double)ph.n_ramp;
+  if (ramp > 1.0) ramp = 1.0;
+  if (ramp < 1.0) dt = ramp * dt;
+  if (clip_to_finish && c.time + dt > c.finish) dt = c.finish - c.time;
+  c.dt = dt;
+}
+
+// Time += dt, iCycle += 1, loop condition of Integrator % Evolve (:311).
+__global__ void advance_clock_kernel(Clock* __restrict__ clk, int n) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Clock& c = clk[b];
+  if (c.done) return;
+  c.time = c.time + c.dt;
+  c.cycle = c.cycle + 1;
+  if (!(c.time < c.finish && c.cycle < c.max_cycle)) c.done = 1;
+}
+
+__global__ void reset_bits_kernel(unsigned long long* __restrict__ bits, int n, int* counter,
+                                  int n_counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bits[i] = 0x0010000000000000ull;  // ordered_bits(-DBL_MAX)
+  if (i < n_counters) counter[i] = 0;
+}
+
+}  // namespace gfx

@@ -1,0 +1,277 @@
+// fluid_physics.cuh -- pointwise FP64 arithmetic of the Fluid_P_I step.
+//
+// Every expression keeps the operand order of the reference's Fortran so that
+// each rounding matches (the library is compiled with --fmad=false).  The
+// baryon mass M and every metric entry are exactly 1 on the rectangular chart,
+// so the products with them that the reference performs are exact and are
+// left out here.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+
+namespace gfx {
+
+constexpr double kTiny = DBL_MIN;                      // tiny(0._KDR)
+constexpr double kSqrtTiny = 1.4916681462400413e-154;  // sqrt(tiny(0._KDR))
+constexpr double kSqrtHuge = 1.3407807929942596e+154;  // sqrt(huge(1._KDR))
+
+struct Phys {
+  double gamma;  // AdiabaticIndex
+  double gm1;    // AdiabaticIndex - 1
+  double c_v;    // SpecificHeatVolume = 1 / (1 * (gamma - 1))
+  double theta;  // LimiterParameter
+  double nmin;   // BaryonDensityMin
+  double accel;  // UniformAcceleration (z)
+  double shock_threshold;
+  double courant;
+  int use_limiter;
+  int n_ramp;
+};
+
+// Fortran MAX / MIN with gfortran's argument order: the first argument wins ties.
+__device__ __forceinline__ double fmax2(double a, double b) { return (b > a) ? b : a; }
+__device__ __forceinline__ double fmax3(double a, double b, double c) {
+  double r = a;
+  if (b > r) r = b;
+  if (c > r) r = c;
+  return r;
+}
+__device__ __forceinline__ double fmin3(double a, double b, double c) {
+  double r = a;
+  if (b < r) r = b;
+  if (c < r) r = c;
+  return r;
+}
+
+// Generalized-minmod limited slope of one cell, Gradient_Kernel.f90:166-190.
+// vm, v0, vp: values at i-1, i, i+1; dxl = X(i) - X(i-1), dxr = X(i+1) - X(i);
+// sql = dxl*dxl, sqr = dxr*dxr, cden = (dxl*dxr)*(dxl+dxr) come from the
+// per-axis geometry tables (same operations, evaluated once on the host).
+// When the two one-sided differences have opposite signs the reference's
+// factor (sign(1/2,dV_L) + sign(1/2,dV_R)) is exactly +0, and so is the slope:
+// the three quotients are then skipped.
+__device__ __forceinline__ double limited_slope(double vm, double v0, double vp, double dxl,
+                                                double dxr, double sql, double sqr,
+                                                double cden, double theta, int use_limiter) {
+  const double dvl = v0 - vm;
+  const double dvr = vp - v0;
+  if (!use_limiter) return (sqr * dvl + sql * dvr) / cden;
+  const double s = copysign(0.5, dvl) + copysign(0.5, dvr);
+  if (s == 0.0) return 0.0;
+  const double central = (sqr * dvl + sql * dvr) / cden;
+  const double m = fmin3(fabs(theta * dvl / dxl), fabs(theta * dvr / dxr), fabs(central));
+  return s * m;
+}
+
+// State at one face after ComputeFromPrimitiveCommon (Fluid_P_I__Form.f90:509-601):
+// Apply_EOS_I_E (Fluid_P_I__Kernel.f90:244-267), Compute_D_S_G
+// (Fluid_D__Kernel.f90:47-101), Compute_G_G (Fluid_P__Kernel.f90:12-52),
+// Compute_DS_G (:55-91), Compute_FE_P_G (:242-316).
+struct FaceState {
+  double N, V1, V2, V3, E;
+  double D, S1, S2, S3, G;
+  double P, CS, DS;
+};
+
+template <int NF>
+__device__ __forceinline__ void face_state(double N, double V1, double V2, double V3, double E,
+                                           const Phys& ph, FaceState& s) {
+  const double P = ph.gm1 * E;
+  double CS = 0.0, SB = -kSqrtHuge;
+  if (N > 0.0 && P > 0.0) {
+    CS = sqrt(ph.gamma * P / N);
+    if (NF == 6) SB = ph.c_v * log(P * pow(1.0 / N, ph.gamma));
+  }
+  if (N < 0.0) N = 0.0;
+  s.N = N;
+  s.V1 = V1;
+  s.V2 = V2;
+  s.V3 = V3;
+  s.E = E;
+  s.D = N;
+  s.S1 = N * V1;
+  s.S2 = N * V2;
+  s.S3 = N * V3;
+  s.G = E + 0.5 * (s.S1 * V1 + s.S2 * V2 + s.S3 * V3);
+  s.P = P;
+  s.CS = CS;
+  s.DS = (NF == 6) ? SB * N : 0.0;
+}
+
+template <int D>
+__device__ __forceinline__ double vel(const FaceState& s) {
+  return D == 0 ? s.V1 : (D == 1 ? s.V2 : s.V3);
+}
+template <int D>
+__device__ __forceinline__ double mom(const FaceState& s) {
+  return D == 0 ? s.S1 : (D == 1 ? s.S2 : s.S3);
+}
+
+// Riemann flux through one face along direction D: HLL (Current_Kernel.f90:
+// 50-137 with the unit diffusion factor) and, for HLLC, the centre states of
+// Fluid_P__Kernel.f90:319-668.  The HLLC selection is evaluated first; the HLL
+// flux is only formed when the reference would keep it (diffusive-flux flag
+// set, or a vanishing outer wave speed), which leaves every value unchanged.
+// F holds D, S1, S2, S3, G and, for NF == 6, DS.
+template <int D, bool HLLC, int NF>
+__device__ __forceinline__ void riemann_flux(const FaceState& L, const FaceState& R,
+                                             bool diffusive, double* F) {
+  const double vl = vel<D>(L), vr = vel<D>(R);
+  const double AP = fmax3(0.0, vl + L.CS, vr + R.CS);
+  const double AM = fmax3(0.0, -(vl - L.CS), -(vr - R.CS));
+  if (HLLC) {
+    const double fdl = L.D * vl, fdr = R.D * vr;
+    const double fsl = mom<D>(L) * vl + L.P, fsr = mom<D>(R) * vr + R.P;
+    const double MD = AP * R.D + AM * L.D - fdr + fdl;
+    const double SN = AP * mom<D>(R) + AM * mom<D>(L) - fsr + fsl;
+    const double MDinv = fmax2(MD, 0.0) / fmax2(MD * MD, kTiny);
+    const double AC = SN * MDinv;
+    if (!diffusive && AP != 0.0 && AM != 0.0) {
+      const FaceState& S = (AC >= 0.0) ? L : R;
+      const double vs = vel<D>(S);
+      double A_V, A_AC;
+      if (AC >= 0.0) {
+        A_V = AM + vs;
+        A_AC = AM + AC;
+      } else {
+        A_V = AP - vs;
+        A_AC = AP - AC;
+      }
+      const double inv = 1.0 / fmax2(fabs(A_AC), kSqrtTiny);
+      const double Dc = S.D * A_V * inv;
+      const double v1 = (D == 0) ? AC : S.V1;
+      const double v2 = (D == 1) ? AC : S.V2;
+      const double v3 = (D == 2) ? AC : S.V3;
+      const double s1 = Dc * v1, s2 = Dc * v2, s3 = Dc * v3;
+      const double sd = (D == 0) ? s1 : (D == 1 ? s2 : s3);
+      double Pc, Gc;
+      if (AC >= 0.0) {
+        Pc = S.P + mom<D>(S) * A_V - sd * A_AC;
+        Gc = (S.G * A_V + vs * S.P - AC * Pc) * inv;
+      } else {
+        Pc = S.P - mom<D>(S) * A_V + sd * A_AC;
+        Gc = (S.G * A_V - vs * S.P + AC * Pc) * inv;
+      }
+      F[0] = Dc * AC;
+      F[1] = s1 * AC;
+      F[2] = s2 * AC;
+      F[3] = s3 * AC;
+      F[1 + D] = F[1 + D] + Pc;
+      F[4] = (Gc + Pc) * AC;
+      if (NF == 6) F[5] = S.DS * A_V * inv * AC;
+      return;
+    }
+  }
+  // HLL
+  double FL[NF], FR[NF];
+  FL[0] = L.D * vl;  FR[0] = R.D * vr;
+  FL[1] = L.S1 * vl; FR[1] = R.S1 * vr;
+  FL[2] = L.S2 * vl; FR[2] = R.S2 * vr;
+  FL[3] = L.S3 * vl; FR[3] = R.S3 * vr;
+  FL[1 + D] = FL[1 + D] + L.P;
+  FR[1 + D] = FR[1 + D] + R.P;
+  FL[4] = (L.G + L.P) * vl;
+  FR[4] = (R.G + R.P) * vr;
+  if (NF == 6) {
+    FL[5] = L.DS * vl;
+    FR[5] = R.DS * vr;
+  }
+  const double UL[6] = {L.D, L.S1, L.S2, L.S3, L.G, L.DS};
+  const double UR[6] = {R.D, R.S1, R.S2, R.S3, R.G, R.DS};
+  const double den = fmax2(AP + AM, kTiny);
+  const double apam = AP * AM;
+#pragma unroll
+  for (int u = 0; u < NF; ++u) F[u] = (AP * FL[u] + AM * FR[u] - apam * (UR[u] - UL[u])) / den;
+}
+
+// Compute_N_V_E_G_Kernel (Fluid_P__Kernel.f90:94-192, both loops): the floored
+// conserved values and the primitives of one value.
+struct Prim {
+  double N, V1, V2, V3, E;
+};
+struct Cons {
+  double D, S1, S2, S3, G;
+};
+
+__device__ __forceinline__ void cons_to_prim(Cons& u, Prim& w, double nmin) {
+  if (u.D > nmin) {
+    w.N = u.D;
+    w.V1 = u.S1 / u.D;
+    w.V2 = u.S2 / u.D;
+    w.V3 = u.S3 / u.D;
+    w.E = u.G - 0.5 * (u.S1 * w.V1 + u.S2 * w.V2 + u.S3 * w.V3);
+  } else {
+    w.N = nmin;
+    w.V1 = 0.0;
+    w.V2 = 0.0;
+    w.V3 = 0.0;
+    w.E = 0.0;
+    u.D = nmin;
+    u.S1 = 0.0;
+    u.S2 = 0.0;
+    u.S3 = 0.0;
+    u.G = 0.0;
+  }
+  if (w.E < 0.0) {
+    w.E = 0.0;
+    u.G = w.E + 0.5 * (u.S1 * w.V1 + u.S2 * w.V2 + u.S3 * w.V3);
+  }
+}
+
+// The floored conserved values that cons_to_prim would have produced, rebuilt
+// from the original conserved values and the primitives without divisions:
+// D' = N; S' = S unless D <= nmin; G' = 0.5 (S'.V) exactly when the recovered
+// E is zero (E < 0 floored, or G - 0.5 (S.V) == 0, where G already equals it).
+__device__ __forceinline__ Cons floored_cons(const Cons& u, const Prim& w, double nmin) {
+  Cons f;
+  const bool live = u.D > nmin;
+  f.D = w.N;
+  f.S1 = live ? u.S1 : 0.0;
+  f.S2 = live ? u.S2 : 0.0;
+  f.S3 = live ? u.S3 : 0.0;
+  f.G = live ? u.G : 0.0;
+  if (w.E == 0.0) f.G = w.E + 0.5 * (f.S1 * w.V1 + f.S2 * w.V2 + f.S3 * w.V3);
+  return f;
+}
+
+// Apply_EOS_I_E_Kernel for a cell value: pressure, sound speed and (when
+// asked) the entropy per baryon.
+__device__ __forceinline__ void eos_cell(double N, double E, const Phys& ph, double& P,
+                                         double& CS, double* SB) {
+  P = ph.gm1 * E;
+  if (N > 0.0 && P > 0.0) {
+    CS = sqrt(ph.gamma * P / N);
+    if (SB) *SB = ph.c_v * log(P * pow(1.0 / N, ph.gamma));
+  } else {
+    CS = 0.0;
+    if (SB) *SB = -kSqrtHuge;
+  }
+}
+
+// Inverse CFL time of one cell, Integrator_C_PS__Kernel.f90:122-137
+// (coarsening factors are 1 on this chart).
+__device__ __forceinline__ double inverse_cfl_time(const Prim& w, double CS, double w0,
+                                                   double w1, double w2) {
+  return fmax2(w.V1 + CS, -(w.V1 - CS)) / w0 + fmax2(w.V2 + CS, -(w.V2 - CS)) / w1 +
+         fmax2(w.V3 + CS, -(w.V3 - CS)) / w2;
+}
+
+// Total order of doubles as unsigned integers, for atomicMax reductions.
+__device__ __forceinline__ unsigned long long ordered_bits(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_bits_dev(unsigned long long u) {
+  const unsigned long long b = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+  return __longlong_as_double((long long)b);
+}
+inline double from_ordered_bits(unsigned long long u) {
+  const unsigned long long b = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+  double x;
+  memcpy(&x, &b, sizeof(x));
+  return x;
+}
+
+}  // namespace gfx

@@ -1,0 +1,738 @@
+// gfx_fluid.cu -- host side of the C ABI in include/gfx_fluid.h.
+//
+// One gfx_fluid handle = one single-brick chart with its Fluid_P_I current,
+// the RK2 step and the integrator's time-step logic.  The handle owns the
+// per-axis geometry tables, the stage scratch (primitives of the intermediate
+// state Y and the partial solution U + K1/2, both without ghosts), the shock
+// feature bits and a device-side clock for the evolve loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "aux_kernels.cuh"
+#include "gfx_fluid.h"
+
+using namespace gfx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (expr);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(GFX_ERR_CUDA, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                  \
+  } while (0)
+
+// Per-axis geometry of the reference chart, Chart_Template.f90:478-560 (edges
+// by repeated addition; the ghost widths pass through real(KDL), i.e. default
+// single precision, as declared at :476-478), :827-841 (centres), :973-990
+// (half widths); GeometryFlat_Kernel.f90:22-24 (widths); Difference_Kernel on
+// the centres; the limiter's denominators of Gradient_Kernel.f90:176-180.
+struct HostAxis {
+  std::vector<double> X, WL, WR, W, dXI, SQ, CDEN;
+};
+
+HostAxis build_axis(int n, double mn, double mx, int g) {
+  const int m = n + 2 * g;
+  std::vector<double> edge(m + 1);
+  double* E1 = edge.data() + g - 1;  // E1[i] = Edge(i), i in [1-g, n+g+1]
+  const double width = (mx - mn) / (double)n;
+  E1[1] = mn;
+  for (int i = 2; i <= n + 1; ++i) E1[i] = E1[i - 1] + width;
+  for (int iC = 1; iC <= g; ++iC) {
+    const float w_ig = (float)(E1[iC + 1] - E1[iC]);
+    const float w_og = (float)(E1[n - iC + 2] - E1[n - iC + 1]);
+    E1[1 - iC] = E1[2 - iC] - (double)w_ig;
+    E1[n + 1 + iC] = E1[n + iC] + (double)w_og;
+  }
+  HostAxis a;
+  a.X.resize(m);
+  a.WL.resize(m);
+  a.WR.resize(m);
+  a.W.resize(m);
+  a.dXI.assign(m + 1, 0.0);
+  a.SQ.assign(m + 1, 0.0);
+  a.CDEN.assign(m + 1, 0.0);
+  for (int t = 0; t < m; ++t) {
+    const double c = 0.5 * (edge[t] + edge[t + 1]);
+    a.X[t] = c;
+    a.WL[t] = c - edge[t];
+    a.WR[t] = edge[t + 1] - c;
+    a.W[t] = a.WL[t] + a.WR[t];
+  }
+  for (int t = 1; t < m; ++t) {
+    a.dXI[t] = a.X[t] - a.X[t - 1];
+    a.SQ[t] = a.dXI[t] * a.dXI[t];
+  }
+  for (int t = 1; t + 1 < m; ++t)
+    a.CDEN[t] = a.dXI[t] * a.dXI[t + 1] * (a.dXI[t] + a.dXI[t + 1]);
+  return a;
+}
+
+enum FeatureState { FEAT_ZERO = 0, FEAT_VALID = 1, FEAT_PENDING = 2 };
+
+int g_num_sms = 0;
+std::once_flag g_sm_once;
+
+int num_sms() {
+  std::call_once(g_sm_once, [] {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  });
+  return g_num_sms;
+}
+
+}  // namespace
+
+struct gfx_fluid {
+  gfx_fluid_config cfg;
+  Phys ph;
+  Box box;
+  HostAxis axis[3];
+  double* geo = nullptr;  // device tables
+  AxisGeo dgeo[3];
+  double* Yp = nullptr;
+  double* H = nullptr;
+  double* Pst = nullptr;
+  uint8_t* df = nullptr;
+  uint8_t* sb = nullptr;
+  unsigned long long* tsi_bits = nullptr;  // [1]
+  int* counters = nullptr;                 // [4]
+  Clock* clock = nullptr;                  // evolve clock
+  double* dt_slot = nullptr;               // dt of gfx_fluid_step
+  WorkItem* items = nullptr;
+  int n_items = 0;
+  double* U_stage = nullptr;  // device copy for gfx_fluid_step_host
+  cudaStream_t host_stream = nullptr;
+  int features = FEAT_ZERO;
+  const double* features_src = nullptr;
+  bool prims_pending = false;
+  size_t face_size = 0;
+  // evolve graph cache
+  cudaGraphExec_t graph = nullptr;
+  double* graph_U = nullptr;
+  long long graph_kernels = 0;  // kernel nodes per replay
+  long long launches = 0;       // kernels launched so far
+};
+
+namespace {
+
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF>
+cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
+                           int n_items, int* counter, const Phys& ph, cudaStream_t s) {
+  using SM = StageSmem<MODE, IN_PRIM, HLLC, GRAV, NF>;
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF>;
+  std::call_once(once, [&] {
+    attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)SM::kBytes);
+  });
+  if (attr_err != cudaSuccess) return attr_err;
+  const int grid = std::max(1, std::min(n_items, num_sms()));
+  kern<<<grid, NT, SM::kBytes, s>>>(d, many, items, n_items, counter, ph);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const BrickDesc& d,
+                         const BrickDesc* many, const WorkItem* items, int n_items,
+                         int* counter, const Phys& ph, cudaStream_t s) {
+#define GFX_STAGE(M, IP, HC, GR, NF)                                                     \
+  if (mode == M && in_prim == IP && hllc == HC && grav == GR)                           \
+    return launch_stage_t<M, IP, HC, GR, NF>(d, many, items, n_items, counter, ph, s);
+  GFX_STAGE(MODE_INCREMENT, false, false, false, 6)
+  GFX_STAGE(MODE_INCREMENT, false, true, false, 6)
+  GFX_STAGE(MODE_INCREMENT, true, false, false, 6)
+  GFX_STAGE(MODE_INCREMENT, true, true, false, 6)
+  GFX_STAGE(MODE_STAGE1, false, false, false, 5)
+  GFX_STAGE(MODE_STAGE1, false, true, false, 5)
+  GFX_STAGE(MODE_STAGE1, false, false, true, 5)
+  GFX_STAGE(MODE_STAGE1, false, true, true, 5)
+  GFX_STAGE(MODE_STAGE1, true, false, false, 5)
+  GFX_STAGE(MODE_STAGE1, true, true, false, 5)
+  GFX_STAGE(MODE_STAGE1, true, false, true, 5)
+  GFX_STAGE(MODE_STAGE1, true, true, true, 5)
+  GFX_STAGE(MODE_STAGE2, true, false, false, 5)
+  GFX_STAGE(MODE_STAGE2, true, true, false, 5)
+  GFX_STAGE(MODE_STAGE2, true, false, true, 5)
+  GFX_STAGE(MODE_STAGE2, true, true, true, 5)
+#undef GFX_STAGE
+  return cudaErrorInvalidValue;
+}
+
+int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  const long long cap = (long long)num_sms() * 16;
+  return (int)std::max(1LL, std::min(g, cap));
+}
+
+int validate(const gfx_fluid_config* c) {
+  if (!c) return fail(GFX_ERR_ARGUMENT, "config is NULL");
+  for (int d = 0; d < 3; ++d) {
+    if (c->n_cells[d] < 4)
+      return fail(GFX_ERR_ARGUMENT, "n_cells[%d] = %d: need at least 4 proper cells", d,
+                  c->n_cells[d]);
+    if (!(c->max_coordinate[d] > c->min_coordinate[d]))
+      return fail(GFX_ERR_ARGUMENT, "max_coordinate[%d] must exceed min_coordinate[%d]", d, d);
+    for (int s = 0; s < 2; ++s)
+      if (c->boundary[d][s] < GFX_BC_OUTFLOW || c->boundary[d][s] > GFX_BC_PERIODIC)
+        return fail(GFX_ERR_ARGUMENT, "boundary[%d][%d] = %d is not a boundary condition", d,
+                    s, c->boundary[d][s]);
+    if ((c->boundary[d][0] == GFX_BC_PERIODIC) != (c->boundary[d][1] == GFX_BC_PERIODIC))
+      return fail(GFX_ERR_ARGUMENT, "axis %d: PERIODIC must be set on both faces", d);
+  }
+  if (c->n_ghost_layers != 2)
+    return fail(GFX_ERR_UNSUPPORTED, "n_ghost_layers = %d: only 2 (the reference default)",
+                c->n_ghost_layers);
+  if (c->riemann_solver != GFX_RIEMANN_HLL && c->riemann_solver != GFX_RIEMANN_HLLC)
+    return fail(GFX_ERR_ARGUMENT, "riemann_solver = %d", c->riemann_solver);
+  if (!(c->adiabatic_index > 1.0)) return fail(GFX_ERR_ARGUMENT, "adiabatic_index must be > 1");
+  if (c->n_ramp_cycles < 1) return fail(GFX_ERR_ARGUMENT, "n_ramp_cycles must be >= 1");
+  if (!(c->courant_factor > 0.0)) return fail(GFX_ERR_ARGUMENT, "courant_factor must be > 0");
+  return GFX_OK;
+}
+
+// Work list of one brick: TX x TY columns, cut along z into chunks so that the
+// persistent grid has several items per SM.
+std::vector<WorkItem> make_items(const int n[3], int brick) {
+  const int cx = (n[0] + TX - 1) / TX, cy = (n[1] + TY - 1) / TY;
+  const long long cols = (long long)cx * cy;
+  const long long want = 8LL * num_sms();
+  int chunks = (int)std::max(1LL, std::min<long long>(n[2] / 16, (want + cols - 1) / cols));
+  if (chunks < 1) chunks = 1;
+  const int len = (n[2] + chunks - 1) / chunks;
+  std::vector<WorkItem> v;
+  for (int z = 0; z < n[2]; z += len)
+    for (int y = 0; y < cy; ++y)
+      for (int x = 0; x < cx; ++x) v.push_back({brick, x * TX, y * TY, z, std::min(n[2], z + len)});
+  return v;
+}
+
+BrickDesc make_desc(gfx_fluid* h, const double* U_in, double* U_out, double* K,
+                    const double* P_in, const uint8_t* df, double* fluence,
+                    const double* dt_ptr, double weight, const int* skip) {
+  BrickDesc d;
+  memset(&d, 0, sizeof(d));
+  for (int a = 0; a < 3; ++a) {
+    d.n[a] = h->box.n[a];
+    d.m[a] = h->box.m[a];
+    d.bc[a][0] = h->box.bc[a][0];
+    d.bc[a][1] = h->box.bc[a][1];
+    d.geo[a] = h->dgeo[a];
+  }
+  d.nV = h->box.nV;
+  d.nP = h->box.nP;
+  d.U_in = U_in;
+  d.U_out = U_out;
+  d.K = K;
+  d.P_in = P_in;
+  d.Yp = h->Yp;
+  d.H = h->H;
+  d.df = df;
+  d.fluence = fluence;
+  d.face_size = (long long)h->face_size;
+  d.dt = dt_ptr;
+  d.weight = weight;
+  d.tsi_bits = h->tsi_bits;
+  d.skip = skip;
+  return d;
+}
+
+__global__ void set_scalar_kernel(double* p, double v) { *p = v; }
+
+// Compact proper-cell flag bytes into the ghost layout (ghosts get 0).
+__global__ void scatter_flags_kernel(Box b, const uint8_t* __restrict__ df,
+                                     uint8_t* __restrict__ out) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < b.nV;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(v % b.m[0]) - 2;
+    const int j = (int)((v / b.m[0]) % b.m[1]) - 2;
+    const int k = (int)(v / ((long long)b.m[0] * b.m[1])) - 2;
+    uint8_t f = 0;
+    if (i >= 0 && j >= 0 && k >= 0 && i < b.n[0] && j < b.n[1] && k < b.n[2])
+      f = df[i + (long long)b.n[0] * (j + (long long)b.n[1] * k)];
+    out[v] = f;
+  }
+}
+
+int run_features(gfx_fluid* h, const double* U, const double* Pst, cudaStream_t s) {
+  const int blk = 256;
+  detect_shock_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->ph, U, Pst, h->sb);
+  CUDA_TRY(cudaGetLastError());
+  detect_flags_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->sb, h->df);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 2;
+  return GFX_OK;
+}
+
+// The launches of one RK2 step on U (in place).  dt_ptr, skip: device scalars.
+// detect: whether the shock flags must be recomputed from U first.  ev (may
+// be null): 5 events recorded between the phases for gfx_fluid_step_timed.
+int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
+                 double* fluence, bool detect, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  const bool grav = h->cfg.uniform_acceleration != 0.0;
+  reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  if (fluence)
+    CUDA_TRY(cudaMemsetAsync(fluence, 0, sizeof(double) * 36 * h->face_size, s));
+  if (ev) CUDA_TRY(cudaEventRecord(ev[0], s));
+  if (hllc && detect) {
+    int rc = run_features(h, U, nullptr, s);
+    if (rc) return rc;
+  }
+  if (ev) CUDA_TRY(cudaEventRecord(ev[1], s));
+  const uint8_t* df = hllc ? h->df : nullptr;
+  const bool in_prim = h->prims_pending;
+  BrickDesc d1 = make_desc(h, U, nullptr, nullptr, in_prim ? h->Pst : nullptr, df, fluence,
+                           dt_ptr, 0.5, skip);
+  CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, hllc, grav, d1, nullptr, h->items, h->n_items,
+                        h->counters, h->ph, s));
+  if (ev) CUDA_TRY(cudaEventRecord(ev[2], s));
+  BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fluence, dt_ptr, 0.5, skip);
+  CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
+                        h->counters + 1, h->ph, s));
+  if (ev) CUDA_TRY(cudaEventRecord(ev[3], s));
+  const int blk = 256;
+  ghost_refresh_kernel<<<grid_for(h->box.nV, blk), blk, 0, s>>>(h->box, h->ph, U);
+  CUDA_TRY(cudaGetLastError());
+  if (ev) CUDA_TRY(cudaEventRecord(ev[4], s));
+  h->launches += 3;
+  return GFX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfx_fluid_config_default(gfx_fluid_config* c) {
+  if (!c) return fail(GFX_ERR_ARGUMENT, "config is NULL");
+  memset(c, 0, sizeof(*c));
+  for (int d = 0; d < 3; ++d) {
+    c->n_cells[d] = 32;
+    c->min_coordinate[d] = 0.0;
+    c->max_coordinate[d] = 1.0;
+    c->boundary[d][0] = c->boundary[d][1] = GFX_BC_OUTFLOW;
+  }
+  c->n_ghost_layers = 2;
+  c->riemann_solver = GFX_RIEMANN_HLLC;
+  c->use_limiter = 1;
+  c->limiter_parameter = 1.4;
+  c->adiabatic_index = 1.4;
+  c->shock_threshold = 0.1;
+  c->courant_factor = 0.7;
+  c->baryon_density_min = 0.0;
+  c->uniform_acceleration = 0.0;
+  c->n_ramp_cycles = 100;
+  return GFX_OK;
+}
+
+int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
+  if (!out) return fail(GFX_ERR_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  int rc = validate(cfg);
+  if (rc) return rc;
+  gfx_fluid* h = new (std::nothrow) gfx_fluid();
+  if (!h) return fail(GFX_ERR_NO_MEMORY, "host allocation failed");
+  h->cfg = *cfg;
+  Phys& ph = h->ph;
+  ph.gamma = cfg->adiabatic_index;
+  ph.gm1 = cfg->adiabatic_index - 1.0;
+  ph.c_v = 1.0 / (1.0 * (cfg->adiabatic_index - 1.0));
+  ph.theta = cfg->limiter_parameter;
+  ph.nmin = cfg->baryon_density_min;
+  ph.accel = cfg->uniform_acceleration;
+  ph.shock_threshold = cfg->shock_threshold;
+  ph.courant = cfg->courant_factor;
+  ph.use_limiter = cfg->use_limiter ? 1 : 0;
+  ph.n_ramp = cfg->n_ramp_cycles;
+  Box& b = h->box;
+  for (int d = 0; d < 3; ++d) {
+    b.n[d] = cfg->n_cells[d];
+    b.m[d] = cfg->n_cells[d] + 4;
+    b.bc[d][0] = cfg->boundary[d][0];
+    b.bc[d][1] = cfg->boundary[d][1];
+    h->axis[d] = build_axis(b.n[d], cfg->min_coordinate[d], cfg->max_coordinate[d], 2);
+  }
+  b.nV = (long long)b.m[0] * b.m[1] * b.m[2];
+  b.nP = (long long)b.n[0] * b.n[1] * b.n[2];
+  h->face_size = (size_t)std::max({(long long)b.n[1] * b.n[2], (long long)b.n[0] * b.n[2],
+                                   (long long)b.n[0] * b.n[1]});
+  auto cleanup = [&](int code) {
+    gfx_fluid_destroy(h);
+    return code;
+  };
+  // geometry arena: 6 tables per axis, each m + 1 long
+  size_t geo_len = 0;
+  for (int d = 0; d < 3; ++d) geo_len += 6 * (size_t)(b.m[d] + 1);
+  if (cudaMalloc(&h->geo, geo_len * sizeof(double)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc geometry"));
+  {
+    std::vector<double> host(geo_len, 0.0);
+    size_t off = 0;
+    for (int d = 0; d < 3; ++d) {
+      const HostAxis& a = h->axis[d];
+      const int L = b.m[d] + 1;
+      const std::vector<double>* tabs[6] = {&a.W, &a.WL, &a.WR, &a.dXI, &a.SQ, &a.CDEN};
+      const double** dst[6] = {&h->dgeo[d].W, &h->dgeo[d].WL, &h->dgeo[d].WR,
+                               &h->dgeo[d].dXI, &h->dgeo[d].SQ, &h->dgeo[d].CDEN};
+      for (int q = 0; q < 6; ++q) {
+        std::copy(tabs[q]->begin(), tabs[q]->end(), host.begin() + off);
+        *dst[q] = h->geo + off;
+        off += L;
+      }
+    }
+    if (cudaMemcpy(h->geo, host.data(), geo_len * sizeof(double), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return cleanup(fail(GFX_ERR_CUDA, "copy geometry tables"));
+  }
+  const size_t nP = (size_t)b.nP;
+  if (cudaMalloc(&h->Yp, 5 * nP * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->H, 5 * nP * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->Pst, 5 * nP * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->df, nP) != cudaSuccess || cudaMalloc(&h->sb, nP) != cudaSuccess ||
+      cudaMalloc(&h->tsi_bits, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&h->counters, 4 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&h->clock, 2 * sizeof(Clock)) != cudaSuccess ||
+      cudaMalloc(&h->dt_slot, sizeof(double)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc of the stage scratch (%zu cells)", nP));
+  if (cudaMemset(h->df, 0, nP) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_CUDA, "clear features"));
+  std::vector<WorkItem> items = make_items(b.n, 0);
+  h->n_items = (int)items.size();
+  if (cudaMalloc(&h->items, items.size() * sizeof(WorkItem)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc work items"));
+  if (cudaMemcpy(h->items, items.data(), items.size() * sizeof(WorkItem),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_CUDA, "copy work items"));
+  h->features = FEAT_ZERO;
+  *out = h;
+  return GFX_OK;
+}
+
+int gfx_fluid_destroy(gfx_fluid* h) {
+  if (!h) return GFX_OK;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  cudaFree(h->geo);
+  cudaFree(h->Yp);
+  cudaFree(h->H);
+  cudaFree(h->Pst);
+  cudaFree(h->df);
+  cudaFree(h->sb);
+  cudaFree(h->tsi_bits);
+  cudaFree(h->counters);
+  cudaFree(h->clock);
+  cudaFree(h->dt_slot);
+  cudaFree(h->items);
+  cudaFree(h->U_stage);
+  if (h->host_stream) cudaStreamDestroy(h->host_stream);
+  delete h;
+  return GFX_OK;
+}
+
+int gfx_fluid_n_values(const gfx_fluid* h, size_t* n) {
+  if (!h || !n) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *n = (size_t)h->box.nV;
+  return GFX_OK;
+}
+
+int gfx_fluid_fluence_face_size(const gfx_fluid* h, size_t* face_size) {
+  if (!h || !face_size) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *face_size = h->face_size;
+  return GFX_OK;
+}
+
+int gfx_fluid_geometry(const gfx_fluid* h, int axis, double* c, double* wl, double* wr) {
+  if (!h || axis < 0 || axis > 2) return fail(GFX_ERR_ARGUMENT, "bad handle or axis");
+  const HostAxis& a = h->axis[axis];
+  if (c) std::copy(a.X.begin(), a.X.end(), c);
+  if (wl) std::copy(a.WL.begin(), a.WL.end(), wl);
+  if (wr) std::copy(a.WR.begin(), a.WR.end(), wr);
+  return GFX_OK;
+}
+
+int gfx_fluid_from_primitive(gfx_fluid* h, const double* prim, double* U, void* stream) {
+  if (!h || !prim || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  from_primitive_kernel<<<grid_for(h->box.nV, 256), 256, 0, s>>>(h->box, h->ph, prim, U,
+                                                                  h->Pst);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  h->prims_pending = true;
+  return GFX_OK;
+}
+
+int gfx_fluid_to_primitive(gfx_fluid* h, double* U, double* prim, double* aux, void* stream) {
+  if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  to_primitive_kernel<<<grid_for(h->box.nV, 256), 256, 0, s>>>(h->box, h->ph, U, prim, aux);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  h->prims_pending = false;
+  return GFX_OK;
+}
+
+int gfx_fluid_detect_features(gfx_fluid* h, const double* U, void* stream) {
+  if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  int rc = run_features(h, U, h->prims_pending ? h->Pst : nullptr, (cudaStream_t)stream);
+  if (rc) return rc;
+  h->features = FEAT_VALID;
+  return GFX_OK;
+}
+
+int gfx_fluid_clear_features(gfx_fluid* h, void* stream) {
+  if (!h) return fail(GFX_ERR_ARGUMENT, "NULL handle");
+  CUDA_TRY(cudaMemsetAsync(h->df, 0, (size_t)h->box.nP, (cudaStream_t)stream));
+  h->features = FEAT_ZERO;
+  return GFX_OK;
+}
+
+int gfx_fluid_get_features(gfx_fluid* h, uint8_t* flags, void* stream) {
+  if (!h || !flags) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->features == FEAT_PENDING) {
+    int rc = run_features(h, h->features_src, nullptr, s);
+    if (rc) return rc;
+    h->features = FEAT_VALID;
+  }
+  scatter_flags_kernel<<<grid_for(h->box.nV, 256), 256, 0, s>>>(h->box, h->df, flags);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  return GFX_OK;
+}
+
+int gfx_fluid_increment(gfx_fluid* h, const double* U, double* K, double dt, double weight,
+                        double* fluence, void* stream) {
+  if (!h || !U || !K) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  if (hllc && h->features == FEAT_PENDING) {
+    int rc = run_features(h, h->features_src, nullptr, s);
+    if (rc) return rc;
+    h->features = FEAT_VALID;
+  }
+  set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
+  reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
+  CUDA_TRY(cudaGetLastError());
+  const bool in_prim = h->prims_pending;
+  BrickDesc d = make_desc(h, U, nullptr, K, in_prim ? h->Pst : nullptr, hllc ? h->df : nullptr,
+                          fluence, h->dt_slot, weight, nullptr);
+  CUDA_TRY(launch_stage(MODE_INCREMENT, in_prim, hllc, false, d, nullptr, h->items,
+                        h->n_items, h->counters, h->ph, s));
+  h->launches += 3;
+  return GFX_OK;
+}
+
+int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* stream) {
+  if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  cudaStream_t s = (cudaStream_t)stream;
+  set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  const bool detect = (h->features == FEAT_PENDING);
+  int rc = enqueue_step(h, U, h->dt_slot, nullptr, fluence, detect, s);
+  if (rc) return rc;
+  h->prims_pending = false;
+  h->features = FEAT_PENDING;
+  h->features_src = U;
+  return GFX_OK;
+}
+
+int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence_host) {
+  if (!h || !U_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  const size_t bytes = 6 * (size_t)h->box.nV * sizeof(double);
+  if (!h->host_stream) CUDA_TRY(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
+  if (!h->U_stage) {
+    if (cudaMalloc(&h->U_stage, bytes + 36 * h->face_size * sizeof(double)) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc host-step staging");
+  }
+  cudaStream_t s = h->host_stream;
+  double* fl = fluence_host ? h->U_stage + 6 * (size_t)h->box.nV : nullptr;
+  CUDA_TRY(cudaMemcpyAsync(h->U_stage, U_host, bytes, cudaMemcpyHostToDevice, s));
+  int rc = gfx_fluid_step(h, h->U_stage, dt, fl, s);
+  if (rc) return rc;
+  h->features_src = h->U_stage;
+  CUDA_TRY(cudaMemcpyAsync(U_host, h->U_stage, bytes, cudaMemcpyDeviceToHost, s));
+  if (fluence_host)
+    CUDA_TRY(cudaMemcpyAsync(fluence_host, fl, 36 * h->face_size * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return GFX_OK;
+}
+
+int gfx_fluid_timestep(gfx_fluid* h, const double* U, int i_cycle, double* dt_host,
+                       void* stream) {
+  if (!h || !U || !dt_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 0);
+  CUDA_TRY(cudaGetLastError());
+  inverse_timestep_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(
+      h->box, h->ph, U, h->prims_pending ? h->Pst : nullptr, h->dgeo[0].W, h->dgeo[1].W,
+      h->dgeo[2].W, h->tsi_bits);
+  CUDA_TRY(cudaGetLastError());
+  Clock c;
+  memset(&c, 0, sizeof(c));
+  c.cycle = i_cycle;
+  c.time = 0.0;
+  c.finish = DBL_MAX;
+  c.max_cycle = 0x7fffffff;
+  Clock* dc = h->clock + 1;
+  CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  finalize_dt_kernel<<<1, 1, 0, s>>>(h->ph, h->tsi_bits, dc, 1, 0);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 3;
+  CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  *dt_host = c.dt;
+  return GFX_OK;
+}
+
+int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double finish_time,
+                     int n_cycles_max, double* time_out, int* i_cycle_out, void* stream) {
+  if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (n_cycles_max < 0) return fail(GFX_ERR_ARGUMENT, "n_cycles_max < 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  Clock c;
+  memset(&c, 0, sizeof(c));
+  c.time = time;
+  c.finish = finish_time;
+  c.cycle = i_cycle;
+  c.max_cycle = (int)std::min<long long>(0x7fffffffLL, (long long)i_cycle + n_cycles_max);
+  c.done = !(c.time < c.finish && c.cycle < c.max_cycle);
+  Clock* dc = h->clock;
+  CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  if (!c.done) {
+    // initial dt from the state (ComputeNewTime before the first cycle)
+    reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 0);
+    inverse_timestep_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(
+        h->box, h->ph, U, h->prims_pending ? h->Pst : nullptr, h->dgeo[0].W, h->dgeo[1].W,
+        h->dgeo[2].W, h->tsi_bits);
+    finalize_dt_kernel<<<1, 1, 0, s>>>(h->ph, h->tsi_bits, dc, 1, 1);
+    CUDA_TRY(cudaGetLastError());
+    h->launches += 3;
+    // first cycle eagerly (its features follow the handle's state)
+    int rc = enqueue_step(h, U, &dc->dt, &dc->done, nullptr, h->features == FEAT_PENDING, s);
+    if (rc) return rc;
+    advance_clock_kernel<<<1, 1, 0, s>>>(dc, 1);
+    finalize_dt_kernel<<<1, 1, 0, s>>>(h->ph, h->tsi_bits, dc, 1, 1);
+    CUDA_TRY(cudaGetLastError());
+    h->launches += 2;
+    h->prims_pending = false;
+    h->features = FEAT_PENDING;
+    h->features_src = U;
+    // remaining cycles: one graph per cycle, replayed
+    if (h->graph && (h->graph_U != U)) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    if (!h->graph) {
+      cudaStream_t cs;
+      CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      const long long before = h->launches;
+      CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      int rc2 = enqueue_step(h, U, &dc->dt, &dc->done, nullptr, true, cs);
+      advance_clock_kernel<<<1, 1, 0, cs>>>(dc, 1);
+      finalize_dt_kernel<<<1, 1, 0, cs>>>(h->ph, h->tsi_bits, dc, 1, 1);
+      cudaError_t ce = cudaStreamEndCapture(cs, &g);
+      cudaStreamDestroy(cs);
+      h->graph_kernels = h->launches - before + 2;
+      h->launches = before;
+      if (rc2) return rc2;
+      if (ce != cudaSuccess) return fail(GFX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&h->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess)
+        return fail(GFX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      h->graph_U = U;
+    }
+    int done_cycles = 1;
+    const int chunk = 8;
+    while (done_cycles < n_cycles_max) {
+      const int nrep = std::min(chunk, n_cycles_max - done_cycles);
+      for (int r = 0; r < nrep; ++r) CUDA_TRY(cudaGraphLaunch(h->graph, s));
+      h->launches += (long long)nrep * h->graph_kernels;
+      done_cycles += nrep;
+      CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaStreamSynchronize(s));
+      if (c.done) break;
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (time_out) *time_out = c.time;
+  if (i_cycle_out) *i_cycle_out = c.cycle;
+  return GFX_OK;
+}
+
+int gfx_fluid_step_timed(gfx_fluid* h, double* U, double dt, double* fluence, double* ms_out,
+                         void* stream) {
+  if (!h || !U || !ms_out) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t ev[5];
+  for (int i = 0; i < 5; ++i) CUDA_TRY(cudaEventCreate(&ev[i]));
+  set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  const bool detect = (h->features == FEAT_PENDING);
+  int rc = enqueue_step(h, U, h->dt_slot, nullptr, fluence, detect, s, ev);
+  if (rc == GFX_OK) {
+    h->prims_pending = false;
+    h->features = FEAT_PENDING;
+    h->features_src = U;
+    cudaError_t e = cudaEventSynchronize(ev[4]);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+      float ms = 0.f;
+      e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      ms_out[i] = ms;
+    }
+    if (e != cudaSuccess) rc = fail(GFX_ERR_CUDA, "event timing: %s", cudaGetErrorString(e));
+  }
+  for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+  return rc;
+}
+
+int gfx_fluid_kernel_launches(const gfx_fluid* h, long long* count) {
+  if (!h || !count) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *count = h->launches;
+  return GFX_OK;
+}
+
+int gfx_fluid_check_state(gfx_fluid* h, void* stream) {
+  if (!h) return fail(GFX_ERR_ARGUMENT, "NULL handle");
+  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return GFX_OK;
+}
+
+int gfx_fluid_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return GFX_ERR_ARGUMENT;
+  snprintf(buf, len, "%s", g_last_error.c_str());
+  return GFX_OK;
+}
+
+}  // extern "C"

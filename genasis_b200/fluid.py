@@ -1,0 +1,212 @@
+"""Host-side mirror of the reference's operator interface for the fluid step.
+
+The classes keep the reference's names and call surfaces, backed by the C ABI
+of libgfx_fluid.so; PyTorch provides device memory and the current stream.
+
+  FluidBox                 FluidBox_Form (Universes/FluidBox_Form.f90:37-241):
+                           one brick, its Fluid_P_I current (the conserved state
+                           U with ghosts) and features
+  Step_RK2_C_ASC.compute   Step_RK_C_ASC_Template % Compute (time, time_step)
+  IncrementDivergence_FV.compute
+                           IncrementDivergence_FV_Form % Compute
+                           (increment, time_step, weight_rk)
+  Integrator_C_PS          ComputeTimeStep / Evolve of the integrator
+
+Errors come back as GfxError (the library never aborts); the reference shows
+them and calls PROGRAM_HEADER % Abort, which the caller may still do.
+"""
+import ctypes
+
+import numpy as np
+
+from . import lib
+from .config import FluidConfig
+
+
+def _torch():
+    import torch  # noqa: WPS433 (device memory and streams only)
+
+    return torch
+
+
+def _stream():
+    return ctypes.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class FluidBox:
+    """One brick of Fluid_P_I on the current CUDA device."""
+
+    def __init__(self, config: FluidConfig, device=None):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("FluidBox needs a CUDA device (there is no CPU path)")
+        self.config = config
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self._c = config.to_c()
+        h = ctypes.c_void_p()
+        lib.call("gfx_fluid_create", ctypes.byref(self._c), ctypes.byref(h))
+        self.h = h
+        n = ctypes.c_size_t()
+        lib.call("gfx_fluid_n_values", self.h, ctypes.byref(n))
+        self.n_values = int(n.value)
+        fs = ctypes.c_size_t()
+        lib.call("gfx_fluid_fluence_face_size", self.h, ctypes.byref(fs))
+        self.face_size = int(fs.value)
+        self.U = torch.zeros((6,) + config.shape, dtype=torch.float64, device=self.device)
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            lib.load().gfx_fluid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 -- interpreter shutdown
+            pass
+
+    # -- geometry ------------------------------------------------------------
+    def geometry(self, axis):
+        m = int(self.config.n_cells[axis]) + 2 * int(self.config.n_ghost_layers)
+        c, wl, wr = (np.zeros(m) for _ in range(3))
+        lib.call("gfx_fluid_geometry", self.h, axis, c.ctypes.data_as(ctypes.c_void_p),
+                 wl.ctypes.data_as(ctypes.c_void_p), wr.ctypes.data_as(ctypes.c_void_p))
+        return c, wl, wr
+
+    # -- Fluid_P_I ------------------------------------------------------------
+    def compute_from_primitive(self, prim):
+        """ComputeFromPrimitive on every value (after the periodic exchange);
+        prim: [N, V1, V2, V3, E] over the ghost-inclusive brick."""
+        torch = _torch()
+        p = torch.as_tensor(np.ascontiguousarray(prim) if isinstance(prim, np.ndarray) else prim,
+                            dtype=torch.float64, device=self.device).contiguous()
+        assert tuple(p.shape) == (5,) + self.config.shape
+        lib.call("gfx_fluid_from_primitive", self.h, _ptr(p), _ptr(self.U), _stream())
+        return self.U
+
+    def set_conserved(self, U):
+        torch = _torch()
+        self.U.copy_(torch.as_tensor(U, dtype=torch.float64))
+        return self.U
+
+    def compute_from_conserved(self, detect_features=False, primitive=False, aux=False):
+        """ComputeFromConserved (floors U in place); optionally returns the
+        primitives [5][...] and (P, CS, SB)."""
+        torch = _torch()
+        prim = torch.empty((5,) + self.config.shape, dtype=torch.float64,
+                           device=self.device) if primitive else None
+        ax = torch.empty((3,) + self.config.shape, dtype=torch.float64,
+                         device=self.device) if aux else None
+        lib.call("gfx_fluid_to_primitive", self.h, _ptr(self.U), _ptr(prim), _ptr(ax), _stream())
+        if detect_features:
+            self.detect_features()
+        return prim, ax
+
+    def detect_features(self):
+        lib.call("gfx_fluid_detect_features", self.h, _ptr(self.U), _stream())
+
+    def clear_features(self):
+        lib.call("gfx_fluid_clear_features", self.h, _stream())
+
+    def features(self):
+        """DIFFUSIVE_FLUX_I bits (bit d = direction d) over every value."""
+        torch = _torch()
+        f = torch.zeros(self.config.shape, dtype=torch.uint8, device=self.device)
+        lib.call("gfx_fluid_get_features", self.h, _ptr(f), _stream())
+        return f
+
+    def new_fluence(self):
+        torch = _torch()
+        return torch.zeros((6, 6, self.face_size), dtype=torch.float64, device=self.device)
+
+    # -- increment, step, time step --------------------------------------------
+    def increment(self, K, time_step, weight_rk=1.0, fluence=None):
+        lib.call("gfx_fluid_increment", self.h, _ptr(self.U), _ptr(K), float(time_step),
+                 float(weight_rk), _ptr(fluence), _stream())
+        return K
+
+    def step(self, time_step, fluence=None):
+        lib.call("gfx_fluid_step", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
+                 _stream())
+
+    def step_host(self, U_host, time_step, fluence_host=None):
+        """One step on a host (ideally pinned) tensor: copy in, step, copy out."""
+        lib.call("gfx_fluid_step_host", self.h, _ptr(U_host), float(time_step),
+                 _ptr(fluence_host))
+
+    def step_timed(self, time_step, fluence=None):
+        """One step with CUDA events around each launch; returns the device
+        milliseconds of (features, stage 1, stage 2, ghost refresh)."""
+        ms = (ctypes.c_double * 4)()
+        lib.call("gfx_fluid_step_timed", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
+                 ms, _stream())
+        return tuple(ms)
+
+    def kernel_launches(self):
+        n = ctypes.c_longlong()
+        lib.call("gfx_fluid_kernel_launches", self.h, ctypes.byref(n))
+        return int(n.value)
+
+    def compute_time_step(self, i_cycle=0):
+        dt = ctypes.c_double()
+        lib.call("gfx_fluid_timestep", self.h, _ptr(self.U), int(i_cycle), ctypes.byref(dt),
+                 _stream())
+        return dt.value
+
+    def evolve(self, finish_time, time=0.0, i_cycle=0, max_cycles=2**31 - 1):
+        t = ctypes.c_double()
+        c = ctypes.c_int()
+        lib.call("gfx_fluid_evolve", self.h, _ptr(self.U), float(time), int(i_cycle),
+                 float(finish_time), int(max_cycles), ctypes.byref(t), ctypes.byref(c),
+                 _stream())
+        return t.value, c.value
+
+
+class Step_RK2_C_ASC:
+    """Step_RK_C_ASC_Template % Compute (Step_RK_C_ASC__Template.f90:504-542)
+    on a FluidBox's current."""
+
+    def __init__(self, box: FluidBox):
+        self.box = box
+        self.boundary_fluence = box.new_fluence()
+
+    def compute(self, time, time_step):
+        del time  # the RK2 stages of this fluid do not depend on the time
+        self.box.step(time_step, self.boundary_fluence)
+
+
+class IncrementDivergence_FV:
+    """IncrementDivergence_FV_Form % Compute (IncrementDivergence_FV__Form.f90:344-412)."""
+
+    def __init__(self, box: FluidBox):
+        self.box = box
+        self.boundary_fluence = box.new_fluence()
+
+    def compute(self, increment, time_step, weight_rk):
+        """increment: [6][...] device tensor, assumed cleared by the caller as
+        the reference assumes."""
+        return self.box.increment(increment, time_step, weight_rk, self.boundary_fluence)
+
+
+class Integrator_C_PS:
+    """The integrator's ComputeTimeStep and Evolve loop (Integrator_Template.f90)."""
+
+    def __init__(self, box: FluidBox, finish_time, finish_cycle=2**31 - 1):
+        self.box = box
+        self.time = 0.0
+        self.i_cycle = 0
+        self.finish_time = finish_time
+        self.finish_cycle = finish_cycle
+
+    def compute_time_step(self):
+        return self.box.compute_time_step(self.i_cycle)
+
+    def evolve(self):
+        self.time, self.i_cycle = self.box.evolve(
+            self.finish_time, self.time, self.i_cycle, self.finish_cycle - self.i_cycle)
+        return self.time, self.i_cycle

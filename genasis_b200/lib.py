@@ -1,0 +1,93 @@
+"""ctypes binding of libgfx_fluid.so (the C ABI of include/gfx_fluid.h).
+
+The library is the only compute path: if it is missing or cannot load, every
+entry point raises; there is no CPU fallback."""
+import ctypes
+import os
+
+from .config import GfxConfig
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgfx_fluid.so")
+
+GFX_OK = 0
+STATUS = {
+    -1: "GFX_ERR_ARGUMENT",
+    -2: "GFX_ERR_CUDA",
+    -3: "GFX_ERR_UNSUPPORTED",
+    -4: "GFX_ERR_STATE",
+    -5: "GFX_ERR_TIMEOUT",
+    -6: "GFX_ERR_NO_MEMORY",
+}
+
+# name -> (restype, argtypes); every entry point returns an int status.
+P = ctypes.c_void_p
+D = ctypes.c_double
+I = ctypes.c_int
+SZ = ctypes.c_size_t
+SIGNATURES = {
+    "gfx_fluid_config_default": [ctypes.POINTER(GfxConfig)],
+    "gfx_fluid_create": [ctypes.POINTER(GfxConfig), ctypes.POINTER(P)],
+    "gfx_fluid_destroy": [P],
+    "gfx_fluid_n_values": [P, ctypes.POINTER(SZ)],
+    "gfx_fluid_geometry": [P, I, P, P, P],
+    "gfx_fluid_from_primitive": [P, P, P, P],
+    "gfx_fluid_to_primitive": [P, P, P, P, P],
+    "gfx_fluid_detect_features": [P, P, P],
+    "gfx_fluid_clear_features": [P, P],
+    "gfx_fluid_get_features": [P, P, P],
+    "gfx_fluid_increment": [P, P, P, D, D, P, P],
+    "gfx_fluid_fluence_face_size": [P, ctypes.POINTER(SZ)],
+    "gfx_fluid_step": [P, P, D, P, P],
+    "gfx_fluid_step_host": [P, P, D, P],
+    "gfx_fluid_timestep": [P, P, I, ctypes.POINTER(D), P],
+    "gfx_fluid_evolve": [P, P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I), P],
+    "gfx_fluid_step_timed": [P, P, D, P, P, P],
+    "gfx_fluid_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
+    "gfx_fluid_check_state": [P, P],
+    "gfx_fluid_last_error": [ctypes.c_char_p, SZ],
+}
+
+_lib = None
+
+
+class GfxError(RuntimeError):
+    def __init__(self, status, where, message):
+        super().__init__("%s: %s (%s)" % (where, message, STATUS.get(status, status)))
+        self.status = status
+
+
+def load():
+    """Loads the in-tree library (raises if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            "libgfx_fluid.so is not built (run genasis_b200/build_ext.py or "
+            "__graft_entry__.build()); there is no fallback path")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = ctypes.c_int
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(1024)
+    load().gfx_fluid_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def call(name, *args):
+    """Calls an entry point and raises GfxError on a nonzero status."""
+    rc = getattr(load(), name)(*args)
+    if rc != GFX_OK:
+        raise GfxError(rc, name, last_error())
+    return rc
+
+
+def exported_symbols():
+    return list(SIGNATURES)

@@ -1,0 +1,167 @@
+/*
+ * gfx_fluid.h -- C ABI of the B200 finite-volume step for the GenASiS
+ * polytropic / ideal-gas fluid (Fluid_P_I): PLM reconstruction with the
+ * generalized-minmod limiter, HLL / HLLC fluxes, flux divergence, RK2 stages,
+ * conserved-to-primitive recovery, shock features and the CFL time step.
+ *
+ * Every entry point returns an int status (GFX_OK = 0, negative on error) and
+ * never aborts; gfx_fluid_last_error() gives the message of the last failure
+ * on the calling thread.  The Fortran side reaches these through
+ * ISO_C_BINDING interfaces.
+ *
+ * Data layout (the reference's StorageForm % Value(nValues, nVariables),
+ * Storage_Form.f90:30): one contiguous FP64 array per variable, x fastest,
+ * over the brick including n_ghost_layers (= 2) ghosts on every side,
+ * nV = (nx+4)(ny+4)(nz+4) values per variable.
+ *   conserved U : [D, S1, S2, S3, G, DS][nV]   (Fluid_D__Form.f90:650-654,
+ *                                               Fluid_P__Template.f90:718-725)
+ *   primitive   : [N, V1, V2, V3, E][nV]
+ * Pointers named *_dev are device pointers; *_host are host pointers.
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ */
+#ifndef GFX_FLUID_H
+#define GFX_FLUID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFX_FLUID_ABI_VERSION 1
+
+enum gfx_status {
+  GFX_OK = 0,
+  GFX_ERR_ARGUMENT = -1,    /* bad pointer, size or configuration value */
+  GFX_ERR_CUDA = -2,        /* a CUDA runtime call or kernel launch failed */
+  GFX_ERR_UNSUPPORTED = -3, /* option the reference has but this build does not */
+  GFX_ERR_STATE = -4,       /* non-finite or non-positive state detected */
+  GFX_ERR_TIMEOUT = -5,     /* a bounded device-side wait expired */
+  GFX_ERR_NO_MEMORY = -6    /* device or host allocation failed */
+};
+
+/* Atlas boundary conditions (Atlas_SC__Template.f90:244-324) */
+enum { GFX_BC_OUTFLOW = 0, GFX_BC_REFLECTING = 1, GFX_BC_PERIODIC = 2 };
+/* Fluid_ASC RiemannSolverType (Fluid_ASC__Form.f90:128-137) */
+enum { GFX_RIEMANN_HLL = 0, GFX_RIEMANN_HLLC = 1 };
+
+/* Parameters of one single-brick chart + Fluid_P_I + Step_RK2 + Integrator.
+ * Names follow the reference's GetParameter names; gfx_fluid_config_default
+ * fills the reference defaults. */
+typedef struct gfx_fluid_config {
+  int    n_cells[3];            /* nCells (proper cells per axis) */
+  int    n_ghost_layers;        /* nGhostLayers; must be 2 */
+  double min_coordinate[3];     /* MinCoordinate (0) */
+  double max_coordinate[3];     /* MaxCoordinate (1) */
+  int    boundary[3][2];        /* BoundaryConditionsFace, [axis][inner, outer] */
+  int    riemann_solver;        /* RiemannSolverType (HLLC) */
+  int    use_limiter;           /* UseLimiter (1) */
+  double limiter_parameter;     /* LimiterParameter (1.4) */
+  double adiabatic_index;       /* AdiabaticIndex (1.4) */
+  double shock_threshold;       /* ShockThreshold (0.1) */
+  double courant_factor;        /* CourantFactor (0.7) */
+  double baryon_density_min;    /* BaryonDensityMin (0) */
+  double uniform_acceleration;  /* UniformAcceleration along z (0 = no gravity) */
+  int    n_ramp_cycles;         /* nRampCycles (100) */
+} gfx_fluid_config;
+
+typedef struct gfx_fluid gfx_fluid;
+
+/* Reference defaults (ChartHeader_SL__Form.f90:345-366, Fluid_ASC__Form.f90,
+ * FluidFeatures_ASC__Form.f90:61-65, Integrator_C_PS__Form.f90:136,
+ * IntegratorHeader_Form.f90:95). */
+int gfx_fluid_config_default(gfx_fluid_config *cfg);
+
+/* Creates the handle: device geometry tables, scratch and feature storage.
+ * Replaces FluidBox / Step_RK2_C_ASC Initialize (FluidBox_Form.f90:37-241). */
+int gfx_fluid_create(const gfx_fluid_config *cfg, gfx_fluid **out);
+int gfx_fluid_destroy(gfx_fluid *h);
+
+int gfx_fluid_n_values(const gfx_fluid *h, size_t *n_values);
+
+/* Cell centres and left / right half widths of one axis over the ghost-
+ * inclusive index range (n_cells[axis] + 4 values each; host pointers).
+ * Chart_Template.f90:478-560, 827-841, 973-990. */
+int gfx_fluid_geometry(const gfx_fluid *h, int axis, double *center_host,
+                       double *width_left_host, double *width_right_host);
+
+/* Fluid_P_I % ComputeFromPrimitive on every value after the periodic ghost
+ * exchange of the primitives (Integrator_C_PS__Form.f90:194-203,
+ * Fluid_P_I__Form.f90:509-601): prim_dev -> U_dev.  The primitives are kept
+ * as the state of the next step, as the reference's Current keeps them. */
+int gfx_fluid_from_primitive(gfx_fluid *h, const double *prim_dev, double *U_dev,
+                             void *stream);
+
+/* Fluid_P_I % ComputeFromConserved on every value (Fluid_P_I__Form.f90:604-722):
+ * U_dev is floored in place (and its DS recomputed); prim_dev ([5][nV], may be
+ * NULL) receives N, V1, V2, V3, E; aux_dev ([3][nV], may be NULL) receives the
+ * pressure P, sound speed CS and entropy per baryon SB. */
+int gfx_fluid_to_primitive(gfx_fluid *h, double *U_dev, double *prim_dev, double *aux_dev,
+                           void *stream);
+
+/* FluidFeatures_P % Detect (FluidFeatures_P__Form.f90:145-171) on the state
+ * U_dev; the flags feed the HLLC flux of the following increments / steps.
+ * gfx_fluid_clear_features zeroes them (the state after initialisation). */
+int gfx_fluid_detect_features(gfx_fluid *h, const double *U_dev, void *stream);
+int gfx_fluid_clear_features(gfx_fluid *h, void *stream);
+/* DIFFUSIVE_FLUX_I flags of every value as bytes, bit d = direction d. */
+int gfx_fluid_get_features(gfx_fluid *h, uint8_t *flags_dev, void *stream);
+
+/* IncrementDivergence_FV % Compute (IncrementDivergence_FV__Form.f90:344-412):
+ * K_dev ([6][nV]) += the divergence increment of the state U_dev over proper
+ * cells, all six conserved fields; fluence_dev ([6 fields][6 faces][face_size],
+ * may be NULL) += weight_rk * dt * F on the boundary faces
+ * (RecordBoundaryFluence_CSL, :1002-1069). */
+int gfx_fluid_increment(gfx_fluid *h, const double *U_dev, double *K_dev, double dt,
+                        double weight_rk, double *fluence_dev, void *stream);
+int gfx_fluid_fluence_face_size(const gfx_fluid *h, size_t *face_size);
+
+/* Step_RK_C_ASC % Compute (Step_RK_C_ASC__Template.f90:504-542): one RK2 step
+ * of size dt on U_dev in place, ending with ComputeFromConserved and feature
+ * detection of the new state.  fluence_dev (may be NULL) is cleared and
+ * receives the step's boundary fluence.  Ghost values are refreshed as the
+ * reference leaves them (periodic images; floors on physical ghosts). */
+int gfx_fluid_step(gfx_fluid *h, double *U_dev, double dt, double *fluence_dev,
+                   void *stream);
+
+/* The same step with U in host memory: copies in, steps, copies out, and
+ * returns after the result is back on the host. */
+int gfx_fluid_step_host(gfx_fluid *h, double *U_host, double dt, double *fluence_host);
+
+/* Integrator ComputeTimeStep (Integrator_Template.f90:896-939) on U_dev:
+ * CourantFactor / max inverse CFL time (Integrator_C_PS__Kernel.f90:97-142),
+ * ramped by min((i_cycle + 1) / nRampCycles, 1).  Synchronises the stream. */
+int gfx_fluid_timestep(gfx_fluid *h, const double *U_dev, int i_cycle, double *dt_host,
+                       void *stream);
+
+/* Integrator % Evolve loop on the device (Integrator_Template.f90:291-346):
+ * from (time, i_cycle) advance U_dev until finish_time (the last step is cut
+ * to land on it, as CheckpointTimeExact does) or until n_cycles_max cycles,
+ * each cycle = time step + RK2 step.  Uses a CUDA graph per cycle; returns
+ * after the work completes with the final time and cycle count. */
+int gfx_fluid_evolve(gfx_fluid *h, double *U_dev, double time, int i_cycle,
+                     double finish_time, int n_cycles_max, double *time_out,
+                     int *i_cycle_out, void *stream);
+
+/* gfx_fluid_step with a CUDA event recorded around each launch (the
+ * reference's per-phase timers, StorageDivergence_Form.f90:45-74): ms_out[4]
+ * receives the device milliseconds of features, stage 1, stage 2 and the
+ * ghost refresh.  Synchronises the stream. */
+int gfx_fluid_step_timed(gfx_fluid *h, double *U_dev, double dt, double *fluence_dev,
+                         double *ms_out, void *stream);
+
+/* Number of kernels this handle has launched (graph replays included). */
+int gfx_fluid_kernel_launches(const gfx_fluid *h, long long *count);
+
+/* Bit pattern of the device-side error word accumulated by the kernels since
+ * the last call (GFX_ERR_STATE if non-finite or non-positive density / energy
+ * was produced); clears it.  Synchronises the stream. */
+int gfx_fluid_check_state(gfx_fluid *h, void *stream);
+
+int gfx_fluid_last_error(char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

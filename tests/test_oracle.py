@@ -1,0 +1,293 @@
+"""CPU tests of the oracle (the reference restatement) and of the properties
+of the reference step that the CUDA kernels rely on.
+
+The reference ships no golden vectors for this path and cannot be compiled
+here (Fortran + MPI), so the oracle is pinned by hand-derived known answers,
+invariants of the scheme and the committed regression fixtures."""
+import math
+
+import numpy as np
+import pytest
+
+from genasis_b200 import problems
+from genasis_b200.config import FluidConfig
+from oracle.oracle import Oracle
+
+
+def proper(cfg):
+    return cfg.proper
+
+
+def test_geometry_matches_python_restatement_bitwise():
+    for n, lo, hi in [(16, 0.0, 1.0), (37, 0.0, 1.0), (384, 0.0, 0.5), (768, 0.0, 1.0)]:
+        cfg = FluidConfig(n_cells=(n, 4, 4), min_coordinate=(lo, 0, 0), max_coordinate=(hi, 1, 1))
+        o = Oracle(cfg)
+        c, wl, wr = o.geometry(0)
+        pc, pwl, pwr = problems.axis_geometry(n, lo, hi)
+        assert np.array_equal(c, pc) and np.array_equal(wl, pwl) and np.array_equal(wr, pwr)
+
+
+def test_ghost_widths_are_single_precision():
+    # Chart_Template.f90 declares the ghost widths real(KDL): single precision.
+    n = 768
+    c, wl, wr = problems.axis_geometry(n, 0.0, 1.0)
+    ghost_width = wl[0] + wr[0]
+    proper_width = wl[2] + wr[2]
+    assert ghost_width != proper_width
+    assert abs(ghost_width - proper_width) < 1e-7 * proper_width
+    assert float(np.float32(ghost_width)) == pytest.approx(ghost_width, rel=1e-15)
+
+
+def _uniform(cfg, v=(0.3, -0.2, 0.1)):
+    prim = np.zeros((5,) + cfg.shape)
+    prim[0] = 1.3
+    for d in range(3):
+        prim[1 + d] = v[d]
+    prim[4] = 2.0
+    return prim
+
+
+@pytest.mark.parametrize("rs", ["HLL", "HLLC"])
+@pytest.mark.parametrize("bc", ["OUTFLOW", "PERIODIC"])
+def test_uniform_state_has_zero_increment(rs, bc):
+    cfg = FluidConfig(n_cells=(8, 6, 5), riemann_solver=rs, boundary=((bc, bc),) * 3)
+    o = Oracle(cfg)
+    o.set_primitive(_uniform(cfg, (0.0, 0.0, 0.0) if bc == "OUTFLOW" else (0.3, -0.2, 0.1)))
+    K = o.increment(1e-3)
+    assert np.all(K[(slice(None),) + cfg.proper] == 0.0)
+
+
+def test_linear_profile_is_reconstructed_exactly():
+    # A linear density with uniform velocity and pressure: the limiter returns
+    # the profile's slope, the two face states agree, the HLL diffusion term
+    # vanishes and K_D = -dt v dN/dx in the interior.
+    n = 24
+    cfg = FluidConfig(n_cells=(n, 4, 4), riemann_solver="HLL")
+    X, Y, Z = problems.centers(cfg)
+    prim = np.zeros((5,) + cfg.shape)
+    slope = 0.5
+    prim[0] = 1.0 + slope * X
+    prim[1] = 1.0
+    prim[4] = 2.5
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    dt = 1e-3
+    K = o.increment(dt)
+    kd = K[0][cfg.proper][:, :, 3:-3]
+    assert np.allclose(kd, -dt * slope, rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize("rs", ["HLL", "HLLC"])
+def test_periodic_totals_are_conserved(rs):
+    cfg, prim = problems.sine_wave(16, riemann_solver=rs)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    U0 = o.conserved()
+    for i in range(4):
+        o.step(o.timestep(i))
+    U1 = o.conserved()
+    p = cfg.proper
+    for f in range(5):
+        scale = np.abs(U0[f][p]).sum() + 1.0
+        assert abs(U1[f][p].sum() - U0[f][p].sum()) <= 1e-13 * scale
+
+
+def test_outflow_change_equals_boundary_fluence():
+    cfg = FluidConfig(n_cells=(12, 10, 8), riemann_solver="HLLC")
+    prim = problems.random_state(cfg, seed=3)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    p = cfg.proper
+    # volume and face areas of the uniform interior cells
+    w = [problems.axis_geometry(int(cfg.n_cells[d]), 0.0, 1.0)[1][2] * 2 for d in range(3)]
+    vol = w[0] * w[1] * w[2]
+    areas = [w[1] * w[2], w[2] * w[0], w[0] * w[1]]
+    U0 = o.conserved()
+    fl = o.new_fluence()
+    o.step(o.timestep(5), fl)
+    U1 = o.conserved()
+    for f in range(5):
+        dq = (U1[f][p].sum() - U0[f][p].sum()) * vol
+        net = sum(areas[d] * (fl[f, 2 * d].sum() - fl[f, 2 * d + 1].sum()) for d in range(3))
+        assert dq == pytest.approx(net, rel=1e-9, abs=1e-12)
+
+
+def test_sod_keeps_transverse_symmetry():
+    cfg, prim = problems.sod(16)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    for i in range(3):
+        o.step(o.timestep(i))
+    U = o.conserved()[(slice(None),) + cfg.proper]
+    assert np.array_equal(U[0], U[0][:, ::-1, :])
+    assert np.array_equal(U[0], U[0][::-1, :, :])
+    assert np.all(U[2] == 0.0) and np.all(U[3] == 0.0)
+
+
+def _exact_sod_density(x, t, gamma=1.4):
+    """Exact solution of the Sod problem (Toro, ch. 4) at x (diaphragm 0.5)."""
+    rl, pl, rr, pr = 1.0, 1.0, 0.125, 0.1
+    cl, cr = math.sqrt(gamma * pl / rl), math.sqrt(gamma * pr / rr)
+
+    def f(p, rk, pk, ck):
+        if p > pk:
+            A, B = 2 / ((gamma + 1) * rk), (gamma - 1) / (gamma + 1) * pk
+            return (p - pk) * math.sqrt(A / (p + B))
+        return 2 * ck / (gamma - 1) * ((p / pk) ** ((gamma - 1) / (2 * gamma)) - 1)
+
+    lo, hi = 1e-6, 10.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(mid, rl, pl, cl) + f(mid, rr, pr, cr) > 0:
+            hi = mid
+        else:
+            lo = mid
+    ps = 0.5 * (lo + hi)
+    us = 0.5 * (f(ps, rr, pr, cr) - f(ps, rl, pl, cl))
+    rsl = rl * (ps / pl) ** (1 / gamma)
+    rsr = rr * ((ps / pr + (gamma - 1) / (gamma + 1)) / ((gamma - 1) / (gamma + 1) * ps / pr + 1))
+    shock = us * 0 + math.sqrt(gamma * pr / rr) * math.sqrt((gamma + 1) / (2 * gamma) * ps / pr
+                                                             + (gamma - 1) / (2 * gamma))
+    csl = cl * (ps / pl) ** ((gamma - 1) / (2 * gamma))
+    out = np.empty_like(x)
+    for i, xi in enumerate(x):
+        s = (xi - 0.5) / t
+        if s < -cl:
+            out[i] = rl
+        elif s < us - csl:
+            u = 2 / (gamma + 1) * (cl + s)
+            c = cl - (gamma - 1) / 2 * u
+            out[i] = rl * (c / cl) ** (2 / (gamma - 1))
+        elif s < us:
+            out[i] = rsl
+        elif s < shock:
+            out[i] = rsr
+        else:
+            out[i] = rr
+    return out
+
+
+def test_sod_tracks_the_exact_riemann_solution():
+    n = 96
+    cfg = FluidConfig(n_cells=(n, 4, 4), riemann_solver="HLL", courant_factor=0.8,
+                      n_ramp_cycles=1)
+    prim = problems.riemann(cfg, 1.0, 1.0, (0, 0, 0), 0.125, 0.1, (0, 0, 0), (0.5, 0, 0),
+                            (1.0, 0, 0))
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    t, i = 0.0, 0
+    while t < 0.15 - 1e-14:
+        dt = min(o.timestep(i), 0.15 - t)
+        o.step(dt)
+        t += dt
+        i += 1
+    x = problems.axis_geometry(n, 0.0, 1.0)[0][2:-2]
+    rho = o.conserved()[0][cfg.proper][2, 2, :]
+    err = np.abs(rho - _exact_sod_density(x, t)).mean()
+    assert err < 0.02
+
+
+def compact_flags(P, V, n):
+    """DIFFUSIVE_FLUX_I bits from the proper cells only, as the CUDA kernels
+    compute them (valid for a single brick, see FluidFeatures_P__Kernel.f90)."""
+    nz, ny, nx = n
+    shock = np.zeros((3, nz, ny, nx), dtype=bool)
+    for e in range(3):
+        ax = 2 - e
+        Pm = np.roll(P, 1, axis=ax)
+        Vm = np.roll(V[e], 1, axis=ax)
+        dP = np.abs(P - Pm)
+        pmin = np.maximum(np.minimum(P, Pm), math.sqrt(np.finfo(float).tiny))
+        s = (dP / pmin > 0.1) & (V[e] - Vm <= 0.0)
+        idx = [slice(None)] * 3
+        idx[ax] = 0
+        s[tuple(idx)] = False
+        shock[e] = s
+    flags = np.zeros((3, nz, ny, nx), dtype=bool)
+    for d in range(3):
+        for e in range(3):
+            if e == d:
+                continue
+            s = shock[e]
+            ae, ad = 2 - e, 2 - d
+            acc = s | np.roll(s, -1, axis=ae) | np.roll(s, 1, axis=ad) | np.roll(
+                np.roll(s, -1, axis=ae), 1, axis=ad)
+            flags[d] |= acc
+    interior = np.zeros((nz, ny, nx), dtype=bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    return flags & interior[None]
+
+
+@pytest.mark.parametrize("bc", ["OUTFLOW", "PERIODIC", "REFLECTING"])
+def test_feature_flags_depend_on_proper_cells_only(bc):
+    cfg = FluidConfig(n_cells=(14, 11, 9), boundary=((bc, bc),) * 3)
+    o = Oracle(cfg)
+    o.set_primitive(problems.random_state(cfg, seed=7))
+    o.step(o.timestep(3))
+    feat = o.features()
+    aux = o.aux()
+    prim = o.primitive()
+    p = cfg.proper
+    P = aux[0][p]
+    V = [prim[1 + d][p] for d in range(3)]
+    mine = compact_flags(P, V, P.shape)
+    ref = np.stack([feat[d][p] > 0 for d in range(3)])
+    assert ref.any()
+    assert np.array_equal(mine, ref)
+    # the outer face of each direction (a ghost index) never carries a flag
+    g = cfg.n_ghost_layers
+    for d in range(3):
+        idx = list(cfg.proper)
+        idx[2 - d] = g + int(cfg.n_cells[d])
+        assert not feat[d][tuple(idx)].any()
+
+
+@pytest.mark.parametrize("bc", ["OUTFLOW", "REFLECTING"])
+def test_proper_results_do_not_depend_on_physical_ghosts(bc):
+    cfg = FluidConfig(n_cells=(10, 9, 8), boundary=((bc, bc),) * 3, riemann_solver="HLLC")
+    prim = problems.random_state(cfg, seed=11)
+    a, b = Oracle(cfg), Oracle(cfg)
+    a.set_primitive(prim)
+    U = a.conserved()
+    U2 = U.copy()
+    ghost = np.ones(cfg.shape, dtype=bool)
+    ghost[cfg.proper] = False
+    rng = np.random.default_rng(0)
+    U2[0][ghost] *= 1.0 + 0.5 * rng.uniform(size=ghost.sum())
+    U2[4][ghost] *= 1.0 + 0.5 * rng.uniform(size=ghost.sum())
+    a.set_conserved(U)
+    b.set_conserved(U2)
+    for i in range(2):
+        dt = a.timestep(i)
+        assert dt == b.timestep(i)
+        a.step(dt)
+        b.step(dt)
+    p = (slice(None),) + cfg.proper
+    assert np.array_equal(a.conserved()[p], b.conserved()[p])
+
+
+def test_conserved_entropy_input_is_dead():
+    # UseEntropy = .false.: ComputeFromConserved rewrites DS = N SB, so the
+    # incoming DS (and its increment) never reach the next state.
+    cfg = FluidConfig(n_cells=(9, 8, 7), riemann_solver="HLLC")
+    o1, o2 = Oracle(cfg), Oracle(cfg)
+    o1.set_primitive(problems.random_state(cfg, seed=5))
+    U = o1.conserved()
+    U2 = U.copy()
+    U2[5] = np.random.default_rng(1).normal(size=U2[5].shape)
+    o1.set_conserved(U)
+    o2.set_conserved(U2)
+    o1.step(1e-3)
+    o2.step(1e-3)
+    assert np.array_equal(o1.conserved(), o2.conserved())
+
+
+def test_time_step_ramp():
+    cfg, prim = problems.sod(8, n_ramp_cycles=10)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    full = o.timestep(50)
+    assert o.timestep(0) == pytest.approx(0.1 * full, rel=1e-15)
+    assert o.timestep(4) == pytest.approx(0.5 * full, rel=1e-15)
+    tsi = o.inverse_timestep()
+    assert full == cfg.courant_factor * (1.0 / tsi)
