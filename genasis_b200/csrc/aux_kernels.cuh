@@ -229,9 +229,7 @@ __global__ void detect_flags_kernel(Box b, const uint8_t* __restrict__ sb,
 // (ComputeTimeStepKernel_CSL, Integrator_C_PS__Kernel.f90:97-142).
 __global__ void inverse_timestep_kernel(Box b, Phys ph, const double* __restrict__ U,
                                         const double* __restrict__ Pst,
-                                        const double* __restrict__ W0,
-                                        const double* __restrict__ W1,
-                                        const double* __restrict__ W2,
+                                        AxisGeo G0, AxisGeo G1, AxisGeo G2,
                                         unsigned long long* __restrict__ tsi_bits) {
   __shared__ double s_red[32];
   const long long nP = b.nP;
@@ -255,7 +253,8 @@ __global__ void inverse_timestep_kernel(Box b, Phys ph, const double* __restrict
     }
     double P, CS;
     eos_cell(w.N, w.E, ph, P, CS, nullptr);
-    m = fmax2(m, inverse_cfl_time(w, CS, W0[i + 2], W1[j + 2], W2[k + 2]));
+    m = fmax2(m, inverse_cfl_time(w, CS, G0.W[i + 2], G1.W[j + 2], G2.W[k + 2], G0.RW[i + 2],
+                                  G1.RW[j + 2], G2.RW[k + 2]));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax2(m, __shfl_xor_sync(0xffffffffu, m, o));

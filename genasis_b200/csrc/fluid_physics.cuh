@@ -45,24 +45,93 @@ __device__ __forceinline__ double fmin3(double a, double b, double c) {
   return r;
 }
 
+// Correctly rounded a / b from r = RN(1 / b), by two Markstein corrections
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990): the first correction
+// makes the quotient faithful, the second rounds it correctly, each remainder
+// a - b q being exact through the fused multiply-add as long as nothing
+// underflows or overflows.  markstein() is that straight-line sequence;
+// quotient_in_range() tells whether a and the first approximation a r lie in
+// the exponent range where it is exact (zero included, whose sign may come out
+// flipped: no branch of the step distinguishes the zeros).  Callers evaluate a
+// group of independent quotients branch-free and redo the group with the IEEE
+// division in the rare case that one of them is out of range.
+__device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
+
+__device__ __forceinline__ double markstein(double a, double b, double r) {
+  const double q0 = a * r;
+  const double e0 = __fma_rn(-b, q0, a);
+  const double q1 = __fma_rn(e0, r, q0);
+  const double e1 = __fma_rn(-b, q1, a);
+  return __fma_rn(e1, r, q1);
+}
+
+// |x| == 0 or 2^-900 <= |x| < 2^1001, from the exponent bits (integer pipe).
+__device__ __forceinline__ bool exp_in_range(double x) {
+  const unsigned hi = (unsigned)__double2hiint(x) & 0x7fffffffu;
+  const unsigned e = hi >> 20;
+  return (e - 123u) < 1901u || (hi | (unsigned)__double2loint(x)) == 0u;
+}
+
+__device__ __forceinline__ bool quotient_in_range(double a, double r) {
+  return exp_in_range(a) & exp_in_range(a * r);
+}
+
+__device__ __forceinline__ double div_rn(double a, double b, double r) {
+  const double q = markstein(a, b, r);
+  return quotient_in_range(a, r) ? q : div_ieee(a, b);
+}
+
+// The limiter exactly as Gradient_Kernel.f90:176-180 writes it, with IEEE
+// divisions: the slow path of limited_slope.
+__device__ __noinline__ double limited_slope_ieee(double dvl, double dvr, double dxl, double dxr,
+                                                  double sql, double sqr, double cden,
+                                                  double theta) {
+  const double central = (sqr * dvl + sql * dvr) / cden;
+  const double s = copysign(0.5, dvl) + copysign(0.5, dvr);
+  return s * fmin3(fabs(theta * dvl / dxl), fabs(theta * dvr / dxr), fabs(central));
+}
+
 // Generalized-minmod limited slope of one cell, Gradient_Kernel.f90:166-190.
 // vm, v0, vp: values at i-1, i, i+1; dxl = X(i) - X(i-1), dxr = X(i+1) - X(i);
-// sql = dxl*dxl, sqr = dxr*dxr, cden = (dxl*dxr)*(dxl+dxr) come from the
-// per-axis geometry tables (same operations, evaluated once on the host).
-// When the two one-sided differences have opposite signs the reference's
-// factor (sign(1/2,dV_L) + sign(1/2,dV_R)) is exactly +0, and so is the slope:
-// the three quotients are then skipped.
+// sql = dxl*dxl, sqr = dxr*dxr, cden = (dxl*dxr)*(dxl+dxr) and the rounded
+// reciprocals come from the per-axis geometry tables (same operations,
+// evaluated once on the host).
+//   slope = (sign(1/2, dV_L) + sign(1/2, dV_R))
+//           * min(|theta dV_L / dX_L|, |theta dV_R / dX_R|, |num / cden|)
+// The correctly rounded quotients are monotone in the exact ones, so the
+// minimum is the rounded quotient of the smallest exact one: approximate
+// quotients (within 2^-52 relative) pick it, and only that one is divided
+// exactly.  When two non-zero candidates are too close to separate, or a
+// quotient is outside the Markstein range, the whole slope is redone the
+// reference's way.
+// When the signs differ the factor is +0 and so is the slope.
 __device__ __forceinline__ double limited_slope(double vm, double v0, double vp, double dxl,
                                                 double dxr, double sql, double sqr,
-                                                double cden, double theta, int use_limiter) {
+                                                double cden, double rdxl, double rdxr,
+                                                double rcden, double theta, int use_limiter) {
   const double dvl = v0 - vm;
   const double dvr = vp - v0;
-  if (!use_limiter) return (sqr * dvl + sql * dvr) / cden;
+  const double num = sqr * dvl + sql * dvr;
+  if (!use_limiter) return div_rn(num, cden, rcden);
   const double s = copysign(0.5, dvl) + copysign(0.5, dvr);
+  const double a1 = fabs(theta * dvl), a2 = fabs(theta * dvr), a3 = fabs(num);
+  const double t1 = a1 * rdxl, t2 = a2 * rdxr, t3 = a3 * rcden;
+  // branch-free argmin of the approximations and the runner-up
+  const bool p12 = t1 <= t2;
+  double tm = p12 ? t1 : t2, tr = p12 ? t2 : t1;
+  double am = p12 ? a1 : a2, bm = p12 ? dxl : dxr, rm = p12 ? rdxl : rdxr;
+  const bool p3 = t3 < tm;
+  tr = p3 ? tm : fmin(tr, t3);
+  tm = p3 ? t3 : tm;
+  am = p3 ? a3 : am;
+  bm = p3 ? cden : bm;
+  rm = p3 ? rcden : rm;
+  const double q = markstein(am, bm, rm);
+  // a zero candidate is the minimum whatever the ties
+  const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && quotient_in_range(am, rm);
   if (s == 0.0) return 0.0;
-  const double central = (sqr * dvl + sql * dvr) / cden;
-  const double m = fmin3(fabs(theta * dvl / dxl), fabs(theta * dvr / dxr), fabs(central));
-  return s * m;
+  return fast ? s * q : limited_slope_ieee(dvl, dvr, dxl, dxr, sql, sqr, cden, theta);
 }
 
 // State at one face after ComputeFromPrimitiveCommon (Fluid_P_I__Form.f90:509-601):
@@ -181,9 +250,20 @@ __device__ __forceinline__ void riemann_flux(const FaceState& L, const FaceState
   const double UL[6] = {L.D, L.S1, L.S2, L.S3, L.G, L.DS};
   const double UR[6] = {R.D, R.S1, R.S2, R.S3, R.G, R.DS};
   const double den = fmax2(AP + AM, kTiny);
+  const double rden = 1.0 / den;
   const double apam = AP * AM;
+  double num[NF];
+  bool ok = true;
 #pragma unroll
-  for (int u = 0; u < NF; ++u) F[u] = (AP * FL[u] + AM * FR[u] - apam * (UR[u] - UL[u])) / den;
+  for (int u = 0; u < NF; ++u) {
+    num[u] = AP * FL[u] + AM * FR[u] - apam * (UR[u] - UL[u]);
+    F[u] = markstein(num[u], den, rden);
+    ok &= quotient_in_range(num[u], rden);
+  }
+  if (!ok) {
+#pragma unroll
+    for (int u = 0; u < NF; ++u) F[u] = div_ieee(num[u], den);
+  }
 }
 
 // Compute_N_V_E_G_Kernel (Fluid_P__Kernel.f90:94-192, both loops): the floored
@@ -198,9 +278,16 @@ struct Cons {
 __device__ __forceinline__ void cons_to_prim(Cons& u, Prim& w, double nmin) {
   if (u.D > nmin) {
     w.N = u.D;
-    w.V1 = u.S1 / u.D;
-    w.V2 = u.S2 / u.D;
-    w.V3 = u.S3 / u.D;
+    const double rd = 1.0 / u.D;
+    w.V1 = markstein(u.S1, u.D, rd);
+    w.V2 = markstein(u.S2, u.D, rd);
+    w.V3 = markstein(u.S3, u.D, rd);
+    if (!(quotient_in_range(u.S1, rd) & quotient_in_range(u.S2, rd) &
+          quotient_in_range(u.S3, rd))) {
+      w.V1 = div_ieee(u.S1, u.D);
+      w.V2 = div_ieee(u.S2, u.D);
+      w.V3 = div_ieee(u.S3, u.D);
+    }
     w.E = u.G - 0.5 * (u.S1 * w.V1 + u.S2 * w.V2 + u.S3 * w.V3);
   } else {
     w.N = nmin;
@@ -253,9 +340,11 @@ __device__ __forceinline__ void eos_cell(double N, double E, const Phys& ph, dou
 // Inverse CFL time of one cell, Integrator_C_PS__Kernel.f90:122-137
 // (coarsening factors are 1 on this chart).
 __device__ __forceinline__ double inverse_cfl_time(const Prim& w, double CS, double w0,
-                                                   double w1, double w2) {
-  return fmax2(w.V1 + CS, -(w.V1 - CS)) / w0 + fmax2(w.V2 + CS, -(w.V2 - CS)) / w1 +
-         fmax2(w.V3 + CS, -(w.V3 - CS)) / w2;
+                                                   double w1, double w2, double r0, double r1,
+                                                   double r2) {
+  return div_rn(fmax2(w.V1 + CS, -(w.V1 - CS)), w0, r0) +
+         div_rn(fmax2(w.V2 + CS, -(w.V2 - CS)), w1, r1) +
+         div_rn(fmax2(w.V3 + CS, -(w.V3 - CS)), w2, r2);
 }
 
 // Total order of doubles as unsigned integers, for atomicMax reductions.

@@ -49,7 +49,7 @@ int fail(int code, const char* fmt, ...) {
 // (half widths); GeometryFlat_Kernel.f90:22-24 (widths); Difference_Kernel on
 // the centres; the limiter's denominators of Gradient_Kernel.f90:176-180.
 struct HostAxis {
-  std::vector<double> X, WL, WR, W, dXI, SQ, CDEN;
+  std::vector<double> X, WL, WR, W, dXI, SQ, CDEN, RDXI, RCDEN, RW;
 };
 
 HostAxis build_axis(int n, double mn, double mx, int g) {
@@ -86,6 +86,13 @@ HostAxis build_axis(int n, double mn, double mx, int g) {
   }
   for (int t = 1; t + 1 < m; ++t)
     a.CDEN[t] = a.dXI[t] * a.dXI[t + 1] * (a.dXI[t] + a.dXI[t + 1]);
+  // correctly rounded reciprocals for the exact divisions of the kernels
+  a.RDXI.assign(m + 1, 0.0);
+  a.RCDEN.assign(m + 1, 0.0);
+  a.RW.assign(m + 1, 0.0);
+  for (int t = 1; t < m; ++t) a.RDXI[t] = 1.0 / a.dXI[t];
+  for (int t = 1; t + 1 < m; ++t) a.RCDEN[t] = 1.0 / a.CDEN[t];
+  for (int t = 0; t < m; ++t) a.RW[t] = 1.0 / a.W[t];
   return a;
 }
 
@@ -142,17 +149,23 @@ namespace {
 template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF>
 cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
                            int n_items, int* counter, const Phys& ph, cudaStream_t s) {
-  using SM = StageSmem<MODE, IN_PRIM, HLLC, GRAV, NF>;
+  using SM = StageLayout<NF>;
+  (void)many;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
+  static int per_sm = 1;
   auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF>;
   std::call_once(once, [&] {
     attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)SM::kBytes);
+    if (attr_err == cudaSuccess)
+      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, SM::kBytes);
+    if (per_sm < 1) per_sm = 1;
   });
   if (attr_err != cudaSuccess) return attr_err;
-  const int grid = std::max(1, std::min(n_items, num_sms()));
-  kern<<<grid, NT, SM::kBytes, s>>>(d, many, items, n_items, counter, ph);
+  // persistent grid: every resident CTA slot pulls work items
+  const int grid = std::max(1, std::min(n_items, num_sms() * per_sm));
+  kern<<<grid, NT, SM::kBytes, s>>>(d, items, n_items, counter, ph);
   return cudaGetLastError();
 }
 
@@ -219,7 +232,7 @@ int validate(const gfx_fluid_config* c) {
 std::vector<WorkItem> make_items(const int n[3], int brick) {
   const int cx = (n[0] + TX - 1) / TX, cy = (n[1] + TY - 1) / TY;
   const long long cols = (long long)cx * cy;
-  const long long want = 8LL * num_sms();
+  const long long want = 16LL * num_sms();
   int chunks = (int)std::max(1LL, std::min<long long>(n[2] / 16, (want + cols - 1) / cols));
   if (chunks < 1) chunks = 1;
   const int len = (n[2] + chunks - 1) / chunks;
@@ -387,7 +400,7 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
   };
   // geometry arena: 6 tables per axis, each m + 1 long
   size_t geo_len = 0;
-  for (int d = 0; d < 3; ++d) geo_len += 6 * (size_t)(b.m[d] + 1);
+  for (int d = 0; d < 3; ++d) geo_len += 9 * (size_t)(b.m[d] + 1);
   if (cudaMalloc(&h->geo, geo_len * sizeof(double)) != cudaSuccess)
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc geometry"));
   {
@@ -396,11 +409,14 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
     for (int d = 0; d < 3; ++d) {
       const HostAxis& a = h->axis[d];
       const int L = b.m[d] + 1;
-      const std::vector<double>* tabs[6] = {&a.W, &a.WL, &a.WR, &a.dXI, &a.SQ, &a.CDEN};
-      const double** dst[6] = {&h->dgeo[d].W, &h->dgeo[d].WL, &h->dgeo[d].WR,
-                               &h->dgeo[d].dXI, &h->dgeo[d].SQ, &h->dgeo[d].CDEN};
-      for (int q = 0; q < 6; ++q) {
+      const std::vector<double>* tabs[9] = {&a.W,   &a.WL,   &a.WR,    &a.dXI, &a.SQ,
+                                            &a.CDEN, &a.RDXI, &a.RCDEN, &a.RW};
+      const double** dst[9] = {&h->dgeo[d].W,    &h->dgeo[d].WL,   &h->dgeo[d].WR,
+                               &h->dgeo[d].dXI,  &h->dgeo[d].SQ,   &h->dgeo[d].CDEN,
+                               &h->dgeo[d].RDXI, &h->dgeo[d].RCDEN, &h->dgeo[d].RW};
+      for (int q = 0; q < 9; ++q) {
         std::copy(tabs[q]->begin(), tabs[q]->end(), host.begin() + off);
+        // tables are m long except the difference-based ones (m + 1)
         *dst[q] = h->geo + off;
         off += L;
       }
@@ -591,8 +607,8 @@ int gfx_fluid_timestep(gfx_fluid* h, const double* U, int i_cycle, double* dt_ho
   reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 0);
   CUDA_TRY(cudaGetLastError());
   inverse_timestep_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(
-      h->box, h->ph, U, h->prims_pending ? h->Pst : nullptr, h->dgeo[0].W, h->dgeo[1].W,
-      h->dgeo[2].W, h->tsi_bits);
+      h->box, h->ph, U, h->prims_pending ? h->Pst : nullptr, h->dgeo[0], h->dgeo[1],
+      h->dgeo[2], h->tsi_bits);
   CUDA_TRY(cudaGetLastError());
   Clock c;
   memset(&c, 0, sizeof(c));
@@ -629,8 +645,8 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
     // initial dt from the state (ComputeNewTime before the first cycle)
     reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 0);
     inverse_timestep_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(
-        h->box, h->ph, U, h->prims_pending ? h->Pst : nullptr, h->dgeo[0].W, h->dgeo[1].W,
-        h->dgeo[2].W, h->tsi_bits);
+        h->box, h->ph, U, h->prims_pending ? h->Pst : nullptr, h->dgeo[0], h->dgeo[1],
+        h->dgeo[2], h->tsi_bits);
     finalize_dt_kernel<<<1, 1, 0, s>>>(h->ph, h->tsi_bits, dc, 1, 1);
     CUDA_TRY(cudaGetLastError());
     h->launches += 3;

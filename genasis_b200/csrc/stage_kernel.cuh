@@ -32,12 +32,15 @@ enum { BC_OUTFLOW = 0, BC_REFLECTING = 1, BC_PERIODIC = 2 };
 
 // Per-axis tables over the ghost-inclusive index t in [0, n + 4) (t = cell + 2).
 struct AxisGeo {
-  const double* W;     // cell width WL + WR (GeometryFlat_Kernel.f90:22-24)
-  const double* WL;    // centre - inner edge
-  const double* WR;    // outer edge - centre
-  const double* dXI;   // X(t) - X(t-1), Difference_Kernel.f90 on the centres
-  const double* SQ;    // dXI(t)^2
-  const double* CDEN;  // (dXI(t) dXI(t+1)) (dXI(t) + dXI(t+1))
+  const double* W;      // cell width WL + WR (GeometryFlat_Kernel.f90:22-24)
+  const double* WL;     // centre - inner edge
+  const double* WR;     // outer edge - centre
+  const double* dXI;    // X(t) - X(t-1), Difference_Kernel.f90 on the centres
+  const double* SQ;     // dXI(t)^2
+  const double* CDEN;   // (dXI(t) dXI(t+1)) (dXI(t) + dXI(t+1))
+  const double* RDXI;   // RN(1 / dXI(t))
+  const double* RCDEN;  // RN(1 / CDEN(t))
+  const double* RW;     // RN(1 / W(t))
 };
 
 struct BrickDesc {
@@ -87,19 +90,6 @@ __device__ __forceinline__ int bc_map(int g, int n, int bc_lo, int bc_hi, bool& 
   return max(0, min(n - 1, s));
 }
 
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF>
-struct StageSmem {
-  static constexpr int kRing = 3 * 5 * PS;
-  static constexpr int kSzc = 2 * 5 * NT;
-  static constexpr int kFzc = 2 * NF * NT;
-  static constexpr int kSx = 5 * TY * (TX + 2);
-  static constexpr int kSy = 5 * (TY + 2) * TX;
-  static constexpr int kFx = NF * TY * (TX + 1);
-  static constexpr int kFy = NF * (TY + 1) * TX;
-  static constexpr int kDoubles = kRing + kSzc + kFzc + kSx + kSy + kFx + kFy;
-  static constexpr size_t kBytes = sizeof(double) * kDoubles;
-};
-
 // Loads the primitives of cell (gx, gy) of plane gz (all possibly ghosts) into
 // a ring plane at local (ly, lx).
 template <bool IN_PRIM>
@@ -141,6 +131,45 @@ __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, do
   plane[4 * PS + o] = w.E;
 }
 
+// Loads the primitives of one cell into a column slot (5 values at stride NT).
+template <bool IN_PRIM>
+__device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph, double* dst,
+                                              int gx, int gy, int gz) {
+  bool nx, ny, nz;
+  const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
+  const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
+  const int sz = bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
+  Prim w;
+  if (IN_PRIM) {
+    const long long o = sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz);
+    const double* p = B.P_in;
+    w.N = __ldg(p + o);
+    w.V1 = __ldg(p + B.nP + o);
+    w.V2 = __ldg(p + 2 * B.nP + o);
+    w.V3 = __ldg(p + 3 * B.nP + o);
+    w.E = __ldg(p + 4 * B.nP + o);
+  } else {
+    const long long o =
+        (sx + 2) + (long long)B.m[0] * ((sy + 2) + (long long)B.m[1] * (sz + 2));
+    const double* u = B.U_in;
+    Cons c;
+    c.D = __ldg(u + o);
+    c.S1 = __ldg(u + B.nV + o);
+    c.S2 = __ldg(u + 2 * B.nV + o);
+    c.S3 = __ldg(u + 3 * B.nV + o);
+    c.G = __ldg(u + 4 * B.nV + o);
+    cons_to_prim(c, w, ph.nmin);
+  }
+  if (nx) w.V1 = -w.V1;
+  if (ny) w.V2 = -w.V2;
+  if (nz) w.V3 = -w.V3;
+  dst[0] = w.N;
+  dst[NT] = w.V1;
+  dst[2 * NT] = w.V2;
+  dst[3 * NT] = w.V3;
+  dst[4 * NT] = w.E;
+}
+
 // Reconstructed face states of the face between cells (im) and (ip) along one
 // axis, IncrementDivergence_FV__Kernel.f90:70-90: V_IL = V(i-1) + dXR(i-1) dVdX(i-1),
 // V_IR = V(i) - dXL(i) dVdX(i).
@@ -177,236 +206,365 @@ __device__ __forceinline__ void record_fluence(const BrickDesc& B, int face, int
   }
 }
 
+// Boundary fluence of one face.  The stages evolve five fields (the DS
+// increment is dead: ComputeFromConserved rewrites DS = N SB), but the
+// reference records all six fluxes on the boundary faces, so the six-field
+// flux is formed there from the same reconstructed primitives.  Kept out of
+// line: it runs on boundary faces only.
+struct FacePrims {
+  double l[5], r[5];
+};
+
+template <int D, bool HLLC>
+__device__ __noinline__ void boundary_fluence6(const BrickDesc& B, const Phys& ph, FacePrims p,
+                                               bool diffusive, int face, int a, int na, int b,
+                                               double factor) {
+  FaceState L, R;
+  face_state<6>(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], ph, L);
+  face_state<6>(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], ph, R);
+  double F6[6];
+  riemann_flux<D, HLLC, 6>(L, R, diffusive, F6);
+  record_fluence<6>(B, face, a, na, b, F6, factor);
+}
+
+template <int D, bool HLLC, int NF>
+__device__ __forceinline__ void boundary_fluence(const BrickDesc& B, const Phys& ph,
+                                                 const double* l, const double* r,
+                                                 bool diffusive, const double* F, int face,
+                                                 int a, int na, int b, double factor) {
+  if (NF == 6) {
+    record_fluence<6>(B, face, a, na, b, F, factor);
+    return;
+  }
+  FacePrims p;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    p.l[v] = l[v];
+    p.r[v] = r[v];
+  }
+  boundary_fluence6<D, HLLC>(B, ph, p, diffusive, face, a, na, b, factor);
+}
+
+// Relabels the velocity and momentum components of a face state so that
+// direction d comes first (d = 1: swap 1 and 2).  The sums that depend on the
+// component order (G) are formed before, in the reference's frame; the flux
+// formulas treat every component alike, so the relabelled solve is exact.
+__device__ __forceinline__ void to_normal_frame_y(FaceState& s) {
+  const double v = s.V1, m = s.S1;
+  s.V1 = s.V2;
+  s.S1 = s.S2;
+  s.V2 = v;
+  s.S2 = m;
+}
+
+// The reconstructed primitives of a face, IncrementDivergence_FV__Kernel.f90:
+// 70-90: V_IL = V(i-1) + dXR(i-1) dVdX(i-1), V_IR = V(i) - dXL(i) dVdX(i).
+__device__ __forceinline__ void face_prims(const double* vm, const double* sm_, int stride_m,
+                                           const double* vp, const double* sp, int stride_p,
+                                           int sstride_m, int sstride_p, double wr, double wl,
+                                           double* l, double* r) {
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    l[v] = vm[v * stride_m] + wr * sm_[v * sstride_m];
+    r[v] = vp[v * stride_p] - wl * sp[v * sstride_p];
+  }
+}
+
+// Per-tile copy of the geometry tables of one axis, entries t0 .. t0 + L - 1.
+enum { G_W, G_WL, G_WR, G_DXI, G_SQ, G_CDEN, G_RDXI, G_RCDEN, G_RW, G_NTAB };
+
+__device__ __forceinline__ void fill_geo(const AxisGeo& G, int m, int t0, int L, double* dst,
+                                         int tid) {
+  const double* tabs[G_NTAB] = {G.W, G.WL, G.WR, G.dXI, G.SQ, G.CDEN, G.RDXI, G.RCDEN, G.RW};
+  for (int i = tid; i < G_NTAB * L; i += NT) {
+    const int q = i / L, j = i % L, t = t0 + j;
+    dst[i] = (t >= 0 && t <= m) ? __ldg(tabs[q] + t) : 0.0;
+  }
+}
+
+template <int NF>
+struct StageLayout {
+  static constexpr int kFull = 5 * PS;            // plane k with its x / y halo
+  static constexpr int kCen = 2 * 5 * NT;         // centres of planes k+1, k+2
+  static constexpr int kZs = 5 * NT;              // z slope of plane k (own column)
+  static constexpr int kZf = NF * NT;             // z flux of face k (own column)
+  static constexpr int kSx = 5 * TY * (TX + 2);
+  static constexpr int kSy = 5 * (TY + 2) * TX;
+  static constexpr int kFx = NF * TY * (TX + 1);
+  static constexpr int kFy = NF * (TY + 1) * TX;
+  static constexpr int kGx = G_NTAB * (TX + 4);
+  static constexpr int kGy = G_NTAB * (TY + 4);
+  static constexpr int kDoubles = kFull + kCen + kZs + kZf + kSx + kSy + kFx + kFy + kGx + kGy;
+  static constexpr size_t kBytes = sizeof(double) * kDoubles;
+};
+
+// Limited slopes of the 5 primitives of one cell; v points at the cell in a
+// buffer with variable stride vs and neighbour stride st; g is a per-tile
+// geometry cache (entry c = the cell's own index).
+__device__ __forceinline__ void cell_slopes(const double* v, int vs, int st, const double* g,
+                                            int L, int c, const Phys& ph, double* out,
+                                            int ostride) {
+  const double dxl = g[G_DXI * L + c], dxr = g[G_DXI * L + c + 1];
+  const double sql = g[G_SQ * L + c], sqr = g[G_SQ * L + c + 1], cden = g[G_CDEN * L + c];
+  const double rdxl = g[G_RDXI * L + c], rdxr = g[G_RDXI * L + c + 1],
+               rcden = g[G_RCDEN * L + c];
+#pragma unroll
+  for (int q = 0; q < 5; ++q)
+    out[q * ostride] = limited_slope(v[q * vs - st], v[q * vs], v[q * vs + st], dxl, dxr, sql,
+                                     sqr, cden, rdxl, rdxr, rcden, ph.theta, ph.use_limiter);
+}
+
 template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF>
-__global__ void __launch_bounds__(NT, 1)
-    stage_kernel(const __grid_constant__ BrickDesc single, const BrickDesc* __restrict__ many,
-                 const WorkItem* __restrict__ items, int n_items, int* __restrict__ counter,
-                 const __grid_constant__ Phys ph) {
-  using SM = StageSmem<MODE, IN_PRIM, HLLC, GRAV, NF>;
+__global__ void __launch_bounds__(NT, 2)
+    stage_kernel(const __grid_constant__ BrickDesc B, const WorkItem* __restrict__ items,
+                 int n_items, int* __restrict__ counter, const __grid_constant__ Phys ph) {
+  using SL = StageLayout<NF>;
   extern __shared__ double smem[];
-  double* ring = smem;
-  double* szc = ring + SM::kRing;
-  double* fzc = szc + SM::kSzc;
-  double* sxs = fzc + SM::kFzc;
-  double* sys = sxs + SM::kSx;
-  double* fxs = sys + SM::kSy;
-  double* fys = fxs + SM::kFx;
+  double* full = smem;
+  double* cen = full + SL::kFull;
+  double* zss = cen + SL::kCen;
+  double* zfs = zss + SL::kZs;
+  double* sxs = zfs + SL::kZf;
+  double* sys = sxs + SL::kSx;
+  double* fxs = sys + SL::kSy;
+  double* fys = fxs + SL::kFx;
+  double* gxc = fys + SL::kFy;
+  double* gyc = gxc + SL::kGx;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
+  constexpr int LX = TX + 4, LY = TY + 4;
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
+  const int c_off = (ty + 2) * PW + (tx + 2);  // own cell in the full plane
+  const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+  const AxisGeo& GZ = B.geo[2];
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(counter, 1);
     __syncthreads();
     const int it = s_item;
     if (it >= n_items) break;
-    const WorkItem W = items[it];
-    const BrickDesc& B = many ? many[W.brick] : single;
     if (B.skip && *B.skip) {
       __syncthreads();
       continue;
     }
+    const WorkItem W = items[it];
     const double dt = *B.dt;
     const int x0 = W.x0, y0 = W.y0, z0 = W.z0, z1 = W.z1;
-    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
     const int gx = x0 + tx, gy = y0 + ty;
     const bool own = (gx < n0) && (gy < n1);
     double tsi_max = -DBL_MAX;
+    fill_geo(B.geo[0], B.m[0], x0, LX, gxc, tid);
+    fill_geo(B.geo[1], B.m[1], y0, LY, gyc, tid);
 
-    auto slot = [](int p) { return ((p % 3) + 3) % 3; };
-    auto plane_ptr = [&](int p) { return ring + slot(p) * 5 * PS; };
-    const int c_off = (ty + 2) * PW + (tx + 2);  // own cell in a plane
-
-    // z slope at plane p (p-1, p, p+1 resident) for the own column -> dst[5][NT]
-    auto z_slope = [&](int p, double* dst) {
-      const double* a = plane_ptr(p - 1);
-      const double* b = plane_ptr(p);
-      const double* c = plane_ptr(p + 1);
+    // own column helpers: a "column pointer" addresses 5 values at stride NT
+    // (centre slots) or PS (full plane)
+    auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
+    auto z_slope = [&](int p, const double* a, int sa, const double* b, int sb,
+                       const double* c, int sc, double* out) {
       const int t = p + 2;
-      const AxisGeo& G = B.geo[2];
-      const double dxl = __ldg(G.dXI + t), dxr = __ldg(G.dXI + t + 1);
-      const double sql = __ldg(G.SQ + t), sqr = __ldg(G.SQ + t + 1), cden = __ldg(G.CDEN + t);
+      const double dxl = __ldg(GZ.dXI + t), dxr = __ldg(GZ.dXI + t + 1);
+      const double sql = __ldg(GZ.SQ + t), sqr = __ldg(GZ.SQ + t + 1),
+                   cden = __ldg(GZ.CDEN + t);
+      const double rdxl = __ldg(GZ.RDXI + t), rdxr = __ldg(GZ.RDXI + t + 1),
+                   rcden = __ldg(GZ.RCDEN + t);
 #pragma unroll
-      for (int v = 0; v < 5; ++v)
-        dst[v * NT + tid] = limited_slope(a[v * PS + c_off], b[v * PS + c_off],
-                                          c[v * PS + c_off], dxl, dxr, sql, sqr, cden,
-                                          ph.theta, ph.use_limiter);
+      for (int q = 0; q < 5; ++q)
+        out[q] = limited_slope(a[q * sa], b[q * sb], c[q * sc], dxl, dxr, sql, sqr, cden, rdxl,
+                               rdxr, rcden, ph.theta, ph.use_limiter);
     };
-    // z face between planes p-1 and p for the own column -> dst[NF][NT]
-    auto z_face = [&](int p, const double* s_m, const double* s_p, double* dst) {
-      const double* a = plane_ptr(p - 1);
-      const double* b = plane_ptr(p);
-      const AxisGeo& G = B.geo[2];
+    // z face between planes p-1 (values a, slopes sm_) and p (values b, slopes sp)
+    auto z_face = [&](int p, const double* a, int sa, const double* sm_, int ssm,
+                      const double* b, int sb, const double* sp, int ssp, double* F) {
+      double l[5], r[5];
+      face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2),
+                 l, r);
       FaceState L, R;
-      face_states<NF>(a + c_off, s_m + tid, PS, b + c_off, s_p + tid, PS, NT, NT,
-                      __ldg(G.WR + p + 1), __ldg(G.WL + p + 2), ph, L, R);
-      double F[NF];
-      riemann_flux<2, HLLC, NF>(L, R, HLLC && df_bit(B, 2, gx, gy, p), F);
-#pragma unroll
-      for (int u = 0; u < NF; ++u) dst[u * NT + tid] = F[u];
-      if (own && (p == 0 || p == n2))
-        record_fluence<NF>(B, p == 0 ? 4 : 5, gx, n0, gy, F, B.weight * dt);
+      face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
+      face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
+      const bool diff = HLLC && df_bit(B, 2, gx, gy, p);
+      riemann_flux<2, HLLC, NF>(L, R, diff, F);
+      if (own && (p == 0 || p == n2) && B.fluence)
+        boundary_fluence<2, HLLC, NF>(B, ph, l, r, diff, F, p == 0 ? 4 : 5, gx, n0, gy,
+                                      B.weight * dt);
     };
 
-    // ---- prologue: planes z0-2 .. z0+1, slopes at z0-1, z0, face z0 ----
-    load_cell<IN_PRIM>(B, ph, plane_ptr(z0 - 2), tx, ty, gx, gy, z0 - 2);
-    load_cell<IN_PRIM>(B, ph, plane_ptr(z0 - 1), tx, ty, gx, gy, z0 - 1);
-    load_cell<IN_PRIM>(B, ph, plane_ptr(z0), tx, ty, gx, gy, z0);
-    __syncthreads();
-    z_slope(z0 - 1, szc);
-    __syncthreads();
-    load_cell<IN_PRIM>(B, ph, plane_ptr(z0 + 1), tx, ty, gx, gy, z0 + 1);
-    __syncthreads();
-    z_slope(z0, szc + 5 * NT);
-    __syncthreads();
-    z_face(z0, szc, szc + 5 * NT, fzc);
-    __syncthreads();
-    int scur = 1, fcur = 0;
+    // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
+    {
+      double* fc = full + c_off;
+      load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 - 2);
+      load_cell_col<IN_PRIM>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
+      load_cell_col<IN_PRIM>(B, ph, cslot(z0), gx, gy, z0);
+      double s_m[5], s_0[5];
+      z_slope(z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
+      load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 + 1);
+      z_slope(z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, s_0);
+      double F[NF];
+      z_face(z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, F);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) zss[q * NT + tid] = s_0[q];
+#pragma unroll
+      for (int u = 0; u < NF; ++u) zfs[u * NT + tid] = F[u];
+      // plane z0+1 into its centre slot (the slot of z0-1)
+      double* d = cslot(z0 + 1);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) d[q * NT] = fc[q * PS];
+    }
+    __syncthreads();  // geometry caches
 
     for (int k = z0; k < z1; ++k) {
-      double* pk = plane_ptr(k);
-      // (1) next plane centre, current plane halo
-      load_cell<IN_PRIM>(B, ph, plane_ptr(k + 2), tx, ty, gx, gy, k + 2);
+      // (1) plane k into the full buffer: own centre from its slot, the
+      // x / y halo loaded; plane k+2 into the freed slot
+      {
+        double* src = cslot(k);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) full[q * PS + c_off] = src[q * NT];
+      }
+      load_cell_col<IN_PRIM>(B, ph, cslot(k + 2), gx, gy, k + 2);
       if (tid < 4 * TX) {
         const int s = tid / TX, lx = tid % TX;
         const int ly = (s < 2) ? s - 2 : TY + s - 2;
-        load_cell<IN_PRIM>(B, ph, pk, lx, ly, x0 + lx, y0 + ly, k);
+        load_cell<IN_PRIM>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
       } else if (tid < 4 * TX + 4 * TY) {
         const int j = tid - 4 * TX;
         const int ly = j / 4, s = j % 4;
         const int lx = (s < 2) ? s - 2 : TX + s - 2;
-        load_cell<IN_PRIM>(B, ph, pk, lx, ly, x0 + lx, y0 + ly, k);
+        load_cell<IN_PRIM>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
       }
       __syncthreads();
 
-      // (2) slopes: x [TY][TX+2], y [TY+2][TX], z at k+1
+      // (2) slopes: x [TY][TX+2], y [TY+2][TX] of plane k
       {
         constexpr int NXS = TY * (TX + 2), NYS = (TY + 2) * TX;
-        constexpr int PXS = (NXS + 31) / 32 * 32, PYS = (NYS + 31) / 32 * 32;
-        constexpr int NITEMS = PXS + PYS + NT;
-        for (int i = tid; i < NITEMS; i += NT) {
+        constexpr int PXS = (NXS + 31) / 32 * 32;
+        for (int i = tid; i < PXS + NYS; i += NT) {
           if (i < PXS) {
             if (i >= NXS) continue;
             const int ly = i / (TX + 2), lx = i % (TX + 2) - 1;
-            const int cx = x0 + lx;
-            if (cx > n0 || y0 + ly >= n1) continue;
-            const AxisGeo& G = B.geo[0];
-            const int t = cx + 2;
-            const double dxl = __ldg(G.dXI + t), dxr = __ldg(G.dXI + t + 1);
-            const double sql = __ldg(G.SQ + t), sqr = __ldg(G.SQ + t + 1),
-                         cden = __ldg(G.CDEN + t);
-            const int o = (ly + 2) * PW + (lx + 2);
-#pragma unroll
-            for (int v = 0; v < 5; ++v)
-              sxs[(v * TY + ly) * (TX + 2) + lx + 1] =
-                  limited_slope(pk[v * PS + o - 1], pk[v * PS + o], pk[v * PS + o + 1], dxl,
-                                dxr, sql, sqr, cden, ph.theta, ph.use_limiter);
-          } else if (i < PXS + PYS) {
-            const int j = i - PXS;
-            if (j >= NYS) continue;
-            const int ly = j / TX - 1, lx = j % TX;
-            const int cy = y0 + ly;
-            if (cy > n1 || x0 + lx >= n0) continue;
-            const AxisGeo& G = B.geo[1];
-            const int t = cy + 2;
-            const double dxl = __ldg(G.dXI + t), dxr = __ldg(G.dXI + t + 1);
-            const double sql = __ldg(G.SQ + t), sqr = __ldg(G.SQ + t + 1),
-                         cden = __ldg(G.CDEN + t);
-            const int o = (ly + 2) * PW + (lx + 2);
-#pragma unroll
-            for (int v = 0; v < 5; ++v)
-              sys[(v * (TY + 2) + ly + 1) * TX + lx] =
-                  limited_slope(pk[v * PS + o - PW], pk[v * PS + o], pk[v * PS + o + PW], dxl,
-                                dxr, sql, sqr, cden, ph.theta, ph.use_limiter);
+            if (x0 + lx > n0 || y0 + ly >= n1) continue;
+            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, 1, gxc, LX, lx + 2, ph,
+                        sxs + ly * (TX + 2) + lx + 1, TY * (TX + 2));
           } else {
-            z_slope(k + 1, szc + (scur ^ 1) * 5 * NT);
+            const int j = i - PXS;
+            const int ly = j / TX - 1, lx = j % TX;
+            if (y0 + ly > n1 || x0 + lx >= n0) continue;
+            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, PW, gyc, LY, ly + 2, ph,
+                        sys + (ly + 1) * TX + lx, (TY + 2) * TX);
           }
         }
       }
       __syncthreads();
 
-      // (3) faces: x [TY][TX+1], y [TY+1][TX], z face k+1
+      // (3) faces: x [TY][TX+1], y [TY+1][TX] of plane k, one code path for
+      // both directions (the y states are relabelled so that y is first)
       {
         constexpr int NXF = TY * (TX + 1), NYF = (TY + 1) * TX;
-        constexpr int PXF = (NXF + 31) / 32 * 32, PYF = (NYF + 31) / 32 * 32;
-        constexpr int NITEMS = PXF + PYF + NT;
+        constexpr int PXF = (NXF + 31) / 32 * 32;
         const double factor = B.weight * dt;
-        for (int i = tid; i < NITEMS; i += NT) {
-          if (i < PXF) {
-            if (i >= NXF) continue;
-            const int ly = i / (TX + 1), lx = i % (TX + 1);
-            const int cx = x0 + lx, cy = y0 + ly;
-            if (cx > n0 || cy >= n1) continue;
-            const AxisGeo& G = B.geo[0];
-            const int o = (ly + 2) * PW + (lx + 2);
-            const double* sl = sxs + ly * (TX + 2) + lx;  // slope of cell lx-1
-            FaceState L, R;
-            face_states<NF>(pk + o - 1, sl, PS, pk + o, sl + 1, PS, TY * (TX + 2),
-                            TY * (TX + 2), __ldg(G.WR + cx + 1), __ldg(G.WL + cx + 2), ph, L,
-                            R);
-            double F[NF];
-            riemann_flux<0, HLLC, NF>(L, R, HLLC && df_bit(B, 0, cx, cy, k), F);
+        for (int i = tid; i < PXF + NYF; i += NT) {
+          const bool isx = i < PXF;
+          if (isx && i >= NXF) continue;
+          const int j = isx ? i : i - PXF;
+          const int ly = isx ? j / (TX + 1) : j / TX;
+          const int lx = isx ? j % (TX + 1) : j % TX;
+          const int cx = x0 + lx, cy = y0 + ly;
+          if (isx ? (cx > n0 || cy >= n1) : (cy > n1 || cx >= n0)) continue;
+          const int o = (ly + 2) * PW + (lx + 2);
+          const int step = isx ? 1 : PW;
+          // slope of the cell before the face, and its stride to the next cell
+          const double* sl = isx ? sxs + ly * (TX + 2) + lx : sys + ly * TX + lx;
+          const int sstep = isx ? 1 : TX;
+          const int sstride = isx ? TY * (TX + 2) : (TY + 2) * TX;
+          const double wr = isx ? gxc[G_WR * LX + lx + 1] : gyc[G_WR * LY + ly + 1];
+          const double wl = isx ? gxc[G_WL * LX + lx + 2] : gyc[G_WL * LY + ly + 2];
+          double l[5], r[5];
+          face_prims(full + o - step, sl, PS, full + o, sl + sstep, PS, sstride, sstride, wr,
+                     wl, l, r);
+          FaceState L, R;
+          face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
+          face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
+          if (!isx) {
+            to_normal_frame_y(L);
+            to_normal_frame_y(R);
+          }
+          const bool diff = HLLC && df_bit(B, isx ? 0 : 1, cx, cy, k);
+          double F[NF];
+          riemann_flux<0, HLLC, NF>(L, R, diff, F);
+          if (!isx) {
+            const double f = F[1];
+            F[1] = F[2];
+            F[2] = f;
+          }
+          double* out = isx ? fxs + ly * (TX + 1) + lx : fys + ly * TX + lx;
+          const int ostride = isx ? TY * (TX + 1) : (TY + 1) * TX;
 #pragma unroll
-            for (int u = 0; u < NF; ++u) fxs[(u * TY + ly) * (TX + 1) + lx] = F[u];
-            if (cx == 0 || cx == n0) record_fluence<NF>(B, cx == 0 ? 0 : 1, cy, n1, k, F, factor);
-          } else if (i < PXF + PYF) {
-            const int j = i - PXF;
-            if (j >= NYF) continue;
-            const int ly = j / TX, lx = j % TX;
-            const int cx = x0 + lx, cy = y0 + ly;
-            if (cy > n1 || cx >= n0) continue;
-            const AxisGeo& G = B.geo[1];
-            const int o = (ly + 2) * PW + (lx + 2);
-            const double* sl = sys + ly * TX + lx;  // slope of cell ly-1
-            FaceState L, R;
-            face_states<NF>(pk + o - PW, sl, PS, pk + o, sl + TX, PS, (TY + 2) * TX,
-                            (TY + 2) * TX, __ldg(G.WR + cy + 1), __ldg(G.WL + cy + 2), ph, L,
-                            R);
-            double F[NF];
-            riemann_flux<1, HLLC, NF>(L, R, HLLC && df_bit(B, 1, cx, cy, k), F);
-#pragma unroll
-            for (int u = 0; u < NF; ++u) fys[(u * (TY + 1) + ly) * TX + lx] = F[u];
-            if (cy == 0 || cy == n1) record_fluence<NF>(B, cy == 0 ? 2 : 3, cx, n0, k, F, factor);
-          } else {
-            z_face(k + 1, szc + scur * 5 * NT, szc + (scur ^ 1) * 5 * NT,
-                   fzc + (fcur ^ 1) * NF * NT);
+          for (int u = 0; u < NF; ++u) out[u * ostride] = F[u];
+          if (B.fluence && (isx ? (cx == 0 || cx == n0) : (cy == 0 || cy == n1))) {
+            if (isx)
+              boundary_fluence<0, HLLC, NF>(B, ph, l, r, diff, F, cx == 0 ? 0 : 1, cy, n1, k,
+                                            factor);
+            else
+              boundary_fluence<1, HLLC, NF>(B, ph, l, r, diff, F, cy == 0 ? 2 : 3, cx, n0, k,
+                                            factor);
           }
         }
       }
+
+      // (4) z slope at k+1 and z face k+1 of the own column
+      double zsn[5], zfn[NF];
+      z_slope(k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
+      z_face(k + 1, full + c_off, PS, zss + tid, NT, cslot(k + 1), NT, zsn, 1, zfn);
       __syncthreads();
 
-      // (4) cell update and stage epilogue
+      // (5) cell update and stage epilogue
       if (own) {
-        const double w0 = __ldg(B.geo[0].W + gx + 2), w1 = __ldg(B.geo[1].W + gy + 2),
-                     w2 = __ldg(B.geo[2].W + k + 2);
+        const double w0 = gxc[G_W * LX + tx + 2], w1 = gyc[G_W * LY + ty + 2],
+                     w2 = __ldg(GZ.W + k + 2);
         const double vol = w0 * w1 * w2;
+        const double rvol = 1.0 / vol;
         const double ax = w1 * w2, ay = w2 * w0, az = w0 * w1;
-        const double* fzm = fzc + fcur * NF * NT;
-        const double* fzp = fzc + (fcur ^ 1) * NF * NT;
         const long long gidx =
             (gx + 2) + (long long)B.m[0] * ((gy + 2) + (long long)B.m[1] * (k + 2));
         const long long cidx = gx + (long long)n0 * (gy + (long long)n1 * k);
+        // dU += dT (A_I F_I(i) - A_I F_I(i+1)) / V per direction
+        // (IncrementDivergence_FV__Kernel.f90:729-748), all quotients at once
+        double nx_[NF], ny_[NF], nz_[NF], qx[NF], qy[NF], qz[NF];
+        bool ok = true;
+#pragma unroll
+        for (int u = 0; u < NF; ++u) {
+          nx_[u] = dt * (ax * fxs[(u * TY + ty) * (TX + 1) + tx] -
+                         ax * fxs[(u * TY + ty) * (TX + 1) + tx + 1]);
+          ny_[u] = dt * (ay * fys[(u * (TY + 1) + ty) * TX + tx] -
+                         ay * fys[(u * (TY + 1) + ty + 1) * TX + tx]);
+          nz_[u] = dt * (az * zfs[u * NT + tid] - az * zfn[u]);
+          qx[u] = markstein(nx_[u], vol, rvol);
+          qy[u] = markstein(ny_[u], vol, rvol);
+          qz[u] = markstein(nz_[u], vol, rvol);
+          ok &= quotient_in_range(nx_[u], rvol) & quotient_in_range(ny_[u], rvol) &
+                quotient_in_range(nz_[u], rvol);
+        }
+        if (!ok) {
+#pragma unroll
+          for (int u = 0; u < NF; ++u) {
+            qx[u] = div_ieee(nx_[u], vol);
+            qy[u] = div_ieee(ny_[u], vol);
+            qz[u] = div_ieee(nz_[u], vol);
+          }
+        }
         double Kc[NF];
 #pragma unroll
         for (int u = 0; u < NF; ++u) {
-          const double dxu =
-              dt * (ax * fxs[(u * TY + ty) * (TX + 1) + tx] -
-                    ax * fxs[(u * TY + ty) * (TX + 1) + tx + 1]) / vol;
-          const double dyu = dt * (ay * fys[(u * (TY + 1) + ty) * TX + tx] -
-                                   ay * fys[(u * (TY + 1) + ty + 1) * TX + tx]) / vol;
-          const double dzu = dt * (az * fzm[u * NT + tid] - az * fzp[u * NT + tid]) / vol;
           if (MODE == MODE_INCREMENT) {
             double* kp = B.K + (long long)u * B.nV + gidx;
-            *kp = *kp + dxu + dyu + dzu;
+            *kp = *kp + qx[u] + qy[u] + qz[u];
           } else {
-            Kc[u] = dxu + dyu + dzu;
+            Kc[u] = qx[u] + qy[u] + qz[u];
           }
         }
         if (MODE != MODE_INCREMENT) {
-          const double N = pk[c_off], V1 = pk[PS + c_off], V2 = pk[2 * PS + c_off],
-                       V3 = pk[3 * PS + c_off], E = pk[4 * PS + c_off];
+          const double N = full[c_off], V1 = full[PS + c_off], V2 = full[2 * PS + c_off],
+                       V3 = full[3 * PS + c_off], E = full[4 * PS + c_off];
           if (GRAV) {
             // ApplyGravity_F (ApplyGravity_F__Command.f90:124-264) with the
             // uniform gradient (0, 0, a); the x and y momentum terms subtract
@@ -464,13 +622,17 @@ __global__ void __launch_bounds__(NT, 1)
             U[3 * B.nV + gidx] = u.S3;
             U[4 * B.nV + gidx] = u.G;
             U[5 * B.nV + gidx] = SB * w.N;
-            tsi_max = fmax2(tsi_max, inverse_cfl_time(w, CS, w0, w1, w2));
+            tsi_max = fmax2(tsi_max,
+                            inverse_cfl_time(w, CS, w0, w1, w2, gxc[G_RW * LX + tx + 2],
+                                             gyc[G_RW * LY + ty + 2], __ldg(GZ.RW + k + 2)));
           }
         }
       }
+#pragma unroll
+      for (int q = 0; q < 5; ++q) zss[q * NT + tid] = zsn[q];
+#pragma unroll
+      for (int u = 0; u < NF; ++u) zfs[u * NT + tid] = zfn[u];
       __syncthreads();
-      scur ^= 1;
-      fcur ^= 1;
     }
 
     if (MODE == MODE_STAGE2) {
