@@ -108,34 +108,71 @@ __global__ void to_primitive_kernel(Box b, Phys ph, double* __restrict__ U,
 // their image (the reference adds the image's exchanged increments to an
 // image copy); every other ghost keeps its conserved values through the
 // floors of ComputeFromConserved, which also recompute its DS.
-__global__ void ghost_refresh_kernel(Box b, Phys ph, double* __restrict__ U) {
+__device__ __forceinline__ void ghost_refresh_value(const Box& b, const Phys& ph, double* U,
+                                                    long long v) {
   const long long nV = b.nV;
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
-       v += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(v % b.m[0]);
-    const int j = (int)((v / b.m[0]) % b.m[1]);
-    const int k = (int)(v / ((long long)b.m[0] * b.m[1]));
-    const bool ghost = i < 2 || j < 2 || k < 2 || i >= b.n[0] + 2 || j >= b.n[1] + 2 ||
-                       k >= b.n[2] + 2;
-    if (!ghost) continue;
-    int si, sj, sk;
-    if (periodic_reachable(b, i, j, k, si, sj, sk)) {
-      const long long s = si + (long long)b.m[0] * (sj + (long long)b.m[1] * sk);
+  const int i = (int)(v % b.m[0]);
+  const int j = (int)((v / b.m[0]) % b.m[1]);
+  const int k = (int)(v / ((long long)b.m[0] * b.m[1]));
+  const bool ghost =
+      i < 2 || j < 2 || k < 2 || i >= b.n[0] + 2 || j >= b.n[1] + 2 || k >= b.n[2] + 2;
+  if (!ghost) return;
+  int si, sj, sk;
+  if (periodic_reachable(b, i, j, k, si, sj, sk)) {
+    const long long s = si + (long long)b.m[0] * (sj + (long long)b.m[1] * sk);
 #pragma unroll
-      for (int f = 0; f < 6; ++f) U[f * nV + v] = U[f * nV + s];
-    } else {
-      Cons u{U[v], U[nV + v], U[2 * nV + v], U[3 * nV + v], U[4 * nV + v]};
-      Prim w;
-      cons_to_prim(u, w, ph.nmin);
-      double P, CS, SB;
-      eos_cell(w.N, w.E, ph, P, CS, &SB);
-      U[v] = u.D;
-      U[nV + v] = u.S1;
-      U[2 * nV + v] = u.S2;
-      U[3 * nV + v] = u.S3;
-      U[4 * nV + v] = u.G;
-      U[5 * nV + v] = SB * w.N;
-    }
+    for (int f = 0; f < 6; ++f) U[f * nV + v] = U[f * nV + s];
+  } else {
+    Cons u{U[v], U[nV + v], U[2 * nV + v], U[3 * nV + v], U[4 * nV + v]};
+    Prim w;
+    cons_to_prim(u, w, ph.nmin);
+    double P, CS, SB;
+    eos_cell(w.N, w.E, ph, P, CS, &SB);
+    U[v] = u.D;
+    U[nV + v] = u.S1;
+    U[2 * nV + v] = u.S2;
+    U[3 * nV + v] = u.S3;
+    U[4 * nV + v] = u.G;
+    U[5 * nV + v] = SB * w.N;
+  }
+}
+
+__global__ void ghost_refresh_kernel(Box b, Phys ph, double* __restrict__ U) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < b.nV;
+       v += (long long)gridDim.x * blockDim.x)
+    ghost_refresh_value(b, ph, U, v);
+}
+
+// One brick of a batch for the element-wise kernels: its box, its state and
+// feature storage, and the offsets of its values in the batch's flat ranges.
+struct BatchBrick {
+  Box box;
+  double* U;
+  uint8_t* sb;
+  uint8_t* df;
+  const int* skip;
+  long long v_off;  // prefix sum of nV
+  long long c_off;  // prefix sum of nP
+};
+
+__device__ __forceinline__ int find_brick(const BatchBrick* bb, int n, long long x, bool cells) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long off = cells ? bb[mid].c_off : bb[mid].v_off;
+    if (off <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void batch_ghost_refresh_kernel(const BatchBrick* __restrict__ bb, int n,
+                                           long long total, Phys ph) {
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = find_brick(bb, n, x, false);
+    if (bb[b].skip && *bb[b].skip) continue;
+    ghost_refresh_value(bb[b].box, ph, bb[b].U, x - bb[b].v_off);
   }
 }
 
@@ -164,64 +201,90 @@ __device__ __forceinline__ void cell_p_v(const Box& b, const Phys& ph, const dou
 
 // DetectShocks_CSL_Kernel (FluidFeatures_P__Kernel.f90:12-186) for the proper
 // cells: bit e of sb[c] = shock along e at c (compared with c - e_e).
+__device__ __forceinline__ void detect_shock_cell(const Box& b, const Phys& ph, const double* U,
+                                                  const double* Pst, uint8_t* sb, long long c) {
+  const int i = (int)(c % b.n[0]);
+  const int j = (int)((c / b.n[0]) % b.n[1]);
+  const int k = (int)(c / ((long long)b.n[0] * b.n[1]));
+  double P0, v0[3];
+  cell_p_v(b, ph, U, Pst, i, j, k, P0, v0);
+  uint8_t bits = 0;
+  const int t[3] = {i, j, k};
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    if (t[e] < 1) continue;
+    double P1, v1[3];
+    cell_p_v(b, ph, U, Pst, i - (e == 0), j - (e == 1), k - (e == 2), P1, v1);
+    const double dP = fabs(P0 - P1);
+    const double pmin = (P0 < P1) ? P0 : P1;  // Fortran MIN: ties give either
+    const double dLnP = dP / fmax2(pmin, kSqrtTiny);
+    const double dV = v0[e] - v1[e];
+    if (dLnP > ph.shock_threshold && dV <= 0.0) bits |= (uint8_t)(1u << e);
+  }
+  sb[c] = bits;
+}
+
 __global__ void detect_shock_kernel(Box b, Phys ph, const double* __restrict__ U,
                                     const double* __restrict__ Pst, uint8_t* __restrict__ sb) {
-  const long long nP = b.nP;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
-       c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % b.n[0]);
-    const int j = (int)((c / b.n[0]) % b.n[1]);
-    const int k = (int)(c / ((long long)b.n[0] * b.n[1]));
-    double P0, v0[3];
-    cell_p_v(b, ph, U, Pst, i, j, k, P0, v0);
-    uint8_t bits = 0;
-    const int t[3] = {i, j, k};
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-      if (t[e] < 1) continue;
-      double P1, v1[3];
-      cell_p_v(b, ph, U, Pst, i - (e == 0), j - (e == 1), k - (e == 2), P1, v1);
-      const double dP = fabs(P0 - P1);
-      const double pmin = (P0 < P1) ? P0 : P1;  // Fortran MIN: ties give either
-      const double dLnP = dP / fmax2(pmin, kSqrtTiny);
-      const double dV = v0[e] - v1[e];
-      if (dLnP > ph.shock_threshold && dV <= 0.0) bits |= (uint8_t)(1u << e);
-    }
-    sb[c] = bits;
-  }
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
+       c += (long long)gridDim.x * blockDim.x)
+    detect_shock_cell(b, ph, U, Pst, sb, c);
 }
 
 // DIFFUSIVE_FLUX_I flags after ClearBoundary_CSL_Kernel (FluidFeatures_P__Kernel.f90:
 // 189-313) on a single brick: only cells at least two cells inside every face
 // keep flags, and DF_d(x) is set by a shock along e != d at x, x + e_e, x - e_d
 // or x + e_e - e_d (the positions DetectShocks_CSL_Kernel writes).
-__global__ void detect_flags_kernel(Box b, const uint8_t* __restrict__ sb,
-                                    uint8_t* __restrict__ df) {
-  const long long nP = b.nP;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
-       c += (long long)gridDim.x * blockDim.x) {
-    const int t[3] = {(int)(c % b.n[0]), (int)((c / b.n[0]) % b.n[1]),
-                      (int)(c / ((long long)b.n[0] * b.n[1]))};
-    uint8_t bits = 0;
-    bool interior = true;
+__device__ __forceinline__ void detect_flags_cell(const Box& b, const uint8_t* sb, uint8_t* df,
+                                                  long long c) {
+  const int t[3] = {(int)(c % b.n[0]), (int)((c / b.n[0]) % b.n[1]),
+                    (int)(c / ((long long)b.n[0] * b.n[1]))};
+  uint8_t bits = 0;
+  bool interior = true;
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-      if (t[d] < 1 || t[d] > b.n[d] - 2) interior = false;
-    if (interior) {
-      const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
+  for (int d = 0; d < 3; ++d)
+    if (t[d] < 1 || t[d] > b.n[d] - 2) interior = false;
+  if (interior) {
+    const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3; ++d) {
 #pragma unroll
-        for (int e = 0; e < 3; ++e) {
-          if (e == d) continue;
-          const uint8_t m = (uint8_t)(1u << e);
-          if ((sb[c] & m) || (sb[c + st[e]] & m) || (sb[c - st[d]] & m) ||
-              (sb[c + st[e] - st[d]] & m))
-            bits |= (uint8_t)(1u << d);
-        }
+      for (int e = 0; e < 3; ++e) {
+        if (e == d) continue;
+        const uint8_t m = (uint8_t)(1u << e);
+        if ((sb[c] & m) || (sb[c + st[e]] & m) || (sb[c - st[d]] & m) ||
+            (sb[c + st[e] - st[d]] & m))
+          bits |= (uint8_t)(1u << d);
       }
     }
-    df[c] = bits;
+  }
+  df[c] = bits;
+}
+
+__global__ void detect_flags_kernel(Box b, const uint8_t* __restrict__ sb,
+                                    uint8_t* __restrict__ df) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
+       c += (long long)gridDim.x * blockDim.x)
+    detect_flags_cell(b, sb, df, c);
+}
+
+__global__ void batch_detect_shock_kernel(const BatchBrick* __restrict__ bb, int n,
+                                          long long total, Phys ph) {
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = find_brick(bb, n, x, true);
+    if (bb[b].skip && *bb[b].skip) continue;
+    detect_shock_cell(bb[b].box, ph, bb[b].U, nullptr, bb[b].sb, x - bb[b].c_off);
+  }
+}
+
+__global__ void batch_detect_flags_kernel(const BatchBrick* __restrict__ bb, int n,
+                                          long long total) {
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = find_brick(bb, n, x, true);
+    if (bb[b].skip && *bb[b].skip) continue;
+    detect_flags_cell(bb[b].box, bb[b].sb, bb[b].df, x - bb[b].c_off);
   }
 }
 
@@ -313,9 +376,11 @@ __global__ void advance_clock_kernel(Clock* __restrict__ clk, int n) {
 
 __global__ void reset_bits_kernel(unsigned long long* __restrict__ bits, int n, int* counter,
                                   int n_counters) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) bits[i] = 0x0010000000000000ull;  // ordered_bits(-DBL_MAX)
-  if (i < n_counters) counter[i] = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < n_counters;
+       i += gridDim.x * blockDim.x) {
+    if (i < n) bits[i] = 0x0010000000000000ull;  // ordered_bits(-DBL_MAX)
+    if (i < n_counters) counter[i] = 0;
+  }
 }
 
 }  // namespace gfx

@@ -146,15 +146,14 @@ struct gfx_fluid {
 
 namespace {
 
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF>
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED>
 cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
                            int n_items, int* counter, const Phys& ph, cudaStream_t s) {
   using SM = StageLayout<NF>;
-  (void)many;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int per_sm = 1;
-  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF>;
+  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BATCHED>;
   std::call_once(once, [&] {
     attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)SM::kBytes);
@@ -165,32 +164,37 @@ cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const Work
   if (attr_err != cudaSuccess) return attr_err;
   // persistent grid: every resident CTA slot pulls work items
   const int grid = std::max(1, std::min(n_items, num_sms() * per_sm));
-  kern<<<grid, NT, SM::kBytes, s>>>(d, items, n_items, counter, ph);
+  kern<<<grid, NT, SM::kBytes, s>>>(d, many, items, n_items, counter, ph);
   return cudaGetLastError();
 }
 
 cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const BrickDesc& d,
                          const BrickDesc* many, const WorkItem* items, int n_items,
                          int* counter, const Phys& ph, cudaStream_t s) {
-#define GFX_STAGE(M, IP, HC, GR, NF)                                                     \
-  if (mode == M && in_prim == IP && hllc == HC && grav == GR)                           \
-    return launch_stage_t<M, IP, HC, GR, NF>(d, many, items, n_items, counter, ph, s);
-  GFX_STAGE(MODE_INCREMENT, false, false, false, 6)
-  GFX_STAGE(MODE_INCREMENT, false, true, false, 6)
-  GFX_STAGE(MODE_INCREMENT, true, false, false, 6)
-  GFX_STAGE(MODE_INCREMENT, true, true, false, 6)
-  GFX_STAGE(MODE_STAGE1, false, false, false, 5)
-  GFX_STAGE(MODE_STAGE1, false, true, false, 5)
-  GFX_STAGE(MODE_STAGE1, false, false, true, 5)
-  GFX_STAGE(MODE_STAGE1, false, true, true, 5)
-  GFX_STAGE(MODE_STAGE1, true, false, false, 5)
-  GFX_STAGE(MODE_STAGE1, true, true, false, 5)
-  GFX_STAGE(MODE_STAGE1, true, false, true, 5)
-  GFX_STAGE(MODE_STAGE1, true, true, true, 5)
-  GFX_STAGE(MODE_STAGE2, true, false, false, 5)
-  GFX_STAGE(MODE_STAGE2, true, true, false, 5)
-  GFX_STAGE(MODE_STAGE2, true, false, true, 5)
-  GFX_STAGE(MODE_STAGE2, true, true, true, 5)
+  const bool bat = many != nullptr;
+#define GFX_STAGE(M, IP, HC, GR, NF, BA)                                                  \
+  if (mode == M && in_prim == IP && hllc == HC && grav == GR && bat == BA)              \
+    return launch_stage_t<M, IP, HC, GR, NF, BA>(d, many, items, n_items, counter, ph, s);
+#define GFX_STAGE_B(M, IP, HC, GR, NF) \
+  GFX_STAGE(M, IP, HC, GR, NF, false)  \
+  GFX_STAGE(M, IP, HC, GR, NF, true)
+  GFX_STAGE(MODE_INCREMENT, false, false, false, 6, false)
+  GFX_STAGE(MODE_INCREMENT, false, true, false, 6, false)
+  GFX_STAGE(MODE_INCREMENT, true, false, false, 6, false)
+  GFX_STAGE(MODE_INCREMENT, true, true, false, 6, false)
+  GFX_STAGE_B(MODE_STAGE1, false, false, false, 5)
+  GFX_STAGE_B(MODE_STAGE1, false, true, false, 5)
+  GFX_STAGE(MODE_STAGE1, false, false, true, 5, false)
+  GFX_STAGE(MODE_STAGE1, false, true, true, 5, false)
+  GFX_STAGE_B(MODE_STAGE1, true, false, false, 5)
+  GFX_STAGE_B(MODE_STAGE1, true, true, false, 5)
+  GFX_STAGE(MODE_STAGE1, true, false, true, 5, false)
+  GFX_STAGE(MODE_STAGE1, true, true, true, 5, false)
+  GFX_STAGE_B(MODE_STAGE2, true, false, false, 5)
+  GFX_STAGE_B(MODE_STAGE2, true, true, false, 5)
+  GFX_STAGE(MODE_STAGE2, true, false, true, 5, false)
+  GFX_STAGE(MODE_STAGE2, true, true, true, 5, false)
+#undef GFX_STAGE_B
 #undef GFX_STAGE
   return cudaErrorInvalidValue;
 }
@@ -334,6 +338,62 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
   CUDA_TRY(cudaGetLastError());
   if (ev) CUDA_TRY(cudaEventRecord(ev[4], s));
   h->launches += 3;
+  return GFX_OK;
+}
+
+}  // namespace
+
+struct gfx_fluid_batch {
+  int n = 0;
+  std::vector<gfx_fluid*> h;
+  std::vector<double*> U;
+  Phys ph;
+  bool hllc = false, grav = false;
+  BrickDesc* d1 = nullptr;   // stage 1 from conserved input, per brick
+  BrickDesc* d1p = nullptr;  // stage 1 from kept primitives, per brick
+  BrickDesc* d2 = nullptr;   // stage 2, per brick
+  WorkItem* items = nullptr;
+  int n_items = 0;
+  BatchBrick* bb = nullptr;
+  long long total_v = 0, total_c = 0;
+  unsigned long long* tsi_bits = nullptr;  // [n]
+  Clock* clocks = nullptr;                 // [n]
+  int* counters = nullptr;                 // [4]
+  cudaGraphExec_t graph = nullptr;
+  long long graph_kernels = 0;
+  long long launches = 0;
+};
+
+namespace {
+
+// The launches of one batched cycle: shock flags (HLLC), the two stages for
+// every brick, ghosts, then each brick's clock and next time step.
+int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, bool in_prim, cudaStream_t s) {
+  const int blk = 256;
+  reset_bits_kernel<<<grid_for(std::max(B->n, 4), blk), blk, 0, s>>>(B->tsi_bits, B->n,
+                                                                      B->counters, 4);
+  CUDA_TRY(cudaGetLastError());
+  B->launches += 1;
+  if (B->hllc && detect) {
+    batch_detect_shock_kernel<<<grid_for(B->total_c, blk), blk, 0, s>>>(B->bb, B->n,
+                                                                        B->total_c, B->ph);
+    batch_detect_flags_kernel<<<grid_for(B->total_c, blk), blk, 0, s>>>(B->bb, B->n,
+                                                                        B->total_c);
+    CUDA_TRY(cudaGetLastError());
+    B->launches += 2;
+  }
+  BrickDesc none;
+  memset(&none, 0, sizeof(none));
+  CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, B->hllc, false, none, in_prim ? B->d1p : B->d1,
+                        B->items, B->n_items, B->counters, B->ph, s));
+  CUDA_TRY(launch_stage(MODE_STAGE2, true, B->hllc, false, none, B->d2, B->items, B->n_items,
+                        B->counters + 1, B->ph, s));
+  batch_ghost_refresh_kernel<<<grid_for(B->total_v, blk), blk, 0, s>>>(B->bb, B->n,
+                                                                       B->total_v, B->ph);
+  advance_clock_kernel<<<grid_for(B->n, blk), blk, 0, s>>>(B->clocks, B->n);
+  finalize_dt_kernel<<<grid_for(B->n, blk), blk, 0, s>>>(B->ph, B->tsi_bits, B->clocks, B->n, 1);
+  CUDA_TRY(cudaGetLastError());
+  B->launches += 5;
   return GFX_OK;
 }
 
@@ -736,6 +796,230 @@ int gfx_fluid_step_timed(gfx_fluid* h, double* U, double dt, double* fluence, do
 int gfx_fluid_kernel_launches(const gfx_fluid* h, long long* count) {
   if (!h || !count) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   *count = h->launches;
+  return GFX_OK;
+}
+
+int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
+                           gfx_fluid_batch** out) {
+  if (!out || n < 1 || !handles || !U) return fail(GFX_ERR_ARGUMENT, "bad batch arguments");
+  *out = nullptr;
+  for (int b = 0; b < n; ++b)
+    if (!handles[b] || !U[b]) return fail(GFX_ERR_ARGUMENT, "brick %d: NULL handle or state", b);
+  const gfx_fluid_config& c0 = handles[0]->cfg;
+  for (int b = 1; b < n; ++b) {
+    const gfx_fluid_config& c = handles[b]->cfg;
+    if (c.riemann_solver != c0.riemann_solver || c.uniform_acceleration != 0.0 ||
+        c.adiabatic_index != c0.adiabatic_index || c.limiter_parameter != c0.limiter_parameter ||
+        c.use_limiter != c0.use_limiter || c.shock_threshold != c0.shock_threshold ||
+        c.courant_factor != c0.courant_factor || c.baryon_density_min != c0.baryon_density_min ||
+        c.n_ramp_cycles != c0.n_ramp_cycles)
+      return fail(GFX_ERR_ARGUMENT, "brick %d: parameters differ from brick 0", b);
+  }
+  if (c0.uniform_acceleration != 0.0)
+    return fail(GFX_ERR_UNSUPPORTED, "batched bricks with gravity are not built");
+  gfx_fluid_batch* B = new (std::nothrow) gfx_fluid_batch();
+  if (!B) return fail(GFX_ERR_NO_MEMORY, "host allocation failed");
+  auto cleanup = [&](int code) {
+    gfx_fluid_batch_destroy(B);
+    return code;
+  };
+  B->n = n;
+  B->h.assign(handles, handles + n);
+  B->U.assign(U, U + n);
+  B->ph = handles[0]->ph;
+  B->hllc = c0.riemann_solver == GFX_RIEMANN_HLLC;
+  if (cudaMalloc(&B->tsi_bits, n * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&B->clocks, n * sizeof(Clock)) != cudaSuccess ||
+      cudaMalloc(&B->counters, 4 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&B->d1, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&B->d1p, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&B->d2, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&B->bb, n * sizeof(BatchBrick)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch tables"));
+  std::vector<BrickDesc> d1(n), d1p(n), d2(n);
+  std::vector<BatchBrick> bb(n);
+  std::vector<WorkItem> items;
+  std::vector<long long> work;
+  for (int b = 0; b < n; ++b) {
+    gfx_fluid* h = handles[b];
+    const uint8_t* df = B->hllc ? h->df : nullptr;
+    const double* dt = &B->clocks[b].dt;
+    const int* skip = &B->clocks[b].done;
+    d1[b] = make_desc(h, U[b], nullptr, nullptr, nullptr, df, nullptr, dt, 0.5, skip);
+    d1p[b] = make_desc(h, U[b], nullptr, nullptr, h->Pst, df, nullptr, dt, 0.5, skip);
+    d2[b] = make_desc(h, U[b], U[b], nullptr, h->Yp, df, nullptr, dt, 0.5, skip);
+    d1[b].tsi_bits = d1p[b].tsi_bits = d2[b].tsi_bits = B->tsi_bits + b;
+    bb[b].box = h->box;
+    bb[b].U = U[b];
+    bb[b].sb = h->sb;
+    bb[b].df = h->df;
+    bb[b].skip = skip;
+    bb[b].v_off = B->total_v;
+    bb[b].c_off = B->total_c;
+    B->total_v += h->box.nV;
+    B->total_c += h->box.nP;
+    // z chunks of 32 planes: few prologues, many items to balance
+    const int* nn = h->box.n;
+    const int len = std::min(nn[2], 32);
+    for (int z = 0; z < nn[2]; z += len)
+      for (int y = 0; y < nn[1]; y += TY)
+        for (int x = 0; x < nn[0]; x += TX) {
+          items.push_back({b, x, y, z, std::min(nn[2], z + len)});
+          work.push_back((long long)std::min(TX, nn[0] - x) * std::min(TY, nn[1] - y) *
+                         (std::min(nn[2], z + len) - z));
+        }
+  }
+  // longest items first (LPT order for the persistent CTAs' work counter)
+  std::vector<int> order(items.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  std::vector<WorkItem> sorted(items.size());
+  for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
+  B->n_items = (int)sorted.size();
+  if (cudaMalloc(&B->items, sorted.size() * sizeof(WorkItem)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch work items"));
+  if (cudaMemcpy(B->d1, d1.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(B->d1p, d1p.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(B->d2, d2.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(B->bb, bb.data(), n * sizeof(BatchBrick), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(B->items, sorted.data(), sorted.size() * sizeof(WorkItem),
+                 cudaMemcpyHostToDevice))
+    return cleanup(fail(GFX_ERR_CUDA, "copy batch tables"));
+  std::vector<Clock> clk(n);
+  for (auto& c : clk) {
+    memset(&c, 0, sizeof(c));
+    c.finish = DBL_MAX;
+    c.max_cycle = 0x7fffffff;
+  }
+  if (cudaMemcpy(B->clocks, clk.data(), n * sizeof(Clock), cudaMemcpyHostToDevice))
+    return cleanup(fail(GFX_ERR_CUDA, "init batch clocks"));
+  *out = B;
+  return GFX_OK;
+}
+
+int gfx_fluid_batch_destroy(gfx_fluid_batch* B) {
+  if (!B) return GFX_OK;
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  cudaFree(B->tsi_bits);
+  cudaFree(B->clocks);
+  cudaFree(B->counters);
+  cudaFree(B->d1);
+  cudaFree(B->d1p);
+  cudaFree(B->d2);
+  cudaFree(B->bb);
+  cudaFree(B->items);
+  delete B;
+  return GFX_OK;
+}
+
+int gfx_fluid_batch_set_clocks(gfx_fluid_batch* B, double time, int i_cycle) {
+  if (!B) return fail(GFX_ERR_ARGUMENT, "NULL batch");
+  std::vector<Clock> clk(B->n);
+  for (auto& c : clk) {
+    memset(&c, 0, sizeof(c));
+    c.time = time;
+    c.cycle = i_cycle;
+    c.finish = DBL_MAX;
+    c.max_cycle = 0x7fffffff;
+  }
+  CUDA_TRY(cudaMemcpy(B->clocks, clk.data(), B->n * sizeof(Clock), cudaMemcpyHostToDevice));
+  return GFX_OK;
+}
+
+// per brick: finish time and cycle limit for this call, done flags
+__global__ void batch_arm_clocks_kernel(Clock* clk, int n, double finish, int n_cycles) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Clock& c = clk[b];
+  c.finish = finish;
+  const long long mc = (long long)c.cycle + n_cycles;
+  c.max_cycle = (int)(mc > 0x7fffffffLL ? 0x7fffffffLL : mc);
+  c.done = !(c.time < c.finish && c.cycle < c.max_cycle);
+}
+
+int gfx_fluid_batch_evolve(gfx_fluid_batch* B, double finish_time, int n_cycles, void* stream) {
+  if (!B || n_cycles < 0) return fail(GFX_ERR_ARGUMENT, "bad batch evolve arguments");
+  if (n_cycles == 0) return GFX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  // one state for the first cycle: every brick's primitives kept, or none
+  int pend = 0, feat_pending = 0, feat_zero = 0;
+  for (gfx_fluid* h : B->h) {
+    pend += h->prims_pending;
+    feat_pending += (h->features == FEAT_PENDING);
+    feat_zero += (h->features == FEAT_ZERO);
+  }
+  if (pend != 0 && pend != B->n)
+    return fail(GFX_ERR_STATE, "batch: bricks mix kept primitives and conserved states");
+  if (B->hllc && feat_pending != 0 && feat_pending != B->n)
+    return fail(GFX_ERR_STATE, "batch: bricks mix pending and current features");
+  const bool in_prim = pend == B->n;
+  const int blk = 256;
+  batch_arm_clocks_kernel<<<grid_for(B->n, blk), blk, 0, s>>>(B->clocks, B->n, finish_time,
+                                                              n_cycles);
+  reset_bits_kernel<<<grid_for(std::max(B->n, 4), blk), blk, 0, s>>>(B->tsi_bits, B->n,
+                                                                      B->counters, 0);
+  CUDA_TRY(cudaGetLastError());
+  B->launches += 2;
+  for (int b = 0; b < B->n; ++b) {
+    gfx_fluid* h = B->h[b];
+    inverse_timestep_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(
+        h->box, h->ph, B->U[b], in_prim ? h->Pst : nullptr, h->dgeo[0], h->dgeo[1],
+        h->dgeo[2], B->tsi_bits + b);
+  }
+  finalize_dt_kernel<<<grid_for(B->n, blk), blk, 0, s>>>(B->ph, B->tsi_bits, B->clocks, B->n, 1);
+  CUDA_TRY(cudaGetLastError());
+  B->launches += B->n + 1;
+  // first cycle eagerly (its primitives and features follow the handles' state)
+  int rc = enqueue_batch_cycle(B, B->hllc && feat_pending == B->n, in_prim, s);
+  if (rc) return rc;
+  for (gfx_fluid* h : B->h) {
+    h->prims_pending = false;
+    h->features = FEAT_PENDING;
+  }
+  for (int b = 0; b < B->n; ++b) B->h[b]->features_src = B->U[b];
+  if (n_cycles > 1) {
+    if (!B->graph) {
+      cudaStream_t cs;
+      CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      const long long before = B->launches;
+      CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      int rc2 = enqueue_batch_cycle(B, true, false, cs);
+      cudaError_t ce = cudaStreamEndCapture(cs, &g);
+      cudaStreamDestroy(cs);
+      B->graph_kernels = B->launches - before;
+      B->launches = before;
+      if (rc2) return rc2;
+      if (ce != cudaSuccess)
+        return fail(GFX_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&B->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess)
+        return fail(GFX_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ce));
+    }
+    for (int r = 1; r < n_cycles; ++r) CUDA_TRY(cudaGraphLaunch(B->graph, s));
+    B->launches += (long long)(n_cycles - 1) * B->graph_kernels;
+  }
+  return GFX_OK;
+}
+
+int gfx_fluid_batch_clocks(gfx_fluid_batch* B, double* time, int* cycle, void* stream) {
+  if (!B) return fail(GFX_ERR_ARGUMENT, "NULL batch");
+  std::vector<Clock> clk(B->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(clk.data(), B->clocks, B->n * sizeof(Clock), cudaMemcpyDeviceToHost,
+                           s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  for (int b = 0; b < B->n; ++b) {
+    if (time) time[b] = clk[b].time;
+    if (cycle) cycle[b] = clk[b].cycle;
+  }
+  return GFX_OK;
+}
+
+int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch* B, long long* count) {
+  if (!B || !count) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *count = B->launches;
   return GFX_OK;
 }
 

@@ -314,10 +314,14 @@ __device__ __forceinline__ void cell_slopes(const double* v, int vs, int st, con
                                      sqr, cden, rdxl, rdxr, rcden, ph.theta, ph.use_limiter);
 }
 
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF>
+// BATCHED: the work items span many bricks; each item's brick descriptor is
+// copied from `many` into shared memory.  Otherwise `single` describes the one
+// brick (read from the constant bank).
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED>
 __global__ void __launch_bounds__(NT, 2)
-    stage_kernel(const __grid_constant__ BrickDesc B, const WorkItem* __restrict__ items,
-                 int n_items, int* __restrict__ counter, const __grid_constant__ Phys ph) {
+    stage_kernel(const __grid_constant__ BrickDesc single, const BrickDesc* __restrict__ many,
+                 const WorkItem* __restrict__ items, int n_items, int* __restrict__ counter,
+                 const __grid_constant__ Phys ph) {
   using SL = StageLayout<NF>;
   extern __shared__ double smem[];
   double* full = smem;
@@ -332,24 +336,34 @@ __global__ void __launch_bounds__(NT, 2)
   double* gyc = gxc + SL::kGx;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
+  __shared__ BrickDesc s_desc;
   constexpr int LX = TX + 4, LY = TY + 4;
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int c_off = (ty + 2) * PW + (tx + 2);  // own cell in the full plane
-  const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
-  const AxisGeo& GZ = B.geo[2];
+  const BrickDesc& B = BATCHED ? s_desc : single;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(counter, 1);
     __syncthreads();
     const int it = s_item;
     if (it >= n_items) break;
+    const WorkItem W = items[it];
+    if (BATCHED) {
+      constexpr int nw = (int)(sizeof(BrickDesc) / sizeof(long long));
+      static_assert(sizeof(BrickDesc) % sizeof(long long) == 0, "descriptor size");
+      if (tid < nw)
+        reinterpret_cast<long long*>(&s_desc)[tid] =
+            reinterpret_cast<const long long*>(many + W.brick)[tid];
+      __syncthreads();
+    }
     if (B.skip && *B.skip) {
       __syncthreads();
       continue;
     }
-    const WorkItem W = items[it];
+    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const AxisGeo& GZ = B.geo[2];
     const double dt = *B.dt;
     const int x0 = W.x0, y0 = W.y0, z0 = W.z0, z1 = W.z1;
     const int gx = x0 + tx, gy = y0 + ty;

@@ -44,6 +44,12 @@ SIGNATURES = {
     "gfx_fluid_evolve": [P, P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I), P],
     "gfx_fluid_step_timed": [P, P, D, P, P, P],
     "gfx_fluid_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
+    "gfx_fluid_batch_create": [I, P, P, ctypes.POINTER(P)],
+    "gfx_fluid_batch_destroy": [P],
+    "gfx_fluid_batch_set_clocks": [P, D, I],
+    "gfx_fluid_batch_evolve": [P, D, I, P],
+    "gfx_fluid_batch_clocks": [P, P, P, P],
+    "gfx_fluid_batch_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
     "gfx_fluid_check_state": [P, P],
     "gfx_fluid_last_error": [ctypes.c_char_p, SZ],
 }

@@ -154,6 +154,27 @@ int gfx_fluid_step_timed(gfx_fluid *h, double *U_dev, double dt, double *fluence
 /* Number of kernels this handle has launched (graph replays included). */
 int gfx_fluid_kernel_launches(const gfx_fluid *h, long long *count);
 
+/* ---- Batched bricks -------------------------------------------------------
+ * Many independent bricks (each its own handle, state U and CFL time step)
+ * advanced together: one persistent launch per RK stage covers every brick's
+ * work, the whole cycle is one CUDA graph.  The handles must share the
+ * Riemann solver, gravity and the fluid / limiter / Courant parameters; the
+ * batch borrows them (destroy the batch first).  Each brick keeps its own
+ * clock (time, cycle); gfx_fluid_batch_evolve advances every brick until its
+ * finish_time (last step cut to land on it) or n_cycles more cycles.  The
+ * reference runs such bricks as separate programs or ranks; this has no
+ * single counterpart in it (Integrator_Template.f90:291-346 per brick). */
+typedef struct gfx_fluid_batch gfx_fluid_batch;
+int gfx_fluid_batch_create(int n_bricks, gfx_fluid *const *handles, double *const *U_dev,
+                           gfx_fluid_batch **out);
+int gfx_fluid_batch_destroy(gfx_fluid_batch *b);
+int gfx_fluid_batch_set_clocks(gfx_fluid_batch *b, double time, int i_cycle);
+int gfx_fluid_batch_evolve(gfx_fluid_batch *b, double finish_time, int n_cycles, void *stream);
+/* time_host[n], cycle_host[n] (either may be NULL); synchronises the stream. */
+int gfx_fluid_batch_clocks(gfx_fluid_batch *b, double *time_host, int *cycle_host,
+                           void *stream);
+int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch *b, long long *count);
+
 /* Bit pattern of the device-side error word accumulated by the kernels since
  * the last call (GFX_ERR_STATE if non-finite or non-positive density / energy
  * was produced); clears it.  Synchronises the stream. */
