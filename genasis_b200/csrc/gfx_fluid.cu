@@ -1036,3 +1036,305 @@ int gfx_fluid_last_error(char* buf, size_t len) {
 }
 
 }  // extern "C"
+
+// ---- One RK2 step that allocates nothing ----------------------------------
+// Some callers cannot call cudaMalloc: a host program whose memory manager
+// claims the device memory up front into a pool of its own (cudaMalloc then
+// fails, or is not theirs to call), or a code path that cannot afford the
+// device-wide synchronisation that cudaMalloc and cudaFree imply.  For them
+// gfx_fluid_step_noalloc runs the step of gfx_fluid_step without a handle:
+// every table and buffer that the step needs besides the caller's state lives
+// in one fixed array of device memory, compiled into this library.  Every GPU
+// that loads the library holds the array until the process exits.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = GFX_FLUID_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// The array's device address on the current device.  In host code the array's
+// name is only a host-side stand-in, so the address is asked of the runtime,
+// once per device, with that device current.
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(GFX_ERR_UNSUPPORTED, "device %d: the no-allocation step serves devices 0..%d",
+                dev, kNoAllocMaxDevices - 1);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(GFX_ERR_CUDA, "cudaGetSymbolAddress of the no-allocation scratch: %s",
+                  cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GFX_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Byte offsets of the step's buffers inside the scratch array.
+struct NoAllocLayout {
+  size_t geo[3], edge[3], yp, h, df, sb, bits, counters, dt, items, total;
+};
+
+// Parameters of the set-up kernel: the chart of the brick, the work list's
+// shape (the same cut of columns and z chunks as the handle's list) and the
+// step's time step.
+struct NoAllocSetup {
+  int n[3], m[3];
+  double mn[3], mx[3];
+  double* geo[3];   // 9 tables of m + 1 values per axis
+  double* edge[3];  // m + 1 cell edges per axis
+  WorkItem* items;
+  int cx, cy, len, n_items;
+  unsigned long long* bits;
+  int* counters;
+  double* dt_slot;
+  double dt;
+};
+
+// Geometry tables, work list, CFL word, work counters and time step of one
+// step, written into the scratch by one CTA.  The tables are the values of
+// build_axis (the same operations in the same order, IEEE divisions), so the
+// step reads the numbers that a handle's tables hold.
+__global__ void noalloc_setup_kernel(NoAllocSetup p) {
+  if (threadIdx.x < 3) {
+    // cell edges by repeated addition, ghost widths through single precision
+    // (Chart_Template.f90:478-560): a sequential chain, one thread per axis
+    const int d = threadIdx.x, n = p.n[d], g = 2;
+    double* E1 = p.edge[d] + g - 1;
+    const double width = (p.mx[d] - p.mn[d]) / (double)n;
+    E1[1] = p.mn[d];
+    for (int i = 2; i <= n + 1; ++i) E1[i] = E1[i - 1] + width;
+    for (int iC = 1; iC <= g; ++iC) {
+      const float w_ig = (float)(E1[iC + 1] - E1[iC]);
+      const float w_og = (float)(E1[n - iC + 2] - E1[n - iC + 1]);
+      E1[1 - iC] = E1[2 - iC] - (double)w_ig;
+      E1[n + 1 + iC] = E1[n + iC] + (double)w_og;
+    }
+  }
+  for (int i = threadIdx.x; i < p.n_items; i += blockDim.x) {
+    const int x = i % p.cx, y = (i / p.cx) % p.cy, zc = i / (p.cx * p.cy);
+    const int z0 = zc * p.len;
+    p.items[i] = {0, x * TX, y * TY, z0, min(p.n[2], z0 + p.len)};
+  }
+  if (threadIdx.x == 0) {
+    p.bits[0] = 0x0010000000000000ull;  // ordered_bits(-DBL_MAX), as reset_bits_kernel
+    p.bits[1] = 0x0010000000000000ull;
+    for (int c = 0; c < 4; ++c) p.counters[c] = 0;
+    *p.dt_slot = p.dt;
+  }
+  __syncthreads();
+  for (int d = 0; d < 3; ++d) {
+    const int m = p.m[d], L = m + 1;
+    const double* e = p.edge[d];
+    double* G = p.geo[d];
+    for (int t = threadIdx.x; t <= m; t += blockDim.x) {
+      double W = 0.0, WL = 0.0, WR = 0.0, RW = 0.0;
+      if (t < m) {
+        const double c = 0.5 * (e[t] + e[t + 1]);
+        WL = c - e[t];
+        WR = e[t + 1] - c;
+        W = WL + WR;
+        RW = 1.0 / W;
+      }
+      double dxi = 0.0, sq = 0.0, rdxi = 0.0, cden = 0.0, rcden = 0.0;
+      if (t >= 1 && t < m) {
+        const double c0 = 0.5 * (e[t - 1] + e[t]);
+        const double c1 = 0.5 * (e[t] + e[t + 1]);
+        dxi = c1 - c0;
+        sq = dxi * dxi;
+        rdxi = 1.0 / dxi;
+        if (t + 1 < m) {
+          const double c2 = 0.5 * (e[t + 1] + e[t + 2]);
+          const double dxn = c2 - c1;
+          cden = dxi * dxn * (dxi + dxn);
+          rcden = 1.0 / cden;
+        }
+      }
+      // table order of the handle's arena: W, WL, WR, dXI, SQ, CDEN, RDXI, RCDEN, RW
+      G[0 * L + t] = W;
+      G[1 * L + t] = WL;
+      G[2 * L + t] = WR;
+      G[3 * L + t] = dxi;
+      G[4 * L + t] = sq;
+      G[5 * L + t] = cden;
+      G[6 * L + t] = rdxi;
+      G[7 * L + t] = rcden;
+      G[8 * L + t] = RW;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// The step of gfx_fluid_step on a handle whose state was set from conserved
+// values (no pending primitives): features detected from U_dev first when
+// detect_features is nonzero, zero features otherwise (the first step after
+// initialisation).  Every buffer besides U_dev and fluence_dev is carved from
+// the fixed scratch array; nothing is allocated.
+int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
+                           int detect_features, double* fluence, void* stream) {
+  int rc = validate(cfg);
+  if (rc) return rc;
+  if (!U) return fail(GFX_ERR_ARGUMENT, "U_dev is NULL");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  // the parameters and chart of gfx_fluid_create, without the handle
+  Phys ph;
+  memset(&ph, 0, sizeof(ph));
+  ph.gamma = cfg->adiabatic_index;
+  ph.gm1 = cfg->adiabatic_index - 1.0;
+  ph.c_v = 1.0 / (1.0 * (cfg->adiabatic_index - 1.0));
+  ph.theta = cfg->limiter_parameter;
+  ph.nmin = cfg->baryon_density_min;
+  ph.accel = cfg->uniform_acceleration;
+  ph.shock_threshold = cfg->shock_threshold;
+  ph.courant = cfg->courant_factor;
+  ph.use_limiter = cfg->use_limiter ? 1 : 0;
+  ph.n_ramp = cfg->n_ramp_cycles;
+  Box b;
+  memset(&b, 0, sizeof(b));
+  for (int d = 0; d < 3; ++d) {
+    b.n[d] = cfg->n_cells[d];
+    b.m[d] = cfg->n_cells[d] + 4;
+    b.bc[d][0] = cfg->boundary[d][0];
+    b.bc[d][1] = cfg->boundary[d][1];
+  }
+  b.nV = (long long)b.m[0] * b.m[1] * b.m[2];
+  b.nP = (long long)b.n[0] * b.n[1] * b.n[2];
+  const long long face_size = std::max({(long long)b.n[1] * b.n[2],
+                                        (long long)b.n[0] * b.n[2],
+                                        (long long)b.n[0] * b.n[1]});
+  // work list shape: the cut of make_items
+  const int cx = (b.n[0] + TX - 1) / TX, cy = (b.n[1] + TY - 1) / TY;
+  const long long cols = (long long)cx * cy;
+  const long long want = 16LL * num_sms();
+  const int chunks =
+      (int)std::max(1LL, std::min<long long>(b.n[2] / 16, (want + cols - 1) / cols));
+  const int len = (b.n[2] + chunks - 1) / chunks;
+  const long long n_items = cols * ((b.n[2] + len - 1) / len);
+  // scratch layout, every buffer on a 256-byte boundary
+  NoAllocLayout L;
+  size_t off = 0;
+  for (int d = 0; d < 3; ++d) {
+    L.geo[d] = off;
+    off = align256(off + 9 * (size_t)(b.m[d] + 1) * sizeof(double));
+    L.edge[d] = off;
+    off = align256(off + (size_t)(b.m[d] + 1) * sizeof(double));
+  }
+  const size_t nP = (size_t)b.nP;
+  L.yp = off;
+  off = align256(off + 5 * nP * sizeof(double));
+  L.h = off;
+  off = align256(off + 5 * nP * sizeof(double));
+  L.df = off;
+  off = align256(off + nP);
+  L.sb = off;
+  off = align256(off + nP);
+  L.bits = off;
+  off = align256(off + 2 * sizeof(unsigned long long));
+  L.counters = off;
+  off = align256(off + 4 * sizeof(int));
+  L.dt = off;
+  off = align256(off + sizeof(double));
+  L.items = off;
+  off = align256(off + (size_t)n_items * sizeof(WorkItem));
+  L.total = off;
+  if (L.total > kNoAllocScratchBytes)
+    return fail(GFX_ERR_ARGUMENT,
+                "brick %d x %d x %d needs %zu bytes of scratch; the no-allocation step has "
+                "%zu: about 82 bytes per proper cell plus the chart tables, so up to about 50000 "
+                "proper cells (37^3 fits, 38^3 does not)",
+                b.n[0], b.n[1], b.n[2], L.total, kNoAllocScratchBytes);
+  unsigned char* base = nullptr;
+  rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+
+  NoAllocSetup p;
+  memset(&p, 0, sizeof(p));
+  AxisGeo geo[3];
+  for (int d = 0; d < 3; ++d) {
+    p.n[d] = b.n[d];
+    p.m[d] = b.m[d];
+    p.mn[d] = cfg->min_coordinate[d];
+    p.mx[d] = cfg->max_coordinate[d];
+    p.geo[d] = (double*)(base + L.geo[d]);
+    p.edge[d] = (double*)(base + L.edge[d]);
+    const int Lt = b.m[d] + 1;
+    const double* G = p.geo[d];
+    geo[d] = {G, G + Lt, G + 2 * Lt, G + 3 * Lt, G + 4 * Lt,
+              G + 5 * Lt, G + 6 * Lt, G + 7 * Lt, G + 8 * Lt};
+  }
+  p.items = (WorkItem*)(base + L.items);
+  p.cx = cx;
+  p.cy = cy;
+  p.len = len;
+  p.n_items = (int)n_items;
+  p.bits = (unsigned long long*)(base + L.bits);
+  p.counters = (int*)(base + L.counters);
+  p.dt_slot = (double*)(base + L.dt);
+  p.dt = dt;
+  // the scratch keeps the previous call's contents: the set-up rewrites the
+  // tables and the work list and zeroes the CFL word and the work counters
+  // (the two things that must start at zero) before the stages run
+  noalloc_setup_kernel<<<1, 256, 0, s>>>(p);
+  CUDA_TRY(cudaGetLastError());
+  if (fluence) CUDA_TRY(cudaMemsetAsync(fluence, 0, sizeof(double) * 36 * face_size, s));
+  const bool hllc = cfg->riemann_solver == GFX_RIEMANN_HLLC;
+  const bool grav = cfg->uniform_acceleration != 0.0;
+  uint8_t* df = (uint8_t*)(base + L.df);
+  uint8_t* sb = (uint8_t*)(base + L.sb);
+  const int blk = 256;
+  if (hllc && detect_features) {
+    detect_shock_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, ph, U, nullptr, sb);
+    CUDA_TRY(cudaGetLastError());
+    detect_flags_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, sb, df);
+    CUDA_TRY(cudaGetLastError());
+  }
+  const uint8_t* feat = (hllc && detect_features) ? df : nullptr;
+  BrickDesc d;
+  memset(&d, 0, sizeof(d));
+  for (int a = 0; a < 3; ++a) {
+    d.n[a] = b.n[a];
+    d.m[a] = b.m[a];
+    d.bc[a][0] = b.bc[a][0];
+    d.bc[a][1] = b.bc[a][1];
+    d.geo[a] = geo[a];
+  }
+  d.nV = b.nV;
+  d.nP = b.nP;
+  d.Yp = (double*)(base + L.yp);
+  d.H = (double*)(base + L.h);
+  d.df = feat;
+  d.fluence = fluence;
+  d.face_size = face_size;
+  d.dt = p.dt_slot;
+  d.weight = 0.5;
+  d.tsi_bits = p.bits;
+  d.skip = nullptr;
+  BrickDesc d1 = d;
+  d1.U_in = U;
+  CUDA_TRY(launch_stage(MODE_STAGE1, false, hllc, grav, d1, nullptr, p.items, p.n_items,
+                        p.counters, ph, s));
+  BrickDesc d2 = d;
+  d2.U_in = U;
+  d2.U_out = U;
+  d2.P_in = d.Yp;
+  CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, p.items, p.n_items,
+                        p.counters + 1, ph, s));
+  ghost_refresh_kernel<<<grid_for(b.nV, blk), blk, 0, s>>>(b, ph, U);
+  CUDA_TRY(cudaGetLastError());
+  return GFX_OK;
+}
+
+}  // extern "C"

@@ -175,6 +175,32 @@ int gfx_fluid_batch_clocks(gfx_fluid_batch *b, double *time_host, int *cycle_hos
                            void *stream);
 int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch *b, long long *count);
 
+/* ---- One step without allocation ------------------------------------------
+ * No counterpart in the reference (which allocates its storage once per
+ * run); added for callers that cannot call cudaMalloc: a host program whose
+ * memory manager has claimed the device memory up front into its own pool, or
+ * a code path that cannot afford the device-wide synchronisation that
+ * cudaMalloc and cudaFree imply.
+ *
+ * gfx_fluid_step_noalloc is gfx_fluid_step without a handle, on a state U_dev
+ * set from conserved values: the same kernels and results, features detected
+ * from U_dev first when detect_features is nonzero (every step after the
+ * first), zero features otherwise (the first step after initialisation).
+ * It allocates nothing: its tables and stage buffers live in one fixed
+ * array of GFX_FLUID_NOALLOC_SCRATCH_BYTES of device memory inside the
+ * library, which every GPU that loads the library holds until exit.  That
+ * bounds the brick at about 82 bytes per proper cell plus the chart tables
+ * (37^3 proper cells fit, 38^3 do not); larger bricks get GFX_ERR_ARGUMENT.
+ * The first call on a device looks up the array's device address (and sets
+ * up the stage kernels' launch attributes if no step ran before); make that
+ * first call before any stream capture.  Every call uses the same array: each
+ * call rewrites what it reads and zeroes its CFL word and work counters, so
+ * calls in sequence are independent, but calls that overlap on the GPU (on
+ * different streams or threads) race on the array and give wrong results. */
+#define GFX_FLUID_NOALLOC_SCRATCH_BYTES (4u << 20)
+int gfx_fluid_step_noalloc(const gfx_fluid_config *cfg, double *U_dev, double dt,
+                           int detect_features, double *fluence_dev, void *stream);
+
 /* Bit pattern of the device-side error word accumulated by the kernels since
  * the last call (GFX_ERR_STATE if non-finite or non-positive density / energy
  * was produced); clears it.  Synchronises the stream. */
