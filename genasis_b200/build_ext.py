@@ -12,7 +12,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgfx_fluid.so")
 SOURCES = ["gfx_fluid.cu"]
-HEADERS = ["fluid_physics.cuh", "stage_kernel.cuh", "aux_kernels.cuh"]
+HEADERS = ["fluid_physics.cuh", "stage_kernel.cuh", "aux_kernels.cuh", "adjoint_physics.cuh",
+           "adjoint_kernels.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

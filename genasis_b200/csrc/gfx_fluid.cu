@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint_kernels.cuh"
 #include "aux_kernels.cuh"
 #include "gfx_fluid.h"
 
@@ -142,6 +143,12 @@ struct gfx_fluid {
   double* graph_U = nullptr;
   long long graph_kernels = 0;  // kernel nodes per replay
   long long launches = 0;       // kernels launched so far
+  // adjoint workspace (allocated by the first gfx_fluid_step_adjoint):
+  // W0, lamZ, lamW, lamK1 (compact, 5 fields each), flags of U^n, and a
+  // recomputed U^n+1 when the caller passes none
+  double* adj = nullptr;
+  uint8_t* adj_flags = nullptr;
+  double* adj_U = nullptr;
 };
 
 namespace {
@@ -524,6 +531,9 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->dt_slot);
   cudaFree(h->items);
   cudaFree(h->U_stage);
+  cudaFree(h->adj);
+  cudaFree(h->adj_flags);
+  cudaFree(h->adj_U);
   if (h->host_stream) cudaStreamDestroy(h->host_stream);
   delete h;
   return GFX_OK;
@@ -1334,6 +1344,136 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
                         p.counters + 1, ph, s));
   ghost_refresh_kernel<<<grid_for(b.nV, blk), blk, 0, s>>>(b, ph, U);
   CUDA_TRY(cudaGetLastError());
+  return GFX_OK;
+}
+
+}  // extern "C"
+
+// ---- Discrete adjoint of one RK2 step --------------------------------------
+namespace {
+
+template <int D>
+cudaError_t launch_adj_face(const AdjDesc& A, bool hllc, const Phys& ph, cudaStream_t s) {
+  constexpr int T1 = (D == 0) ? 1 : 0;
+  constexpr int T2 = (D == 2) ? 1 : 2;
+  const long long total = (long long)A.nseg * A.n[T1] * A.n[T2];
+  const int blk = 128;
+  if (hllc)
+    adj_face_kernel<D, true><<<grid_for(total, blk), blk, 0, s>>>(A, ph);
+  else
+    adj_face_kernel<D, false><<<grid_for(total, blk), blk, 0, s>>>(A, ph);
+  return cudaGetLastError();
+}
+
+// L^T of one stage: lamW += (dK/dW)^T (kscale lamK), one launch per direction.
+int enqueue_adj_stage(gfx_fluid* h, const double* W, const double* lamK, double kscale,
+                      double* lamW, const uint8_t* df, double dt, cudaStream_t s) {
+  AdjDesc A;
+  memset(&A, 0, sizeof(A));
+  for (int a = 0; a < 3; ++a) {
+    A.n[a] = h->box.n[a];
+    A.bc[a][0] = h->box.bc[a][0];
+    A.bc[a][1] = h->box.bc[a][1];
+    A.geo[a] = h->dgeo[a];
+  }
+  A.nP = h->box.nP;
+  A.W = W;
+  A.lamK = lamK;
+  A.lamW = lamW;
+  A.df = df;
+  A.dt = dt;
+  A.kscale = kscale;
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  A.seg = 8;
+  A.nseg = (h->box.n[0] + 1 + A.seg - 1) / A.seg;
+  CUDA_TRY(launch_adj_face<0>(A, hllc, h->ph, s));
+  A.nseg = (h->box.n[1] + 1 + A.seg - 1) / A.seg;
+  CUDA_TRY(launch_adj_face<1>(A, hllc, h->ph, s));
+  A.nseg = (h->box.n[2] + 1 + A.seg - 1) / A.seg;
+  CUDA_TRY(launch_adj_face<2>(A, hllc, h->ph, s));
+  h->launches += 3;
+  return GFX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const double* lam_np1,
+                           double* lam_n, const double* U_np1, int detect_features,
+                           void* stream) {
+  if (!h || !U_n || !lam_np1 || !lam_n) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (lam_n == lam_np1) return fail(GFX_ERR_ARGUMENT, "lam_n must not alias lam_np1");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  cudaStream_t s = (cudaStream_t)stream;
+  const Box& b = h->box;
+  const size_t nP = (size_t)b.nP, nV = (size_t)b.nV;
+  if (!h->adj) {
+    if (cudaMalloc(&h->adj, 20 * nP * sizeof(double)) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
+    if (cudaMalloc(&h->adj_flags, 2 * nP) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
+  }
+  if (!U_np1 && !h->adj_U) {
+    if (cudaMalloc(&h->adj_U, 6 * nV * sizeof(double)) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint state");
+  }
+  double* W0 = h->adj;
+  double* lamZ = W0 + 5 * nP;
+  double* lamW = lamZ + 5 * nP;
+  double* lamK1 = lamW + 5 * nP;
+  uint8_t* df = h->adj_flags;
+  uint8_t* sb = df + nP;
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  const bool grav = h->cfg.uniform_acceleration != 0.0;
+  const int blk = 256;
+  // features of U^n (zero for the first step after initialisation)
+  const uint8_t* feat = nullptr;
+  if (hllc && detect_features) {
+    detect_shock_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, U_n, nullptr, sb);
+    detect_flags_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, sb, df);
+    CUDA_TRY(cudaGetLastError());
+    h->launches += 2;
+    feat = df;
+  }
+  // forward recomputation from the checkpoint: W0, stage 1 (W1 into Yp) and,
+  // without U^n+1 from the caller, stage 2
+  adj_prims_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, U_n, W0);
+  set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
+  reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 3;
+  BrickDesc d1 = make_desc(h, U_n, nullptr, nullptr, nullptr, feat, nullptr, h->dt_slot, 0.5,
+                           nullptr);
+  CUDA_TRY(launch_stage(MODE_STAGE1, false, hllc, grav, d1, nullptr, h->items, h->n_items,
+                        h->counters, h->ph, s));
+  h->launches += 1;
+  const double* Unew = U_np1;
+  if (!Unew) {
+    BrickDesc d2 = make_desc(h, U_n, h->adj_U, nullptr, h->Yp, feat, nullptr, h->dt_slot, 0.5,
+                             nullptr);
+    CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
+                          h->counters + 1, h->ph, s));
+    h->launches += 1;
+    Unew = h->adj_U;
+  }
+  // reverse sweep
+  adj_final_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, lam_np1, Unew, lamZ);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemsetAsync(lamW, 0, 5 * nP * sizeof(double), s));
+  h->launches += 1;
+  int rc = enqueue_adj_stage(h, h->Yp, lamZ, 0.5, lamW, feat, dt, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemsetAsync(lam_n, 0, 6 * nV * sizeof(double), s));
+  adj_mid_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, dt, h->Yp, lamZ, lamW, lamK1,
+                                                      lam_n);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  rc = enqueue_adj_stage(h, W0, lamK1, 1.0, lamW, feat, dt, s);
+  if (rc) return rc;
+  adj_last_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, dt, W0, lamK1, lamW, lam_n);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
   return GFX_OK;
 }
 

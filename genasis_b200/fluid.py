@@ -90,8 +90,11 @@ class FluidBox:
         return self.U
 
     def set_conserved(self, U):
+        """The state from conserved values: copied in, then ComputeFromConserved
+        (floors, DS), so that the next step starts from these values."""
         torch = _torch()
         self.U.copy_(torch.as_tensor(U, dtype=torch.float64))
+        lib.call("gfx_fluid_to_primitive", self.h, _ptr(self.U), None, None, _stream())
         return self.U
 
     def compute_from_conserved(self, detect_features=False, primitive=False, aux=False):

@@ -50,6 +50,7 @@ SIGNATURES = {
     "gfx_fluid_batch_evolve": [P, D, I, P],
     "gfx_fluid_batch_clocks": [P, P, P, P],
     "gfx_fluid_batch_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
+    "gfx_fluid_step_adjoint": [P, P, D, P, P, P, I, P],
     "gfx_fluid_step_noalloc": [ctypes.POINTER(GfxConfig), P, D, I, P, P],
     "gfx_fluid_check_state": [P, P],
     "gfx_fluid_last_error": [ctypes.c_char_p, SZ],

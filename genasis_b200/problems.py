@@ -187,3 +187,16 @@ def random_state(cfg, seed=1, shocks=True):
         prim[4] = np.where(left, prim[4] * 8.0, prim[4])
         prim[1] = np.where(left, prim[1] + 0.8, prim[1])
     return prim
+
+
+def noisy(prim, amp=2e-2, seed=7):
+    """prim with seeded relative noise of amplitude amp on N and E and
+    absolute noise on V: a state without exactly uniform fields, where the
+    limiter and the wave-speed maxima are differentiable (gradient checks)."""
+    rng = np.random.default_rng(seed)
+    out = np.array(prim, dtype=np.float64, copy=True)
+    out[0] *= 1.0 + amp * rng.uniform(-1.0, 1.0, size=out[0].shape)
+    out[4] *= 1.0 + amp * rng.uniform(-1.0, 1.0, size=out[4].shape)
+    for d in range(1, 4):
+        out[d] += amp * rng.uniform(-1.0, 1.0, size=out[d].shape)
+    return out

@@ -175,6 +175,25 @@ int gfx_fluid_batch_clocks(gfx_fluid_batch *b, double *time_host, int *cycle_hos
                            void *stream);
 int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch *b, long long *count);
 
+/* ---- Discrete adjoint of one step -----------------------------------------
+ * No counterpart in the reference (which has no adjoint); it is the reverse
+ * mode of gfx_fluid_step, with dt held fixed.  Given lam_np1_dev ([6][nV],
+ * the gradient of an objective with respect to the conserved state after the
+ * step), writes lam_n_dev ([6][nV]): the gradient with respect to the
+ * conserved state U_n_dev before the step, on proper cells (ghost values and
+ * the dead DS field get 0; a periodic ghost's share goes to its image cell).
+ * The stages are recomputed from the checkpoint U_n_dev; U_np1_dev (may be
+ * NULL, then recomputed too) is the state after the step, as gfx_fluid_step
+ * produced it.  detect_features: 1 if the forward step detected the shock
+ * features of U_n (every step after the first), 0 if it ran on zero features
+ * (the first step after initialisation).  The derivative is that of the
+ * branch the forward step takes at every limiter, wave-speed maximum, HLLC
+ * side and floor.  Allocates a workspace of 20 values per proper cell on the
+ * first call.  lam_n_dev must not alias lam_np1_dev. */
+int gfx_fluid_step_adjoint(gfx_fluid *h, const double *U_n_dev, double dt,
+                           const double *lam_np1_dev, double *lam_n_dev,
+                           const double *U_np1_dev, int detect_features, void *stream);
+
 /* ---- One step without allocation ------------------------------------------
  * No counterpart in the reference (which allocates its storage once per
  * run); added for callers that cannot call cudaMalloc: a host program whose

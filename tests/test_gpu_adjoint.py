@@ -1,0 +1,174 @@
+"""The hand-written discrete adjoint of the RK2 step against central finite
+differences: of the CUDA forward (the same step it differentiates) and of the
+oracle's forward (a gradient from the reference's step), through the
+torch.autograd.Function over a run of several steps.
+
+The states carry seeded noise on every field: at an exactly uniform field
+the limiter sits on its kink (the slope of a constant is zero, and its
+one-sided derivatives differ), where no finite difference defines a gradient."""
+import numpy as np
+import pytest
+
+from genasis_b200 import problems
+from genasis_b200.config import FluidConfig
+from tests.gpu_helpers import to_np
+
+pytestmark = pytest.mark.gpu
+
+EPS = 1e-6
+RTOL = 1e-5
+
+
+def _cases():
+    refl = FluidConfig(n_cells=(14, 10, 12), riemann_solver="HLLC",
+                       boundary=(("REFLECTING", "REFLECTING"),) * 3, courant_factor=0.8,
+                       n_ramp_cycles=1)
+    grav = FluidConfig(n_cells=(12, 10, 16), riemann_solver="HLL",
+                       boundary=(("OUTFLOW", "OUTFLOW"), ("PERIODIC", "PERIODIC"),
+                                 ("REFLECTING", "REFLECTING")),
+                       uniform_acceleration=0.1, courant_factor=0.8, n_ramp_cycles=1)
+    kh_cfg, kh_prim = problems.kelvin_helmholtz(16)
+    return {
+        "random_reflecting_hllc": (refl, problems.noisy(problems.random_state(refl, seed=2,
+                                                                              shocks=False))),
+        "random_hll_gravity": (grav, problems.noisy(problems.random_state(grav, seed=3,
+                                                                          shocks=False))),
+        "kh_noisy_hllc": (kh_cfg, problems.noisy(kh_prim, seed=11)),
+    }
+
+
+CASES = _cases()
+
+
+def _setup(name, n_steps=3):
+    import torch
+
+    from genasis_b200.fluid import FluidBox
+
+    cfg, prim = CASES[name]
+    box = FluidBox(cfg)
+    box.compute_from_primitive(prim)
+    box.compute_from_conserved()
+    U0 = box.U.clone()
+    dts = []
+    for i in range(n_steps):
+        dts.append(box.compute_time_step(i))
+        box.step(dts[-1])
+    torch.cuda.synchronize()
+    return cfg, box, U0, dts
+
+
+def _directions(cfg, count, seed):
+    """Seeded random directions over the proper cells of D, S1..3, G, unit norm."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        d = np.zeros((6,) + cfg.shape)
+        d[(slice(0, 5),) + cfg.proper] = rng.normal(size=(5,) + tuple(
+            int(cfg.n_cells[2 - a]) for a in range(3)))
+        out.append(d / np.linalg.norm(d))
+    return out
+
+
+def _periodic_images(cfg, U):
+    """U with its periodic ghosts refilled from the (perturbed) proper cells."""
+    idx = []
+    for a in range(3):
+        n = int(cfg.n_cells[2 - a])
+        if cfg.boundary[2 - a][0] == "PERIODIC":
+            idx.append((np.arange(n + 4) - 2) % n + 2)
+        else:
+            idx.append(np.arange(n + 4))
+    return U[:, idx[0]][:, :, idx[1]][:, :, :, idx[2]]
+
+
+def central_difference(rho, cfg, dv, U0, d, eps=EPS):
+    """(J(U0 + eps d) - J(U0 - eps d)) / (2 eps) for J = sum rho^2 dV, formed
+    cell by cell as sum (rho+ - rho-)(rho+ + rho-) dV / (2 eps) so that the
+    difference does not cancel in the total."""
+    rp = rho(U0 + eps * d)
+    rm = rho(U0 - eps * d)
+    p = cfg.proper
+    return float(((rp[p] - rm[p]) * (rp[p] + rm[p]) * dv[p]).sum() / (2.0 * eps))
+
+
+def _gradient(box, U0, dts):
+    import torch
+
+    from genasis_b200.adjoint import Evolve, density_squared
+
+    x = U0.clone().requires_grad_(True)
+    J = density_squared(box, Evolve.apply(x, box, dts, False))
+    J.backward()
+    return to_np(x.grad)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_adjoint_matches_central_differences_of_the_cuda_step(name):
+    import torch
+
+    from genasis_b200.adjoint import cell_volumes, run_forward
+
+    cfg, box, U0, dts = _setup(name)
+    g = _gradient(box, U0, dts)
+    dv = to_np(cell_volumes(box))
+    U0n = to_np(U0)
+
+    def rho(U):
+        out, _ = run_forward(box, torch.as_tensor(U, device="cuda"), dts, False, keep=False)
+        return to_np(out[0])
+
+    errs = []
+    for d in _directions(cfg, 6, seed=5):
+        fd = central_difference(rho, cfg, dv, U0n, d)
+        ad = float((g * d).sum())
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    assert max(errs) < RTOL, errs
+    # ghost values and the dead DS field carry no gradient
+    p = cfg.proper
+    mask = np.ones(cfg.shape, dtype=bool)
+    mask[p] = False
+    assert np.all(g[:, mask] == 0.0) and np.all(g[5] == 0.0)
+    box.close()
+
+
+def test_adjoint_matches_oracle_finite_differences():
+    from oracle.oracle import Oracle
+
+    from genasis_b200.adjoint import cell_volumes
+
+    name = "kh_noisy_hllc"
+    cfg, box, U0, dts = _setup(name)
+    g = _gradient(box, U0, dts)
+    dv = to_np(cell_volumes(box))
+    U0n = to_np(U0)
+
+    def rho(U):
+        o = Oracle(cfg)
+        o.set_conserved(_periodic_images(cfg, U))
+        for dt in dts:
+            o.step(dt)
+        return o.conserved()[0]
+
+    errs = []
+    for d in _directions(cfg, 4, seed=9):
+        fd = central_difference(rho, cfg, dv, U0n, d)
+        ad = float((g * d).sum())
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    assert max(errs) < RTOL, errs
+    box.close()
+
+
+def test_adjoint_recomputes_the_new_state_when_not_given():
+    import torch
+
+    from genasis_b200.adjoint import step_adjoint
+
+    cfg, box, U0, dts = _setup("random_hll_gravity", n_steps=1)
+    U1 = box.U.clone()
+    lam = torch.randn_like(U1)
+    a = step_adjoint(box, U0, dts[0], lam, U_np1=U1, detect_features=False)
+    b = step_adjoint(box, U0, dts[0], lam, U_np1=None, detect_features=False)
+    torch.cuda.synchronize()
+    assert np.array_equal(to_np(a), to_np(b))
+    box.close()
