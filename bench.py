@@ -47,9 +47,12 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="cells per axis of the sine wave")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="sine", choices=["sine", "bricks"],
+    ap.add_argument("--workload", default="sine", choices=["sine", "bricks", "adjoint"],
                     help="sine: the 256^3 headline; bricks: 512 uneven bricks, batched "
-                         "launch against a loop of per-brick launches")
+                         "launch against a loop of per-brick launches; adjoint: 128^3 "
+                         "Kelvin-Helmholtz, adjoint against forward and finite differences")
+    ap.add_argument("--directions", type=int, default=64,
+                    help="adjoint workload: finite-difference directions")
     ap.add_argument("--bricks", type=int, default=512)
     return ap.parse_args()
 
@@ -388,12 +391,169 @@ def run_bricks(args):
     batch.close()
 
 
+def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=None):
+    """Central differences (J(U0 + eps d) - J(U0 - eps d)) / (2 eps), J = sum
+    rho^2 dV, along seeded unit directions over all six fields of the proper
+    cells, formed cell by cell; returns the relative errors of the adjoint's
+    directional derivatives."""
+    import torch
+
+    from genasis_b200.adjoint import run_forward
+
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    p = (slice(None),) + cfg.proper
+    if rho_fn is None:
+        def rho_fn(U):
+            return run_forward(box, U, dts, False, keep=False)[0][0]
+    errs = []
+    for _ in range(directions):
+        d = torch.zeros_like(U0)
+        d[p] = torch.randn(d[p].shape, generator=gen, device="cuda", dtype=torch.float64)
+        d /= torch.linalg.vector_norm(d)
+        rp = rho_fn(U0 + eps * d)
+        rm = rho_fn(U0 - eps * d)
+        q = cfg.proper
+        fd = float(((rp[q] - rm[q]) * (rp[q] + rm[q]) * dv[q]).sum() / (2.0 * eps))
+        ad = float((grad * d).sum())
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    return errs
+
+
+def run_adjoint_workload(args):
+    """128^3 periodic Kelvin-Helmholtz (density 2 / 1, shear +-0.5, vy =
+    0.01 sin(4 pi x) + 1e-3 seeded noise, p = 2.5), PLM + HLLC, RK2, CFL 0.8,
+    20 steps; J = sum rho^2 dV at the final time.  Times the forward run with
+    per-step checkpoints against the adjoint run (stage recomputation), then
+    checks the gradient against central differences (eps = 1e-6) along 64
+    seeded directions, on this exact state and on the same state with 2e-2
+    noise on every field."""
+    import numpy as np
+    import torch
+
+    from genasis_b200 import problems
+    from genasis_b200.adjoint import cell_volumes, run_adjoint, run_forward
+    from genasis_b200.fluid import FluidBox
+
+    torch.cuda.set_device(0)
+    n, n_steps = args.n if args.n != 256 else 128, 20
+    out = {}
+    for variant in ("spec", "noisy"):
+        cfg, prim = problems.kelvin_helmholtz(n)
+        if variant == "noisy":
+            prim = problems.noisy(prim, amp=2e-2, seed=20261205)
+        box = FluidBox(cfg)
+        box.compute_from_primitive(prim)
+        box.compute_from_conserved()
+        U0 = box.U.clone()
+        dts = []
+        for i in range(n_steps):
+            dts.append(box.compute_time_step(i))
+            box.step(dts[-1])
+        dv = cell_volumes(box)
+        launches0 = box.kernel_launches()
+        fwd, adj, fwd_plain = [], [], []
+        for rep in range(max(args.warmup, 3) + 3):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            torch.cuda.synchronize()
+            e[0].record()
+            final, cps = run_forward(box, U0, dts, False)
+            e[1].record()
+            lam = torch.zeros_like(final)
+            lam[0] = 2.0 * final[0] * dv
+            grad = run_adjoint(box, cps, dts, lam, False)
+            e[2].record()
+            run_forward(box, U0, dts, False, keep=False)
+            e[3].record()
+            torch.cuda.synchronize()
+            if rep >= max(args.warmup, 3):
+                fwd.append(e[0].elapsed_time(e[1]))
+                adj.append(e[1].elapsed_time(e[2]))
+                fwd_plain.append(e[2].elapsed_time(e[3]))
+            del cps
+        launches = box.kernel_launches() - launches0
+        errs = _fd_check(box, cfg, U0, dts, grad, dv, args.directions, seed=20261205)
+        errs_np = np.array(errs)
+        entry = {
+            "forward_ms": statistics.median(fwd), "adjoint_ms": statistics.median(adj),
+            "forward_no_checkpoints_ms": statistics.median(fwd_plain),
+            "adjoint_over_forward": statistics.median(adj) / statistics.median(fwd),
+            "fd_directions": len(errs), "fd_within_1e-6": int((errs_np <= 1e-6).sum()),
+            "fd_median_rel_err": float(np.median(errs_np)),
+            "fd_max_rel_err": float(errs_np.max()),
+        }
+        if variant == "noisy":
+            # the same check at larger eps: at eps = 1e-6 a unit direction over
+            # all 6 x n^3 values moves each value by ~1e-10, close to the
+            # rounding floor of the differenced states
+            sweep = {}
+            for eps in (1e-5, 1e-4):
+                e_s = np.array(_fd_check(box, cfg, U0, dts, grad, dv, 16, seed=20261207, eps=eps))
+                sweep["%g" % eps] = {"directions": 16, "within_1e-6": int((e_s <= 1e-6).sum()),
+                                     "median_rel_err": float(np.median(e_s)),
+                                     "max_rel_err": float(e_s.max())}
+            entry["fd_eps_sweep"] = sweep
+        if variant == "noisy" and not args.no_cpu_baseline:
+            # the reference-FD gradient: the oracle's step, on a 32^3 brick of
+            # the same noisy state, 4 directions
+            from oracle.oracle import Oracle
+
+            cfg_s, prim_s = problems.kelvin_helmholtz(32)
+            prim_s = problems.noisy(prim_s, amp=2e-2, seed=20261205)
+            bs = FluidBox(cfg_s)
+            bs.compute_from_primitive(prim_s)
+            bs.compute_from_conserved()
+            U0s = bs.U.clone()
+            dts_s = []
+            for i in range(n_steps):
+                dts_s.append(bs.compute_time_step(i))
+                bs.step(dts_s[-1])
+            final_s, cps_s = run_forward(bs, U0s, dts_s, False)
+            dvs = cell_volumes(bs)
+            lam_s = torch.zeros_like(final_s)
+            lam_s[0] = 2.0 * final_s[0] * dvs
+            grad_s = run_adjoint(bs, cps_s, dts_s, lam_s, False)
+            idx = [(np.arange(36) - 2) % 32 + 2] * 3
+
+            def rho_oracle(U):
+                Un = U.cpu().numpy()[:, idx[0]][:, :, idx[1]][:, :, :, idx[2]]
+                o = Oracle(cfg_s)
+                o.set_conserved(np.ascontiguousarray(Un))
+                for dt in dts_s:
+                    o.step(dt)
+                return torch.as_tensor(o.conserved()[0], device="cuda")
+
+            e_ref = _fd_check(bs, cfg_s, U0s, dts_s, grad_s, dvs, 4, seed=20261206,
+                              rho_fn=rho_oracle)
+            entry["oracle_fd_32cubed"] = {"directions": 4, "max_rel_err": max(e_ref)}
+            bs.close()
+        out[variant] = entry
+        box.close()
+    spec = out["spec"]
+    line = {
+        "metric": "adjoint/forward cost", "value": spec["adjoint_over_forward"],
+        "unit": "x (adjoint ms / forward ms)", "n_gpus": 1, "steps": n_steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": spec["adjoint_ms"] / n_steps,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "kelvin_helmholtz_%d_adjoint" % n, "riemann": "HLLC",
+                   "boundary": "periodic", "cfl": 0.8, "steps": n_steps,
+                   "objective": "sum rho^2 dV", "checkpointing": "per step",
+                   "fd_eps": 1e-6, "fd_seed": 20261205},
+        "spec_state": spec, "noisy_state": out["noisy"],
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "bricks":
         run_bricks(args)
+    elif args.workload == "adjoint":
+        run_adjoint_workload(args)
     else:
         run_ours(args)
 

@@ -59,7 +59,7 @@ __device__ __forceinline__ void adj_flush(const AdjDesc& A, int D, long long bas
 }
 
 template <int D, bool HLLC>
-__global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ AdjDesc A,
+__global__ void __launch_bounds__(128, 3) adj_face_kernel(const __grid_constant__ AdjDesc A,
                                                        const __grid_constant__ Phys ph) {
   constexpr int T1 = (D == 0) ? 1 : 0;
   constexpr int T2 = (D == 2) ? 1 : 2;
@@ -85,32 +85,38 @@ __global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ A
     const long long sD = st[D];
     const int s0 = seg * A.seg, s1 = min(nD + 1, s0 + A.seg);
     // coefficient of the face fluxes in a cell's increment: dt A / V = dt / width
-    auto coef = [&](int c) { return A.dt / __ldg(G.W + c + 2) * A.kscale; };
-    auto slope = [&](const double* vm, const double* v0, const double* vp, int c,
-                     double* out) {
+    auto coef = [&](int c) { return A.dt * __ldg(G.RW + c + 2) * A.kscale; };
+    // forward slopes of a cell, with the limiter branch of each field (2 bits)
+    auto slope = [&](const double* vm, const double* v0, const double* vp, int c, double* out,
+                     int& branches) {
       const int tt = c + 2;
       const double dxl = __ldg(G.dXI + tt), dxr = __ldg(G.dXI + tt + 1);
       const double sql = __ldg(G.SQ + tt), sqr = __ldg(G.SQ + tt + 1), cden = __ldg(G.CDEN + tt);
       const double rdxl = __ldg(G.RDXI + tt), rdxr = __ldg(G.RDXI + tt + 1),
                    rcden = __ldg(G.RCDEN + tt);
-#pragma unroll
-      for (int q = 0; q < 5; ++q)
-        out[q] = limited_slope(vm[q], v0[q], vp[q], dxl, dxr, sql, sqr, cden, rdxl, rdxr, rcden,
-                               ph.theta, ph.use_limiter);
-    };
-    auto slope_back = [&](const double* vm, const double* v0, const double* vp, int c,
-                          const double* ls, double* am, double* a0, double* ap) {
-      const int tt = c + 2;
-      const double dxl = __ldg(G.dXI + tt), dxr = __ldg(G.dXI + tt + 1);
-      const double sql = __ldg(G.SQ + tt), sqr = __ldg(G.SQ + tt + 1), cden = __ldg(G.CDEN + tt);
+      branches = 0;
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        if (ls[q] == 0.0) continue;
-        const SlopePartials p = slope_partials(vm[q], v0[q], vp[q], dxl, dxr, sql, sqr, cden,
-                                               ph.theta, ph.use_limiter);
-        am[q] += p.m * ls[q];
-        a0[q] += p.c * ls[q];
-        ap[q] += p.p * ls[q];
+        int br;
+        out[q] = limited_slope_branch(vm[q], v0[q], vp[q], dxl, dxr, sql, sqr, cden, rdxl, rdxr,
+                                      rcden, ph.theta, ph.use_limiter, br);
+        branches |= br << (2 * q);
+      }
+    };
+    // adjoint of the slopes of cell c into its stencil cells c - 1, c, c + 1
+    auto slope_back = [&](int branches, int c, const double* ls, double* am, double* a0,
+                          double* ap) {
+      const int tt = c + 2;
+      const double sql = __ldg(G.SQ + tt), sqr = __ldg(G.SQ + tt + 1);
+      const double rdxl = __ldg(G.RDXI + tt), rdxr = __ldg(G.RDXI + tt + 1),
+                   rcden = __ldg(G.RCDEN + tt);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double gl, gr;
+        slope_coeffs((branches >> (2 * q)) & 3, sql, sqr, rdxl, rdxr, rcden, ph.theta, gl, gr);
+        am[q] -= gl * ls[q];
+        a0[q] += (gl - gr) * ls[q];
+        ap[q] += gr * ls[q];
       }
     };
     auto load_lamk = [&](int c, double* out) {
@@ -129,10 +135,11 @@ __global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ A
     double sm1[5], s0v[5];
     double am2[5], am1[5], a0[5];
     double lsm1[5], lkm1[5], lk0[5];
+    int bm1, b0;  // limiter branches of slope(i - 1), slope(i)
     adj_load(A, D, base, sD, s0 - 2, wm2);
     adj_load(A, D, base, sD, s0 - 1, wm1);
     adj_load(A, D, base, sD, s0, w0);
-    slope(wm2, wm1, w0, s0 - 1, sm1);
+    slope(wm2, wm1, w0, s0 - 1, sm1, bm1);
     load_lamk(s0 - 1, lkm1);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
@@ -143,7 +150,7 @@ __global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ A
     }
     for (int i = s0; i < s1; ++i) {
       adj_load(A, D, base, sD, i + 1, wp1);
-      slope(wm1, w0, wp1, i, s0v);
+      slope(wm1, w0, wp1, i, s0v, b0);
       const double wr = __ldg(G.WR + i + 1), wl = __ldg(G.WL + i + 2);
       double l[5], r[5];
 #pragma unroll
@@ -172,8 +179,9 @@ __global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ A
         ls0[q] = -wl * lr[q];
       }
       // slope(i - 1) has all of this segment's contributions
-      slope_back(wm2, wm1, w0, i - 1, lsm1, am2, am1, a0);
+      slope_back(bm1, i - 1, lsm1, am2, am1, a0);
       adj_flush(A, D, base, sD, i - 2, am2);
+      bm1 = b0;
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
         wm2[q] = wm1[q];
@@ -188,7 +196,7 @@ __global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ A
       }
     }
     // the last slope of the segment: cells s1 - 2, s1 - 1, s1
-    slope_back(wm2, wm1, w0, s1 - 1, lsm1, am2, am1, a0);
+    slope_back(bm1, s1 - 1, lsm1, am2, am1, a0);
     adj_flush(A, D, base, sD, s1 - 2, am2);
     adj_flush(A, D, base, sD, s1 - 1, am1);
     adj_flush(A, D, base, sD, s1, a0);
@@ -197,13 +205,19 @@ __global__ void __launch_bounds__(128) adj_face_kernel(const __grid_constant__ A
 
 // Primitives of the proper cells of U (ghost layout) into a compact array:
 // the stage-1 input W0 of the step.
+__device__ __forceinline__ long long ghost_index(const Box& b, long long c) {
+  // proper-cell counts stay below 2^31 (gfx_fluid_step_adjoint checks), so
+  // 32-bit division
+  const unsigned cc = (unsigned)c, n0 = (unsigned)b.n[0], n1 = (unsigned)b.n[1];
+  const unsigned r = cc / n0, i = cc - r * n0, k = r / n1, j = r - k * n1;
+  return (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
+}
+
 __global__ void adj_prims_kernel(Box b, Phys ph, const double* __restrict__ U,
                                  double* __restrict__ W) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
        c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % b.n[0]), j = (int)((c / b.n[0]) % b.n[1]),
-              k = (int)(c / ((long long)b.n[0] * b.n[1]));
-    const long long g = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
+    const long long g = ghost_index(b, c);
     Cons u{U[g], U[b.nV + g], U[2 * b.nV + g], U[3 * b.nV + g], U[4 * b.nV + g]};
     Prim w;
     cons_to_prim(u, w, ph.nmin);
@@ -213,12 +227,6 @@ __global__ void adj_prims_kernel(Box b, Phys ph, const double* __restrict__ U,
     W[3 * b.nP + c] = w.V3;
     W[4 * b.nP + c] = w.E;
   }
-}
-
-__device__ __forceinline__ long long ghost_index(const Box& b, long long c) {
-  const int i = (int)(c % b.n[0]), j = (int)((c / b.n[0]) % b.n[1]),
-            k = (int)(c / ((long long)b.n[0] * b.n[1]));
-  return (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
 }
 
 // lamZ = final^T lam^n+1 at the primitives of U^n+1 (both ghost layout).

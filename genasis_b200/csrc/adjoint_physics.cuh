@@ -15,51 +15,56 @@
 
 namespace gfx {
 
-// Partial derivatives of limited_slope(vm, v0, vp) with respect to vm, v0,
-// vp on the branch the forward takes (Gradient_Kernel.f90:176-180):
-// slope = s min(|theta dV_L| / dX_L, |theta dV_R| / dX_R, |num| / cden).
-struct SlopePartials {
-  double m, c, p;
-};
-
-__device__ __forceinline__ SlopePartials slope_partials(double vm, double v0, double vp,
-                                                        double dxl, double dxr, double sql,
-                                                        double sqr, double cden, double theta,
-                                                        int use_limiter) {
-  SlopePartials r{0.0, 0.0, 0.0};
-  const double dvl = v0 - vm, dvr = vp - v0;
+// limited_slope (the same value, bit for bit) together with the branch it
+// took: 0 = zero slope (signs differ, or s == 0), 1 = |theta dV_L| / dX_L,
+// 2 = |theta dV_R| / dX_R, 3 = the centred difference.  On that branch the
+// slope is linear in (dV_L, dV_R) with the coefficients of slope_coeffs:
+// s sign(dV_L) = s sign(dV_R) = s sign(num) = 1 whenever s != 0.
+__device__ __forceinline__ double limited_slope_branch(double vm, double v0, double vp,
+                                                       double dxl, double dxr, double sql,
+                                                       double sqr, double cden, double rdxl,
+                                                       double rdxr, double rcden, double theta,
+                                                       int use_limiter, int& branch) {
+  const double dvl = v0 - vm;
+  const double dvr = vp - v0;
   const double num = sqr * dvl + sql * dvr;
-  double gl = 0.0, gr = 0.0;  // d slope / d dV_L, d slope / d dV_R
   if (!use_limiter) {
-    gl = sqr / cden;
-    gr = sql / cden;
-  } else {
-    const double s = copysign(0.5, dvl) + copysign(0.5, dvr);
-    if (s == 0.0) return r;
-    const double c1 = fabs(theta * dvl / dxl), c2 = fabs(theta * dvr / dxr);
-    const double c3 = fabs(num / cden);
-    // fmin3's argument order: the first of equal candidates wins
-    int arg = 1;
-    double best = c1;
-    if (c2 < best) {
-      best = c2;
-      arg = 2;
-    }
-    if (c3 < best) arg = 3;
-    if (arg == 1) {
-      gl = s * copysign(theta, theta * dvl) / dxl;
-    } else if (arg == 2) {
-      gr = s * copysign(theta, theta * dvr) / dxr;
-    } else {
-      const double sg = copysign(1.0, num);
-      gl = s * sg * sqr / cden;
-      gr = s * sg * sql / cden;
-    }
+    branch = 3;
+    return div_rn(num, cden, rcden);
   }
-  r.m = -gl;
-  r.c = gl - gr;
-  r.p = gr;
-  return r;
+  const double s = copysign(0.5, dvl) + copysign(0.5, dvr);
+  const double a1 = fabs(theta * dvl), a2 = fabs(theta * dvr), a3 = fabs(num);
+  const double t1 = a1 * rdxl, t2 = a2 * rdxr, t3 = a3 * rcden;
+  const bool p12 = t1 <= t2;
+  double tm = p12 ? t1 : t2, tr = p12 ? t2 : t1;
+  double am = p12 ? a1 : a2, bm = p12 ? dxl : dxr, rm = p12 ? rdxl : rdxr;
+  const bool p3 = t3 < tm;
+  tr = p3 ? tm : fmin(tr, t3);
+  tm = p3 ? t3 : tm;
+  am = p3 ? a3 : am;
+  bm = p3 ? cden : bm;
+  rm = p3 ? rcden : rm;
+  const double q = markstein(am, bm, rm);
+  const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && quotient_in_range(am, rm);
+  branch = (s == 0.0) ? 0 : (p3 ? 3 : (p12 ? 1 : 2));
+  if (s == 0.0) return 0.0;
+  return fast ? s * q : limited_slope_ieee(dvl, dvr, dxl, dxr, sql, sqr, cden, theta);
+}
+
+// d slope / d dV_L (gl) and d slope / d dV_R (gr) on a branch.
+__device__ __forceinline__ void slope_coeffs(int branch, double sql, double sqr, double rdxl,
+                                             double rdxr, double rcden, double theta,
+                                             double& gl, double& gr) {
+  gl = 0.0;
+  gr = 0.0;
+  if (branch == 1) {
+    gl = theta * rdxl;
+  } else if (branch == 2) {
+    gr = theta * rdxr;
+  } else if (branch == 3) {
+    gl = sqr * rcden;
+    gr = sql * rcden;
+  }
 }
 
 // Adjoint of one face state (face_state<5>): given the adjoints of D, S1..3,
@@ -82,10 +87,11 @@ __device__ __forceinline__ void face_state_adjoint(const double* w, const FaceSt
          a.G * 0.5 * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
   }
   double lE = a.G + ph.gm1 * a.P;
-  if (s.CS > 0.0) {
-    // CS = sqrt(gamma P / N): dCS/dP = gamma / (2 N CS), dCS/dN = -CS / (2 N)
-    lE += a.CS * ph.gamma * ph.gm1 / (2.0 * N * s.CS);
-    lN += -a.CS * s.CS / (2.0 * N);
+  if (s.CS > 0.0 && a.CS != 0.0) {
+    // CS = sqrt(gamma (gamma - 1) E / N): dCS/dE = CS / (2 E), dCS/dN = -CS / (2 N)
+    const double r = 0.5 * s.CS / (N * w[4]);
+    lE += a.CS * r * N;
+    lN += -a.CS * r * w[4];
   }
   lw[0] = lN;
 #pragma unroll
@@ -244,7 +250,7 @@ __device__ __forceinline__ void flux_adjoint(const double* l, const double* r, b
       // AC = SN m, m = max(MD, 0) / max(MD^2, tiny)
       const double lSN = lAC * m;
       double dm = 0.0;
-      if (MD > 0.0) dm = (MD * MD > kTiny) ? -1.0 / (MD * MD) : 1.0 / kTiny;
+      if (MD > 0.0) dm = (MD * MD > kTiny) ? -m * m : 1.0 / kTiny;
       const double lMD = lAC * SN * dm;
       // MD = AP R.D + AM L.D - fdr + fdl
       lAP += lMD * R.D;
@@ -288,14 +294,14 @@ __device__ __forceinline__ void flux_adjoint(const double* l, const double* r, b
     FR[4] = (R.G + R.P) * vr;
     const double sum = AP + AM;
     const bool live = sum > kTiny;
-    const double den = live ? sum : kTiny;
+    const double rden = 1.0 / (live ? sum : kTiny);
     double lden = 0.0;
     double lFL[5], lFR[5];
 #pragma unroll
     for (int u = 0; u < 5; ++u) {
       const double num = AP * FL[u] + AM * FR[u] - AP * AM * (UR[u] - UL[u]);
-      const double ln = lF[u] / den;
-      if (live) lden += -lF[u] * num / (den * den);
+      const double ln = lF[u] * rden;
+      if (live) lden += -ln * num * rden;
       lAP += ln * (FL[u] - AM * (UR[u] - UL[u]));
       lAM += ln * (FR[u] - AP * (UR[u] - UL[u]));
       lFL[u] = AP * ln;

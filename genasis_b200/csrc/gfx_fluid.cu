@@ -1407,6 +1407,8 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   cudaStream_t s = (cudaStream_t)stream;
   const Box& b = h->box;
+  if (b.nP >= (1LL << 31))
+    return fail(GFX_ERR_UNSUPPORTED, "adjoint: %lld proper cells (at most 2^31 - 1)", b.nP);
   const size_t nP = (size_t)b.nP, nV = (size_t)b.nV;
   if (!h->adj) {
     if (cudaMalloc(&h->adj, 20 * nP * sizeof(double)) != cudaSuccess)

@@ -132,9 +132,16 @@ static void check_slope(Tally& t, int use_limiter) {
   };
   const double h = 1e-7;
   const double fd = (S(h) - S(-h)) / (2 * h);
-  const SlopePartials p =
-      slope_partials(v[0], v[1], v[2], dxl, dxr, sql, sqr, cden, 1.4, use_limiter);
-  t.add(fd, p.m * dv[0] + p.c * dv[1] + p.p * dv[2]);
+  int branch;
+  const double s0 = limited_slope_branch(v[0], v[1], v[2], dxl, dxr, sql, sqr, cden, rdxl,
+                                         rdxr, rcden, 1.4, use_limiter, branch);
+  if (s0 != S(0.0)) {  // the branch-recording slope must be the forward's, bit for bit
+    t.add(1.0, 0.0);
+    return;
+  }
+  double gl, gr;
+  slope_coeffs(branch, sql, sqr, rdxl, rdxr, rcden, 1.4, gl, gr);
+  t.add(fd, -gl * dv[0] + (gl - gr) * dv[1] + gr * dv[2]);
 }
 
 static void check_c2p(Tally& t) {
