@@ -47,12 +47,17 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="cells per axis of the sine wave")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="sine", choices=["sine", "bricks", "adjoint"],
+    ap.add_argument("--workload", default="sine",
+                    choices=["sine", "bricks", "adjoint", "adjoint_step", "rt"],
                     help="sine: the 256^3 headline; bricks: 512 uneven bricks, batched "
                          "launch against a loop of per-brick launches; adjoint: 128^3 "
                          "Kelvin-Helmholtz, adjoint against forward and finite differences")
     ap.add_argument("--directions", type=int, default=64,
                     help="adjoint workload: finite-difference directions")
+    ap.add_argument("--adjoint-steps", type=int, default=10,
+                    help="rt workload: steps of the adjoint run at the end")
+    ap.add_argument("--full-crossing", action="store_true",
+                    help="sine workload: also run to t = 1 (one crossing) for the L1 error")
     ap.add_argument("--bricks", type=int, default=512)
     return ap.parse_args()
 
@@ -142,14 +147,22 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest x over the ranks (the slowest replica's time)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(cells, steps, ms_per_rank, world):
+    """Whole-job cell-updates/s of independent replicas: every rank's cells
+    over the slowest rank's time."""
+    return world * cells * steps / (max_over_ranks(ms_per_rank, world) / 1000.0)
 
 
 def cpu_step_rate(n, steps, warmup=1):
@@ -249,7 +262,24 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     ms_max = max_over_ranks(ms, world)
     steps_done = cyc2 - cyc
-    value = world * cells * steps_done / (ms_max / 1000.0)
+    value = replica_rate(cells, steps_done, ms, world)
+
+    # L1 density error against the exact translated profile at the end of the timed
+    # region (before the extra steps below move the state on)
+    prim_t, _ = box.compute_from_conserved(primitive=True)
+    exact = problems.sine_density(cfg, t_sim)
+    l1 = problems.l1_error(prim_t[0].cpu().numpy(), exact, cfg)
+    del prim_t
+    crossing = None
+    if args.full_crossing:
+        # on to t = 1 (one box crossing), the last step cut to land on it
+        t_end, c_end = box.evolve(1.0, t_sim, cyc2)
+        torch.cuda.synchronize()
+        prim_t, _ = box.compute_from_conserved(primitive=True)
+        crossing = {"time": t_end, "cycles": c_end,
+                    "l1_density_error": problems.l1_error(
+                        prim_t[0].cpu().numpy(), problems.sine_density(cfg, t_end), cfg)}
+        del prim_t
 
     # per-kernel device times of the fused stages (CUDA events per launch)
     dt = box.compute_time_step(cyc2)
@@ -273,11 +303,6 @@ def run_ours(args):
                 "kernel_ms": avg,
                 "step_hbm_frac": STEP_BYTES * value / world / 1e9 / peak}
 
-    # L1 density error against the exact translated profile at the final time
-    prim_t, _ = box.compute_from_conserved(primitive=True)
-    exact = problems.sine_density(cfg, t_sim)
-    l1 = problems.l1_error(prim_t[0].cpu().numpy(), exact, cfg)
-    del prim_t
 
     # end to end: H2D of the state from pinned host memory, the step, D2H
     e2e = None
@@ -313,7 +338,8 @@ def run_ours(args):
                        "cfl": 0.8, "rk": 2, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (state %.0f MB)" % (
                            6 * box.n_values * 8 / 1e6),
-                       "l1_density_error": l1, "sim_time": t_sim},
+                       "l1_density_error": l1, "sim_time": t_sim,
+                       "full_crossing": crossing},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -345,6 +371,13 @@ def run_bricks(args):
     cells = sum(c.n_proper for c in cfgs)
     batch = FluidBatch(cfgs)
     K = args.steps
+    # the pencil length of the batch's work items: autotuned (cached per GPU
+    # and brick set), outside the timed region
+    from genasis_b200 import autotune
+
+    t_tune = time.perf_counter()
+    z_chunk, tune_ms, from_cache = autotune.tune_batch(batch, prims)
+    t_tune = time.perf_counter() - t_tune
     # warm-up (graph capture) on a copy of the initial states, then reset
     batch.set_primitives(prims)
     batch.evolve(n_cycles=max(args.warmup, 2))
@@ -384,11 +417,151 @@ def run_bricks(args):
         "plain_loop": {"value": cells * K / t_plain, "ms_per_step": 1000.0 * t_plain / K,
                        "gpu_launches": launches_plain},
         "speedup_vs_plain_loop": t_plain / t_batch,
+        "autotune": {"z_chunk": z_chunk, "ms_per_cycle_by_candidate": tune_ms,
+                     "from_cache": from_cache, "tuning_s": t_tune},
         "bitwise_equal_to_plain": same,
         "gpu_launches": launches_batch,
     }
     print(json.dumps(line), flush=True)
     batch.close()
+
+
+def stage_roofline(box, cells, dt, n):
+    """CUDA-event times of the phases of n steps (gfx_fluid_step_timed) and
+    the roofline of the dominant stage kernel."""
+    per = {"features": [], "stage1": [], "stage2": [], "ghosts": []}
+    for _ in range(n):
+        f, s1, s2, gh = box.step_timed(dt)
+        per["features"].append(f)
+        per["stage1"].append(s1)
+        per["stage2"].append(s2)
+        per["ghosts"].append(gh)
+    avg = {k: sum(v) / len(v) for k, v in per.items()}
+    dom = max(("stage1", "stage2"), key=lambda k: avg[k])
+    peak, peak_kind = peaks()
+    achieved = STAGE_BYTES[dom] * cells / (avg[dom] / 1000.0) / 1e9
+    return {"bound": "hbm", "kernel": "stage_kernel (%s)" % dom, "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_per_launch(dom, cells), "peak_source": peak_kind,
+            "algorithmic_bytes_per_cell": STAGE_BYTES[dom], "avg_launch_ms": avg[dom],
+            "kernel_ms": avg}
+
+
+def run_adjoint_step(args):
+    """A short run for profiling the adjoint: the n^3 Kelvin-Helmholtz state
+    (default 128^3), two forward steps, then --steps calls of
+    gfx_fluid_step_adjoint on the last step (U^n+1 given, features detected),
+    timed with CUDA events."""
+    import torch
+
+    from genasis_b200 import problems
+    from genasis_b200.adjoint import cell_volumes, step_adjoint
+    from genasis_b200.fluid import FluidBox
+
+    torch.cuda.set_device(0)
+    n = args.n if args.n != 256 else 128
+    cfg, prim = problems.kelvin_helmholtz(n)
+    box = FluidBox(cfg)
+    box.compute_from_primitive(prim)
+    box.compute_from_conserved()
+    dts = []
+    for i in range(2):
+        dts.append(box.compute_time_step(i))
+        box.step(dts[-1])
+    U0 = box.U.clone()
+    box.step(dts[-1])
+    U1 = box.U.clone()
+    lam = torch.zeros_like(U1)
+    lam[0] = 2.0 * U1[0] * cell_volumes(box)
+    out = torch.empty_like(U1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        step_adjoint(box, U0, dts[-1], lam, out, U1, True)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"workload": "kelvin_helmholtz_%d_adjoint_step" % n, "steps": args.steps,
+                      "ms_per_adjoint_step": e0.elapsed_time(e1) / args.steps}), flush=True)
+    box.close()
+
+
+def run_rt(args):
+    """3-D Rayleigh-Taylor on 384 x 384 x 768 cells ([0,0.5]^2 x [0,1]),
+    gravity 0.1 along -z as a source in the RK stages, periodic x / y,
+    reflecting z, PLM + HLLC, RK2, CFL 0.8: throughput over --steps cycles
+    with the HBM roofline of the stage kernel and the mass balance, then the
+    adjoint of the last --adjoint-steps steps (per-step checkpoints, stage
+    recomputation) against the forward time of the same steps."""
+    import torch
+
+    from genasis_b200 import problems
+    from genasis_b200.adjoint import cell_volumes, run_adjoint, run_forward
+    from genasis_b200.fluid import FluidBox
+
+    torch.cuda.set_device(0)
+    cfg, prim = problems.rayleigh_taylor()
+    cells = cfg.n_proper
+    box = FluidBox(cfg)
+    box.compute_from_primitive(prim)
+    del prim
+    dv = cell_volumes(box)
+    p = cfg.proper
+    mass0 = float((box.U[0][p] * dv[p]).sum())
+    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(args.warmup, 3))
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    l0 = box.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = box.kernel_launches() - l0
+    ms = e0.elapsed_time(e1)
+    steps = cyc2 - cyc
+    mass1 = float((box.U[0][p] * dv[p]).sum())
+    dt = box.compute_time_step(cyc2)
+    roof = stage_roofline(box, cells, dt, 5)
+    adj = None
+    if args.adjoint_steps > 0:
+        U0 = box.U.clone()
+        dts = []
+        for i in range(args.adjoint_steps):
+            dts.append(box.compute_time_step(cyc2 + i))
+            box.step(dts[-1])
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        final, cps = run_forward(box, U0, dts, True)
+        e[1].record()
+        lam = torch.zeros_like(final)
+        lam[0] = 2.0 * final[0] * dv
+        grad = run_adjoint(box, cps, dts, lam, True)
+        e[2].record()
+        torch.cuda.synchronize()
+        adj = {"steps": len(dts), "forward_ms": e[0].elapsed_time(e[1]),
+               "adjoint_ms": e[1].elapsed_time(e[2]),
+               "adjoint_over_forward": e[1].elapsed_time(e[2]) / e[0].elapsed_time(e[1]),
+               "objective": "sum rho^2 dV", "gradient_finite": bool(torch.isfinite(grad).all())}
+        del cps, grad, final, lam, U0
+    value = cells * steps / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "rayleigh_taylor_384x384x768", "cells": cells,
+                   "riemann": "HLLC", "gravity": 0.1, "boundary": "periodic x/y, reflecting z",
+                   "cfl": 0.8, "sim_time": t_sim,
+                   "l2": "inputs larger than L2 (state %.1f GB)" % (6 * box.n_values * 8 / 1e9),
+                   "mass_rel_change": (mass1 - mass0) / mass0},
+        "roofline": roof, "step_hbm_frac": STEP_BYTES * value / 1e9 / roof["peak"],
+        "adjoint": adj, "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    box.close()
 
 
 def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=None):
@@ -554,6 +727,10 @@ def main():
         run_bricks(args)
     elif args.workload == "adjoint":
         run_adjoint_workload(args)
+    elif args.workload == "adjoint_step":
+        run_adjoint_step(args)
+    elif args.workload == "rt":
+        run_rt(args)
     else:
         run_ours(args)
 

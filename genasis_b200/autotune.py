@@ -1,0 +1,163 @@
+"""Project-written autotuner for speed knobs that leave results unchanged
+(bit for bit for the step; up to the rounding of unordered atomic additions
+for the adjoint).
+
+Knobs (gfx_fluid_set_tuning):
+  z_chunk          z length of the cell pencils a CTA of the stage kernel
+                   marches: longer pencils pay fewer prologues (the two
+                   planes of slopes below the pencil), shorter ones give the
+                   persistent grid more items to balance;
+  adjoint_segment  faces per thread in the adjoint's reverse sweep: longer
+                   segments re-load fewer window cells, shorter ones give
+                   more threads.
+
+Every candidate is timed with CUDA events on a seeded state; the fastest is
+kept in a JSON cache keyed by the GPU's name and a bucket of the problem
+(single brick: edges rounded up to a multiple of 16, solver, gravity; batch:
+the brick count and the sizes' digest).  The shipped cache, tuning/<GPU>.json,
+was measured on B200s; set GFX_TUNING_CACHE to use another file.
+"""
+import hashlib
+import json
+import os
+
+from . import problems
+from .fluid import FluidBox, _torch
+
+Z_CANDIDATES = (0, 8, 16, 32, 64)
+SEGMENT_CANDIDATES = (4, 8, 16, 32)
+BATCH_Z_CANDIDATES = (8, 16, 24, 32, 48, 64, 96)
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def gpu_name():
+    torch = _torch()
+    return torch.cuda.get_device_name().replace(" ", "_")
+
+
+def cache_path():
+    return os.environ.get("GFX_TUNING_CACHE",
+                          os.path.join(_HERE, "tuning", gpu_name() + ".json"))
+
+
+def load_cache():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def save_cache(cache):
+    path = cache_path()
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(cache, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def brick_key(cfg):
+    edges = "x".join(str(16 * ((int(n) + 15) // 16)) for n in cfg.n_cells)
+    grav = "g" if cfg.uniform_acceleration != 0.0 else "0"
+    return "brick:%s:%s:%s" % (edges, cfg.riemann_solver, grav)
+
+
+def batch_key(cfgs):
+    sizes = ",".join("x".join(str(int(n)) for n in c.n_cells) for c in cfgs)
+    digest = hashlib.sha1(sizes.encode()).hexdigest()[:12]
+    return "batch:%d:%s:%s" % (len(cfgs), cfgs[0].riemann_solver, digest)
+
+
+def _time(fn, reps):
+    torch = _torch()
+    fn()  # warm-up (graph capture, first-touch)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(reps):
+        fn()
+    end.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(end) / reps
+
+
+def tune_brick(cfg, reps=3, adjoint=True, seed=1):
+    """Times the step for every pencil length and (if adjoint) the adjoint
+    step for every segment on a seeded state of cfg's size; returns
+    {"z_chunk", "adjoint_segment", "ms": {...}}."""
+    torch = _torch()
+    from .adjoint import step_adjoint
+
+    box = FluidBox(cfg)
+    box.compute_from_primitive(problems.random_state(cfg, seed=seed, shocks=False))
+    box.compute_from_conserved()
+    U0 = box.U.clone()
+    dt = box.compute_time_step(0)
+    ms_z = {}
+    for z in Z_CANDIDATES:
+        box.set_tuning(z, 0)
+
+        def step():
+            box.U.copy_(U0)
+            box.step(dt)
+
+        ms_z[z] = _time(step, reps)
+    best_z = min(ms_z, key=ms_z.get)
+    box.set_tuning(best_z, 0)
+    best_seg, ms_s = 0, {}
+    if adjoint:
+        box.U.copy_(U0)
+        box.step(dt)
+        U1 = box.U.clone()
+        lam = torch.ones_like(U1)
+        out = torch.empty_like(U1)
+        for seg in SEGMENT_CANDIDATES:
+            box.set_tuning(best_z, seg)
+            ms_s[seg] = _time(lambda: step_adjoint(box, U0, dt, lam, out, U1, False), reps)
+        best_seg = min(ms_s, key=ms_s.get)
+    box.close()
+    return {"z_chunk": best_z, "adjoint_segment": best_seg,
+            "ms": {"step": {str(k): v for k, v in ms_z.items()},
+                   "adjoint": {str(k): v for k, v in ms_s.items()}}}
+
+
+def tuned_box(cfg, retune=False, adjoint=True):
+    """A FluidBox with the cached (or freshly tuned) knobs of cfg's bucket."""
+    cache = load_cache()
+    key = brick_key(cfg)
+    if retune or key not in cache:
+        cache[key] = tune_brick(cfg, adjoint=adjoint)
+        save_cache(cache)
+    box = FluidBox(cfg)
+    box.set_tuning(cache[key]["z_chunk"], cache[key]["adjoint_segment"])
+    return box
+
+
+def tune_batch(batch, prims, cycles=3, retune=False):
+    """Chooses the batch's pencil length by timing whole batched cycles for
+    every candidate (the persistent grid's balance depends on all bricks at
+    once, not on one brick alone); applies and caches it.  The bricks'
+    states are reset from prims afterwards.  Returns (z_chunk, ms per cycle
+    by candidate, from_cache)."""
+    cache = load_cache()
+    key = batch_key([b.config for b in batch.boxes])
+    if not retune and key in cache:
+        batch.set_pencil_length(cache[key]["z_chunk"])
+        batch.set_primitives(prims)
+        batch.set_clocks(0.0, 0)
+        return cache[key]["z_chunk"], cache[key]["ms"], True
+    ms = {}
+    batch.set_primitives(prims)
+    for z in BATCH_Z_CANDIDATES:
+        # the states keep evolving from candidate to candidate: the work of a
+        # cycle does not depend on them
+        batch.set_pencil_length(z)
+        ms[str(z)] = _time(lambda: batch.evolve(n_cycles=cycles), 2) / cycles
+    best = int(min(ms, key=ms.get))
+    cache[key] = {"z_chunk": best, "ms": ms}
+    save_cache(cache)
+    batch.set_pencil_length(best)
+    batch.set_primitives(prims)
+    batch.set_clocks(0.0, 0)
+    return best, ms, False

@@ -18,6 +18,15 @@ class FluidBatch:
         self.boxes = [FluidBox(c, device=device) for c in configs]
         self.h = None
 
+    def set_pencil_length(self, z_chunk):
+        """The z length of the cell pencils of every brick's work items (0 =
+        32 planes); rebuilds the batch's work list on its next use."""
+        for b in self.boxes:
+            b.set_tuning(z_chunk, getattr(b, "tuning", (0, 0))[1])
+        if self.h is not None:
+            lib.load().gfx_fluid_batch_destroy(self.h)
+            self.h = None
+
     def set_primitives(self, prims):
         for box, prim in zip(self.boxes, prims):
             box.compute_from_primitive(prim)

@@ -374,6 +374,26 @@ __global__ void advance_clock_kernel(Clock* __restrict__ clk, int n) {
   if (!(c.time < c.finish && c.cycle < c.max_cycle)) c.done = 1;
 }
 
+// Counts of proper cells holding a non-finite value in any field, and of
+// cells at the density floor, for gfx_fluid_check_state.
+__global__ void check_state_kernel(Box b, Phys ph, const double* __restrict__ U,
+                                   unsigned long long* __restrict__ counts) {
+  unsigned long long bad = 0, floor = 0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % b.n[0]), j = (int)((c / b.n[0]) % b.n[1]),
+              k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    const long long g = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
+    bool finite = true;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) finite &= isfinite(U[q * b.nV + g]);
+    bad += finite ? 0 : 1;
+    floor += (U[g] <= ph.nmin) ? 1 : 0;
+  }
+  if (bad) atomicAdd(counts, bad);
+  if (floor) atomicAdd(counts + 1, floor);
+}
+
 __global__ void reset_bits_kernel(unsigned long long* __restrict__ bits, int n, int* counter,
                                   int n_counters) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < n_counters;

@@ -149,6 +149,10 @@ struct gfx_fluid {
   double* adj = nullptr;
   uint8_t* adj_flags = nullptr;
   double* adj_U = nullptr;
+  // tuning (gfx_fluid_set_tuning; 0 = built-in default)
+  int z_chunk = 0;
+  int adjoint_segment = 0;
+  unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
 };
 
 namespace {
@@ -240,13 +244,15 @@ int validate(const gfx_fluid_config* c) {
 
 // Work list of one brick: TX x TY columns, cut along z into chunks so that the
 // persistent grid has several items per SM.
-std::vector<WorkItem> make_items(const int n[3], int brick) {
+// z_chunk > 0 fixes the pencil length instead (the autotuner's knob).
+std::vector<WorkItem> make_items(const int n[3], int brick, int z_chunk = 0) {
   const int cx = (n[0] + TX - 1) / TX, cy = (n[1] + TY - 1) / TY;
   const long long cols = (long long)cx * cy;
   const long long want = 16LL * num_sms();
   int chunks = (int)std::max(1LL, std::min<long long>(n[2] / 16, (want + cols - 1) / cols));
   if (chunks < 1) chunks = 1;
-  const int len = (n[2] + chunks - 1) / chunks;
+  int len = (n[2] + chunks - 1) / chunks;
+  if (z_chunk > 0) len = std::min(n[2], z_chunk);
   std::vector<WorkItem> v;
   for (int z = 0; z < n[2]; z += len)
     for (int y = 0; y < cy; ++y)
@@ -534,6 +540,7 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->adj);
   cudaFree(h->adj_flags);
   cudaFree(h->adj_U);
+  cudaFree(h->state_counts);
   if (h->host_stream) cudaStreamDestroy(h->host_stream);
   delete h;
   return GFX_OK;
@@ -868,9 +875,10 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
     bb[b].c_off = B->total_c;
     B->total_v += h->box.nV;
     B->total_c += h->box.nP;
-    // z chunks of 32 planes: few prologues, many items to balance
+    // z chunks of 32 planes (few prologues, many items to balance), or the
+    // brick's tuned pencil length
     const int* nn = h->box.n;
-    const int len = std::min(nn[2], 32);
+    const int len = std::min(nn[2], h->z_chunk > 0 ? h->z_chunk : 32);
     for (int z = 0; z < nn[2]; z += len)
       for (int y = 0; y < nn[1]; y += TY)
         for (int x = 0; x < nn[0]; x += TX) {
@@ -1033,9 +1041,53 @@ int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch* B, long long* count) 
   return GFX_OK;
 }
 
-int gfx_fluid_check_state(gfx_fluid* h, void* stream) {
+int gfx_fluid_check_state(gfx_fluid* h, const double* U, void* stream) {
+  if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h->state_counts &&
+      cudaMalloc(&h->state_counts, 2 * sizeof(unsigned long long)) != cudaSuccess)
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc state counters");
+  CUDA_TRY(cudaMemsetAsync(h->state_counts, 0, 2 * sizeof(unsigned long long), s));
+  check_state_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(h->box, h->ph, U,
+                                                               h->state_counts);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  unsigned long long c[2] = {0, 0};
+  CUDA_TRY(cudaMemcpyAsync(c, h->state_counts, sizeof(c), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (c[0] != 0)
+    return fail(GFX_ERR_STATE, "%llu proper cells hold non-finite values (%llu at the density "
+                "floor)", c[0], c[1]);
+  return GFX_OK;
+}
+
+int gfx_fluid_set_tuning(gfx_fluid* h, int z_chunk, int adjoint_segment) {
   if (!h) return fail(GFX_ERR_ARGUMENT, "NULL handle");
-  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  if (z_chunk < 0 || adjoint_segment < 0 || adjoint_segment > 4096)
+    return fail(GFX_ERR_ARGUMENT, "z_chunk = %d, adjoint_segment = %d", z_chunk,
+                adjoint_segment);
+  if (z_chunk != h->z_chunk) {
+    std::vector<WorkItem> items = make_items(h->box.n, 0, z_chunk);
+    WorkItem* d = nullptr;
+    if (cudaMalloc(&d, items.size() * sizeof(WorkItem)) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc work items");
+    if (cudaMemcpy(d, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice) !=
+        cudaSuccess) {
+      cudaFree(d);
+      return fail(GFX_ERR_CUDA, "copy work items");
+    }
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(h->items);
+    h->items = d;
+    h->n_items = (int)items.size();
+    // the cycle graph holds the old list
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    h->z_chunk = z_chunk;
+  }
+  h->adjoint_segment = adjoint_segment;
   return GFX_OK;
 }
 
@@ -1384,7 +1436,7 @@ int enqueue_adj_stage(gfx_fluid* h, const double* W, const double* lamK, double 
   A.dt = dt;
   A.kscale = kscale;
   const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
-  A.seg = 8;
+  A.seg = h->adjoint_segment > 0 ? h->adjoint_segment : 8;
   A.nseg = (h->box.n[0] + 1 + A.seg - 1) / A.seg;
   CUDA_TRY(launch_adj_face<0>(A, hllc, h->ph, s));
   A.nseg = (h->box.n[1] + 1 + A.seg - 1) / A.seg;

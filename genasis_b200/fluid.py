@@ -150,6 +150,16 @@ class FluidBox:
                  ms, _stream())
         return tuple(ms)
 
+    def set_tuning(self, z_chunk=0, adjoint_segment=0):
+        """Speed knobs that leave results unchanged (genasis_b200.autotune)."""
+        lib.call("gfx_fluid_set_tuning", self.h, int(z_chunk), int(adjoint_segment))
+        self.tuning = (int(z_chunk), int(adjoint_segment))
+
+    def check_state(self, U=None):
+        """Raises GfxError (GFX_ERR_STATE) if a proper cell of U (default: the
+        box's state) holds a non-finite value."""
+        lib.call("gfx_fluid_check_state", self.h, _ptr(self.U if U is None else U), _stream())
+
     def kernel_launches(self):
         n = ctypes.c_longlong()
         lib.call("gfx_fluid_kernel_launches", self.h, ctypes.byref(n))

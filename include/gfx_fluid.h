@@ -188,8 +188,10 @@ int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch *b, long long *count);
  * features of U_n (every step after the first), 0 if it ran on zero features
  * (the first step after initialisation).  The derivative is that of the
  * branch the forward step takes at every limiter, wave-speed maximum, HLLC
- * side and floor.  Allocates a workspace of 20 values per proper cell on the
- * first call.  lam_n_dev must not alias lam_np1_dev. */
+ * side and floor.  Cells shared by two threads' segments receive atomic
+ * additions in no fixed order, so repeated calls agree to rounding, not bit
+ * for bit.  Allocates a workspace of 20 values per proper cell on the first
+ * call.  lam_n_dev must not alias lam_np1_dev. */
 int gfx_fluid_step_adjoint(gfx_fluid *h, const double *U_n_dev, double dt,
                            const double *lam_np1_dev, double *lam_n_dev,
                            const double *U_np1_dev, int detect_features, void *stream);
@@ -220,10 +222,21 @@ int gfx_fluid_step_adjoint(gfx_fluid *h, const double *U_n_dev, double dt,
 int gfx_fluid_step_noalloc(const gfx_fluid_config *cfg, double *U_dev, double dt,
                            int detect_features, double *fluence_dev, void *stream);
 
-/* Bit pattern of the device-side error word accumulated by the kernels since
- * the last call (GFX_ERR_STATE if non-finite or non-positive density / energy
- * was produced); clears it.  Synchronises the stream. */
-int gfx_fluid_check_state(gfx_fluid *h, void *stream);
+/* Scans the proper cells of U_dev: GFX_ERR_STATE (with the counts in the
+ * error message) if any holds a non-finite value; the number of cells at the
+ * density floor is reported alongside.  The reference checks nothing here
+ * (its floors in Fluid_P__Kernel.f90:94-192 are silent).  Synchronises the
+ * stream. */
+int gfx_fluid_check_state(gfx_fluid *h, const double *U_dev, void *stream);
+
+/* Speed knobs (set by genasis_b200/autotune.py).  The step's results do not
+ * depend on them, bit for bit; the adjoint's change only by the rounding of
+ * its atomic additions, whose order is not fixed in any case:
+ * z_chunk = z length of the cell pencils a CTA marches in the stage kernel
+ * (0 = default: enough items for 16 per SM; a batch created afterwards takes
+ * it per brick, default 32); adjoint_segment = faces per thread in the
+ * adjoint's reverse sweep (0 = 8).  No counterpart in the reference. */
+int gfx_fluid_set_tuning(gfx_fluid *h, int z_chunk, int adjoint_segment);
 
 int gfx_fluid_last_error(char *buf, size_t len);
 

@@ -75,3 +75,53 @@ def test_invalid_configs_are_rejected_before_any_device_call():
         rc = lib.load().gfx_fluid_create(ctypes.byref(c), ctypes.byref(h))
         assert rc in (-1, -3), rc
         assert "n_" in lib.last_error() or "PERIODIC" in lib.last_error()
+
+
+def header_arg_counts():
+    """Arguments of every declared entry point (a void list counts 0)."""
+    text = open(os.path.join(ROOT, "include", "gfx_fluid.h")).read()
+    out = {}
+    for name, args in re.findall(r"\bint\s+(gfx_fluid_\w+)\s*\(([^)]*)\)", text):
+        args = args.strip()
+        out[name] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def fortran_interfaces():
+    """bind(c) name -> argument count of include/gfx_fluid_f.f90's interfaces."""
+    text = open(os.path.join(ROOT, "include", "gfx_fluid_f.f90")).read()
+    text = re.sub(r"&\s*\n\s*", " ", text)  # join continuation lines
+    out = {}
+    for args, name in re.findall(
+            r"function\s+\w+\s*\(([^)]*)\)\s*bind\s*\(\s*c\s*,\s*name\s*=\s*'(\w+)'", text):
+        out[name] = len([a for a in args.split(",") if a.strip()])
+    return out
+
+
+def test_fortran_binding_matches_the_header():
+    h = header_arg_counts()
+    f = fortran_interfaces()
+    assert set(f) == set(h), set(f) ^ set(h)
+    for name, n in h.items():
+        assert f[name] == n, (name, f[name], n)
+
+
+def test_fortran_config_type_has_the_c_layout():
+    """Offsets of GFX_FluidConfig's components under the C alignment rules
+    (which bind(c) types follow) equal those of the C struct."""
+    text = open(os.path.join(ROOT, "include", "gfx_fluid_f.f90")).read()
+    body = text.split("type, bind ( c ), public :: GFX_FluidConfig")[1].split("end type")[0]
+    size = {"c_int": 4, "c_double": 8}
+    off, offsets = 0, []
+    fields = re.findall(r"(?:integer|real) \( (c_int|c_double) \) :: (\w+)(?: \(([^)]*)\))?", body)
+    for kind, name, dims in fields:
+        n = 1
+        for d in (dims.split(",") if dims else []):
+            n *= int(d)
+        a = size[kind]
+        off = (off + a - 1) // a * a
+        offsets.append(off)
+        off += a * n
+    c_fields = [f[0] for f in GfxConfig._fields_]
+    assert len(fields) == len(c_fields)
+    assert offsets == [getattr(GfxConfig, f).offset for f in c_fields]
