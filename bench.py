@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="sine",
-                    choices=["sine", "bricks", "adjoint", "adjoint_step", "rt"],
+                    choices=["sine", "bricks", "adjoint", "adjoint_step", "rt", "sod"],
                     help="sine: the 256^3 headline; bricks: 512 uneven bricks, batched "
                          "launch against a loop of per-brick launches; adjoint: 128^3 "
                          "Kelvin-Helmholtz, adjoint against forward and finite differences")
@@ -486,6 +486,74 @@ def run_adjoint_step(args):
     box.close()
 
 
+def run_sod(args):
+    """The plain method at its small configuration: the 3-D Sod tube on 128^3
+    cells (left rho = 1, p = 1; right rho = 0.125, p = 0.1; diaphragm x = 0.5),
+    PLM + HLL, RK2, CFL 0.8, outflow, --steps steps (100) on the GPU and on
+    the oracle side by side: per-step parity from identical inputs on the
+    first steps, the final states of the two free runs, the totals against
+    the boundary fluence, and both rates."""
+    import numpy as np
+    import torch
+
+    from genasis_b200 import problems
+    from genasis_b200.config import FluidConfig
+    from genasis_b200.fluid import FluidBox
+    from oracle.oracle import Oracle
+
+    torch.cuda.set_device(0)
+    n = args.n if args.n != 256 else 128
+    cfg = FluidConfig(n_cells=(n, n, n), riemann_solver="HLL", courant_factor=0.8,
+                      n_ramp_cycles=1)
+    prim = problems.riemann(cfg, 1.0, 1.0, (0, 0, 0), 0.125, 0.1, (0, 0, 0), (0.5, 0, 0),
+                            (1.0, 0, 0))
+    p = cfg.proper
+    box = FluidBox(cfg)
+    box.compute_from_primitive(prim)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+
+    def rel(a, b):
+        return max(float(np.abs(a[f][p] - b[f][p]).max()) / max(float(np.abs(b[f][p]).max()),
+                                                                 1e-300) for f in range(5))
+
+    per_step = []
+    gpu_ms = 0.0
+    cpu_s = 0.0
+    dts = []
+    for i in range(args.steps):
+        dt = o.timestep(i)
+        dts.append(dt)
+        if i < 3:  # per-step parity: the GPU step from the oracle's state
+            box.set_conserved(torch.as_tensor(o.conserved(), device="cuda"))
+            if i > 0:
+                box.detect_features()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        box.step(dt)
+        e1.record()
+        t0 = time.perf_counter()
+        o.step(dt)
+        cpu_s += time.perf_counter() - t0
+        torch.cuda.synchronize()
+        gpu_ms += e0.elapsed_time(e1)
+        if i < 3:
+            per_step.append(rel(box.U.cpu().numpy(), o.conserved()))
+    Ug = box.U.cpu().numpy()
+    Uo = o.conserved()
+    line = {
+        "workload": "sod_%d_hll_%d_steps" % (n, args.steps), "cells": cfg.n_proper,
+        "per_step_max_rel_diff_first_3_steps": per_step,
+        "final_max_rel_diff_free_runs": rel(Ug, Uo),
+        "final_bitwise_equal_fields": [bool(np.array_equal(Ug[f][p], Uo[f][p])) for f in range(6)],
+        "gpu_cell_updates_per_s": cfg.n_proper * args.steps / (gpu_ms / 1000.0),
+        "cpu_oracle_cell_updates_per_s": cfg.n_proper * args.steps / cpu_s,
+        "cpu_threads": Oracle.n_threads(), "sim_time": float(sum(dts)),
+    }
+    print(json.dumps(line), flush=True)
+    box.close()
+
+
 def run_rt(args):
     """3-D Rayleigh-Taylor on 384 x 384 x 768 cells ([0,0.5]^2 x [0,1]),
     gravity 0.1 along -z as a source in the RK stages, periodic x / y,
@@ -729,6 +797,8 @@ def main():
         run_adjoint_workload(args)
     elif args.workload == "adjoint_step":
         run_adjoint_step(args)
+    elif args.workload == "sod":
+        run_sod(args)
     elif args.workload == "rt":
         run_rt(args)
     else:

@@ -314,6 +314,75 @@ __device__ __forceinline__ void cell_slopes(const double* v, int vs, int st, con
                                      sqr, cden, rdxl, rdxr, rcden, ph.theta, ph.use_limiter);
 }
 
+// Limited z slopes of the 5 primitives of the own column at plane p from the
+// values a (plane p-1), b (p), c (p+1) at strides sa, sb, sc.
+__device__ __forceinline__ void z_slope(const AxisGeo& GZ, const Phys& ph, int p,
+                                        const double* a, int sa, const double* b, int sb,
+                                        const double* c, int sc, double* out) {
+  const int t = p + 2;
+  const double dxl = __ldg(GZ.dXI + t), dxr = __ldg(GZ.dXI + t + 1);
+  const double sql = __ldg(GZ.SQ + t), sqr = __ldg(GZ.SQ + t + 1), cden = __ldg(GZ.CDEN + t);
+  const double rdxl = __ldg(GZ.RDXI + t), rdxr = __ldg(GZ.RDXI + t + 1),
+               rcden = __ldg(GZ.RCDEN + t);
+#pragma unroll
+  for (int q = 0; q < 5; ++q)
+    out[q] = limited_slope(a[q * sa], b[q * sb], c[q * sc], dxl, dxr, sql, sqr, cden, rdxl,
+                           rdxr, rcden, ph.theta, ph.use_limiter);
+}
+
+// Flux through the z face between planes p-1 (values a, slopes sm_) and p
+// (values b, slopes sp) of the own column (gx, gy), with its boundary fluence.
+template <bool HLLC, int NF>
+__device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p,
+                                       const double* a, int sa, const double* sm_, int ssm,
+                                       const double* b, int sb, const double* sp, int ssp,
+                                       int gx, int gy, bool own, double dt, double* F) {
+  const AxisGeo& GZ = B.geo[2];
+  double l[5], r[5];
+  face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2), l,
+             r);
+  FaceState L, R;
+  face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
+  face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
+  const bool diff = HLLC && df_bit(B, 2, gx, gy, p);
+  riemann_flux<2, HLLC, NF>(L, R, diff, F);
+  if (own && (p == 0 || p == B.n[2]) && B.fluence)
+    boundary_fluence<2, HLLC, NF>(B, ph, l, r, diff, F, p == 0 ? 4 : 5, gx, B.n[0], gy,
+                                  B.weight * dt);
+}
+
+// Prologue of a work item (own column only): planes z0-2 .. z0+1, the z
+// slopes at z0-1 and z0 and the z face z0, left in zss / zfs and the centre
+// slots for the plane loop.  Out of line: it runs once per item, and a second
+// inlined copy of the slope and face code would only crowd the instruction
+// cache of the plane loop.
+template <bool IN_PRIM, bool HLLC, int NF>
+__device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, double* full,
+                                            double* cen, double* zss, double* zfs, int tid,
+                                            int tx, int ty, int gx, int gy, int z0, bool own,
+                                            double dt) {
+  auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
+  double* fc = full + (ty + 2) * PW + (tx + 2);
+  load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 - 2);
+  load_cell_col<IN_PRIM>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
+  load_cell_col<IN_PRIM>(B, ph, cslot(z0), gx, gy, z0);
+  double s_m[5], s_0[5];
+  z_slope(B.geo[2], ph, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
+  load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 + 1);
+  z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, s_0);
+  double F[NF];
+  z_face<HLLC, NF>(B, ph, z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, gx, gy, own, dt,
+                   F);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) zss[q * NT + tid] = s_0[q];
+#pragma unroll
+  for (int u = 0; u < NF; ++u) zfs[u * NT + tid] = F[u];
+  // plane z0+1 into its centre slot (the slot of z0-1)
+  double* d = cslot(z0 + 1);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) d[q * NT] = fc[q * PS];
+}
+
 // BATCHED: the work items span many bricks; each item's brick descriptor is
 // copied from `many` into shared memory.  Otherwise `single` describes the one
 // brick (read from the constant bank).
@@ -362,7 +431,7 @@ __global__ void __launch_bounds__(NT, 2)
       __syncthreads();
       continue;
     }
-    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const int n0 = B.n[0], n1 = B.n[1];
     const AxisGeo& GZ = B.geo[2];
     const double dt = *B.dt;
     const int x0 = W.x0, y0 = W.y0, z0 = W.z0, z1 = W.z1;
@@ -375,56 +444,9 @@ __global__ void __launch_bounds__(NT, 2)
     // own column helpers: a "column pointer" addresses 5 values at stride NT
     // (centre slots) or PS (full plane)
     auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
-    auto z_slope = [&](int p, const double* a, int sa, const double* b, int sb,
-                       const double* c, int sc, double* out) {
-      const int t = p + 2;
-      const double dxl = __ldg(GZ.dXI + t), dxr = __ldg(GZ.dXI + t + 1);
-      const double sql = __ldg(GZ.SQ + t), sqr = __ldg(GZ.SQ + t + 1),
-                   cden = __ldg(GZ.CDEN + t);
-      const double rdxl = __ldg(GZ.RDXI + t), rdxr = __ldg(GZ.RDXI + t + 1),
-                   rcden = __ldg(GZ.RCDEN + t);
-#pragma unroll
-      for (int q = 0; q < 5; ++q)
-        out[q] = limited_slope(a[q * sa], b[q * sb], c[q * sc], dxl, dxr, sql, sqr, cden, rdxl,
-                               rdxr, rcden, ph.theta, ph.use_limiter);
-    };
-    // z face between planes p-1 (values a, slopes sm_) and p (values b, slopes sp)
-    auto z_face = [&](int p, const double* a, int sa, const double* sm_, int ssm,
-                      const double* b, int sb, const double* sp, int ssp, double* F) {
-      double l[5], r[5];
-      face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2),
-                 l, r);
-      FaceState L, R;
-      face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
-      face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
-      const bool diff = HLLC && df_bit(B, 2, gx, gy, p);
-      riemann_flux<2, HLLC, NF>(L, R, diff, F);
-      if (own && (p == 0 || p == n2) && B.fluence)
-        boundary_fluence<2, HLLC, NF>(B, ph, l, r, diff, F, p == 0 ? 4 : 5, gx, n0, gy,
-                                      B.weight * dt);
-    };
-
     // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
-    {
-      double* fc = full + c_off;
-      load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 - 2);
-      load_cell_col<IN_PRIM>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
-      load_cell_col<IN_PRIM>(B, ph, cslot(z0), gx, gy, z0);
-      double s_m[5], s_0[5];
-      z_slope(z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
-      load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 + 1);
-      z_slope(z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, s_0);
-      double F[NF];
-      z_face(z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, F);
-#pragma unroll
-      for (int q = 0; q < 5; ++q) zss[q * NT + tid] = s_0[q];
-#pragma unroll
-      for (int u = 0; u < NF; ++u) zfs[u * NT + tid] = F[u];
-      // plane z0+1 into its centre slot (the slot of z0-1)
-      double* d = cslot(z0 + 1);
-#pragma unroll
-      for (int q = 0; q < 5; ++q) d[q * NT] = fc[q * PS];
-    }
+    stage_prologue<IN_PRIM, HLLC, NF>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx, gy, z0, own,
+                                      dt);
     __syncthreads();  // geometry caches
 
     for (int k = z0; k < z1; ++k) {
@@ -436,14 +458,18 @@ __global__ void __launch_bounds__(NT, 2)
         for (int q = 0; q < 5; ++q) full[q * PS + c_off] = src[q * NT];
       }
       load_cell_col<IN_PRIM>(B, ph, cslot(k + 2), gx, gy, k + 2);
-      if (tid < 4 * TX) {
-        const int s = tid / TX, lx = tid % TX;
-        const int ly = (s < 2) ? s - 2 : TY + s - 2;
-        load_cell<IN_PRIM>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
-      } else if (tid < 4 * TX + 4 * TY) {
-        const int j = tid - 4 * TX;
-        const int ly = j / 4, s = j % 4;
-        const int lx = (s < 2) ? s - 2 : TX + s - 2;
+      if (tid < 4 * TX + 4 * TY) {
+        // the halo: two rows below and above the tile, two columns left and right
+        int lx, ly;
+        if (tid < 4 * TX) {
+          const int s = tid / TX;
+          lx = tid % TX;
+          ly = (s < 2) ? s - 2 : TY + s - 2;
+        } else {
+          const int j = tid - 4 * TX, s = j % 4;
+          ly = j / 4;
+          lx = (s < 2) ? s - 2 : TX + s - 2;
+        }
         load_cell<IN_PRIM>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
       }
       __syncthreads();
@@ -453,19 +479,23 @@ __global__ void __launch_bounds__(NT, 2)
         constexpr int NXS = TY * (TX + 2), NYS = (TY + 2) * TX;
         constexpr int PXS = (NXS + 31) / 32 * 32;
         for (int i = tid; i < PXS + NYS; i += NT) {
-          if (i < PXS) {
-            if (i >= NXS) continue;
-            const int ly = i / (TX + 2), lx = i % (TX + 2) - 1;
+          const bool isx = i < PXS;
+          if (isx && i >= NXS) continue;
+          int lx, ly;
+          if (isx) {
+            ly = i / (TX + 2);
+            lx = i % (TX + 2) - 1;
             if (x0 + lx > n0 || y0 + ly >= n1) continue;
-            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, 1, gxc, LX, lx + 2, ph,
-                        sxs + ly * (TX + 2) + lx + 1, TY * (TX + 2));
           } else {
             const int j = i - PXS;
-            const int ly = j / TX - 1, lx = j % TX;
+            ly = j / TX - 1;
+            lx = j % TX;
             if (y0 + ly > n1 || x0 + lx >= n0) continue;
-            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, PW, gyc, LY, ly + 2, ph,
-                        sys + (ly + 1) * TX + lx, (TY + 2) * TX);
           }
+          cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, isx ? 1 : PW, isx ? gxc : gyc,
+                      isx ? LX : LY, isx ? lx + 2 : ly + 2, ph,
+                      isx ? sxs + ly * (TX + 2) + lx + 1 : sys + (ly + 1) * TX + lx,
+                      isx ? TY * (TX + 2) : (TY + 2) * TX);
         }
       }
       __syncthreads();
@@ -527,8 +557,9 @@ __global__ void __launch_bounds__(NT, 2)
 
       // (4) z slope at k+1 and z face k+1 of the own column
       double zsn[5], zfn[NF];
-      z_slope(k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
-      z_face(k + 1, full + c_off, PS, zss + tid, NT, cslot(k + 1), NT, zsn, 1, zfn);
+      z_slope(GZ, ph, k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
+      z_face<HLLC, NF>(B, ph, k + 1, full + c_off, PS, zss + tid, NT, cslot(k + 1), NT, zsn, 1,
+                       gx, gy, own, dt, zfn);
       __syncthreads();
 
       // (5) cell update and stage epilogue
