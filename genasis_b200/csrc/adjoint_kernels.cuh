@@ -8,7 +8,7 @@
 // Its adjoint, given lam^n+1, runs backwards:
 //   lamZ = final^T lam^n+1, lamW1 = L^T(lamZ / 2), lamY = W^T(W1) lamW1,
 //   lamK1 = lamY + lamZ / 2, lamW0 = L^T(lamK1),
-//   lam^n = lamZ + lamY + W^T(W0) lamW0.
+//   lam^n = lamZ + lamY + W^T(W0) lamW0 = lamZ / 2 + lamK1 + W^T(W0) lamW0.
 // The stages are recomputed from the checkpoint U^n (the stage kernels write
 // W1), the shock features are those of U^n in both stages, and dt is held
 // fixed.  L^T is one kernel per direction: a thread sweeps a segment of faces
@@ -249,38 +249,34 @@ __global__ void adj_final_kernel(Box b, Phys ph, const double* __restrict__ lam,
   }
 }
 
-// After L^T of stage 2: lamY = W^T(W1)(lamW1 + gravity^T(lamZ / 2)),
-// lamK1 = lamY + lamZ / 2, lam^n = lamZ + lamY (DS and ghosts left zero);
-// lamW is cleared for the next L^T.
+// After L^T of stage 2: lamY = W^T(W1)(lamW1 + gravity^T(lamZ / 2)) and
+// lamK1 = lamY + lamZ / 2.
 __global__ void adj_mid_kernel(Box b, Phys ph, double dt, const double* __restrict__ W1,
-                               const double* __restrict__ lamZ, double* __restrict__ lamW,
-                               double* __restrict__ lamK1, double* __restrict__ lam) {
+                               const double* __restrict__ lamZ, const double* __restrict__ lamW,
+                               double* __restrict__ lamK1) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
        c += (long long)gridDim.x * blockDim.x) {
-    double w[5], lz[5], lw[5], lk2[5];
+    double w[5], lw[5], lk2[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       w[q] = W1[q * b.nP + c];
-      lz[q] = lamZ[q * b.nP + c];
       lw[q] = lamW[q * b.nP + c];
-      lamW[q * b.nP + c] = 0.0;
-      lk2[q] = 0.5 * lz[q];
+      lk2[q] = 0.5 * lamZ[q * b.nP + c];
     }
     if (ph.accel != 0.0) gravity_adjoint(w, lk2, ph.accel, dt, lw);
     double ly[5];
     c2p_adjoint(w, lw, ph.nmin, ly);
-    const long long g = ghost_index(b, c);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      lamK1[q * b.nP + c] = ly[q] + lk2[q];
-      lam[q * b.nV + g] = lz[q] + ly[q];
-    }
+    for (int q = 0; q < 5; ++q) lamK1[q * b.nP + c] = ly[q] + lk2[q];
   }
 }
 
-// After L^T of stage 1: lam^n += W^T(W0)(lamW0 + gravity^T(lamK1)).
+// After L^T of stage 1: lam^n = lamZ + lamY + W^T(W0)(lamW0 + gravity^T(lamK1)),
+// with lamZ + lamY = lamZ / 2 + lamK1; DS and the ghosts keep the zeros the
+// caller's array was cleared to.
 __global__ void adj_last_kernel(Box b, Phys ph, double dt, const double* __restrict__ W0,
                                 const double* __restrict__ lamK1,
+                                const double* __restrict__ lamZ,
                                 const double* __restrict__ lamW, double* __restrict__ lam) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
        c += (long long)gridDim.x * blockDim.x) {
@@ -296,7 +292,7 @@ __global__ void adj_last_kernel(Box b, Phys ph, double dt, const double* __restr
     c2p_adjoint(w, lw, ph.nmin, lu);
     const long long g = ghost_index(b, c);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) lam[q * b.nV + g] += lu[q];
+    for (int q = 0; q < 5; ++q) lam[q * b.nV + g] = 0.5 * lamZ[q * b.nP + c] + lk[q] + lu[q];
   }
 }
 

@@ -224,6 +224,33 @@ __device__ __forceinline__ void detect_shock_cell(const Box& b, const Phys& ph, 
   sb[c] = bits;
 }
 
+// The same shock bits from the pressure and velocities that the previous
+// step's stage 2 stored for its new state (pv = [P, V1, V2, V3][nP]): the
+// values cell_p_v would recover from that state, without the recovery.
+__global__ void detect_shock_pv_kernel(Box b, Phys ph, const double* __restrict__ pv,
+                                       uint8_t* __restrict__ sb) {
+  const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int t[3] = {(int)(c % b.n[0]), (int)((c / b.n[0]) % b.n[1]),
+                      (int)(c / ((long long)b.n[0] * b.n[1]))};
+    const double P0 = pv[c];
+    uint8_t bits = 0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      if (t[e] < 1) continue;
+      const long long cm = c - st[e];
+      const double P1 = pv[cm];
+      const double dP = fabs(P0 - P1);
+      const double pmin = (P0 < P1) ? P0 : P1;
+      const double dLnP = dP / fmax2(pmin, kSqrtTiny);
+      const double dV = pv[(1 + e) * b.nP + c] - pv[(1 + e) * b.nP + cm];
+      if (dLnP > ph.shock_threshold && dV <= 0.0) bits |= (uint8_t)(1u << e);
+    }
+    sb[c] = bits;
+  }
+}
+
 __global__ void detect_shock_kernel(Box b, Phys ph, const double* __restrict__ U,
                                     const double* __restrict__ Pst, uint8_t* __restrict__ sb) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
@@ -372,6 +399,40 @@ __global__ void advance_clock_kernel(Clock* __restrict__ clk, int n) {
   c.time = c.time + c.dt;
   c.cycle = c.cycle + 1;
   if (!(c.time < c.finish && c.cycle < c.max_cycle)) c.done = 1;
+}
+
+// Volume integrals of the six conserved fields over the proper cells
+// (Current_ASC__Template.f90:203-349, VolumeIntegral_Form.f90:25-117): block b
+// sums the cells [b chunk, (b + 1) chunk) and writes its six partial sums;
+// the host adds the partials in block order, so the result does not depend
+// on timing.
+__global__ void totals_kernel(Box b, const double* __restrict__ U, AxisGeo G0, AxisGeo G1,
+                              AxisGeo G2, long long chunk, double* __restrict__ partial) {
+  __shared__ double s_red[6][32];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const long long c0 = blockIdx.x * chunk, c1 = min(b.nP, c0 + chunk);
+  for (long long c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const int i = (int)(c % b.n[0]), j = (int)((c / b.n[0]) % b.n[1]),
+              k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    const long long g = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
+    const double dv = G0.W[i + 2] * G1.W[j + 2] * G2.W[k + 2];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] += U[q * b.nV + g] * dv;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double v = acc[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) s_red[q][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_red[threadIdx.x][w];
+    partial[blockIdx.x * 6 + threadIdx.x] = v;
+  }
 }
 
 // Counts of proper cells holding a non-finite value in any field, and of

@@ -153,6 +153,8 @@ struct gfx_fluid {
   int z_chunk = 0;
   int adjoint_segment = 0;
   unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
+  double* partials = nullptr;                  // per-block sums of gfx_fluid_totals
+  double* pv = nullptr;  // [4][nP]: P and V of the state the last stage 2 wrote
 };
 
 namespace {
@@ -317,11 +319,26 @@ int run_features(gfx_fluid* h, const double* U, const double* Pst, cudaStream_t 
   return GFX_OK;
 }
 
+// Shock flags of the state the previous step's stage 2 wrote, from its
+// stored pressure and velocities (valid only between the steps of one
+// evolve, where nothing else touches the state).
+int run_features_pv(gfx_fluid* h, cudaStream_t s) {
+  const int blk = 256;
+  detect_shock_pv_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->ph, h->pv, h->sb);
+  CUDA_TRY(cudaGetLastError());
+  detect_flags_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->sb, h->df);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 2;
+  return GFX_OK;
+}
+
 // The launches of one RK2 step on U (in place).  dt_ptr, skip: device scalars.
 // detect: whether the shock flags must be recomputed from U first.  ev (may
 // be null): 5 events recorded between the phases for gfx_fluid_step_timed.
+// from_pv: detect from the pressure and velocities of the previous stage 2.
 int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
-                 double* fluence, bool detect, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+                 double* fluence, bool detect, cudaStream_t s, cudaEvent_t* ev = nullptr,
+                 bool from_pv = false) {
   const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
   const bool grav = h->cfg.uniform_acceleration != 0.0;
   reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
@@ -331,7 +348,7 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
     CUDA_TRY(cudaMemsetAsync(fluence, 0, sizeof(double) * 36 * h->face_size, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[0], s));
   if (hllc && detect) {
-    int rc = run_features(h, U, nullptr, s);
+    int rc = from_pv ? run_features_pv(h, s) : run_features(h, U, nullptr, s);
     if (rc) return rc;
   }
   if (ev) CUDA_TRY(cudaEventRecord(ev[1], s));
@@ -343,6 +360,7 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
                         h->counters, h->ph, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[2], s));
   BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fluence, dt_ptr, 0.5, skip);
+  d2.pv = h->pv;
   CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
                         h->counters + 1, h->ph, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[3], s));
@@ -506,7 +524,8 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
       cudaMalloc(&h->tsi_bits, 2 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&h->counters, 4 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&h->clock, 2 * sizeof(Clock)) != cudaSuccess ||
-      cudaMalloc(&h->dt_slot, sizeof(double)) != cudaSuccess)
+      cudaMalloc(&h->dt_slot, sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->pv, 4 * nP * sizeof(double)) != cudaSuccess)
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc of the stage scratch (%zu cells)", nP));
   if (cudaMemset(h->df, 0, nP) != cudaSuccess)
     return cleanup(fail(GFX_ERR_CUDA, "clear features"));
@@ -541,6 +560,8 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->adj_flags);
   cudaFree(h->adj_U);
   cudaFree(h->state_counts);
+  cudaFree(h->partials);
+  cudaFree(h->pv);
   if (h->host_stream) cudaStreamDestroy(h->host_stream);
   delete h;
   return GFX_OK;
@@ -748,7 +769,9 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
       cudaGraph_t g;
       const long long before = h->launches;
       CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      int rc2 = enqueue_step(h, U, &dc->dt, &dc->done, nullptr, true, cs);
+      // every captured cycle follows a step of this evolve: its flags come
+      // from the pressure and velocities that step's stage 2 stored
+      int rc2 = enqueue_step(h, U, &dc->dt, &dc->done, nullptr, true, cs, nullptr, true);
       advance_clock_kernel<<<1, 1, 0, cs>>>(dc, 1);
       finalize_dt_kernel<<<1, 1, 0, cs>>>(h->ph, h->tsi_bits, dc, 1, 1);
       cudaError_t ce = cudaStreamEndCapture(cs, &g);
@@ -1058,6 +1081,29 @@ int gfx_fluid_check_state(gfx_fluid* h, const double* U, void* stream) {
   if (c[0] != 0)
     return fail(GFX_ERR_STATE, "%llu proper cells hold non-finite values (%llu at the density "
                 "floor)", c[0], c[1]);
+  return GFX_OK;
+}
+
+int gfx_fluid_totals(gfx_fluid* h, const double* U, double* totals, void* stream) {
+  if (!h || !U || !totals) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = 4 * num_sms();
+  const long long chunk = (h->box.nP + blocks - 1) / blocks;
+  if (!h->partials && cudaMalloc(&h->partials, 6 * blocks * sizeof(double)) != cudaSuccess)
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc tally partials");
+  totals_kernel<<<blocks, 256, 0, s>>>(h->box, U, h->dgeo[0], h->dgeo[1], h->dgeo[2], chunk,
+                                       h->partials);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  std::vector<double> part(6 * (size_t)blocks);
+  CUDA_TRY(cudaMemcpyAsync(part.data(), h->partials, part.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  for (int q = 0; q < 6; ++q) {
+    double t = 0.0;
+    for (int b = 0; b < blocks; ++b) t += part[6 * (size_t)b + q];
+    totals[q] = t;
+  }
   return GFX_OK;
 }
 
@@ -1518,14 +1564,15 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
   h->launches += 1;
   int rc = enqueue_adj_stage(h, h->Yp, lamZ, 0.5, lamW, feat, dt, s);
   if (rc) return rc;
-  CUDA_TRY(cudaMemsetAsync(lam_n, 0, 6 * nV * sizeof(double), s));
-  adj_mid_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, dt, h->Yp, lamZ, lamW, lamK1,
-                                                      lam_n);
+  adj_mid_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, dt, h->Yp, lamZ, lamW, lamK1);
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
+  CUDA_TRY(cudaMemsetAsync(lamW, 0, 5 * nP * sizeof(double), s));
+  CUDA_TRY(cudaMemsetAsync(lam_n, 0, 6 * nV * sizeof(double), s));
   rc = enqueue_adj_stage(h, W0, lamK1, 1.0, lamW, feat, dt, s);
   if (rc) return rc;
-  adj_last_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, dt, W0, lamK1, lamW, lam_n);
+  adj_last_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, dt, W0, lamK1, lamZ, lamW,
+                                                       lam_n);
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
   return GFX_OK;

@@ -62,6 +62,7 @@ struct BrickDesc {
   double weight;         // Runge-Kutta weight of the stage (fluence)
   unsigned long long* tsi_bits;  // max inverse CFL time, ordered bits
   const int* skip;       // device flag: nonzero = do nothing (finished evolve)
+  double* pv;            // stage 2: P, V1, V2, V3 of the new state, compact (or null)
   AxisGeo geo[3];
 };
 
@@ -667,6 +668,12 @@ __global__ void __launch_bounds__(NT, 2)
             U[3 * B.nV + gidx] = u.S3;
             U[4 * B.nV + gidx] = u.G;
             U[5 * B.nV + gidx] = SB * w.N;
+            if (B.pv) {
+              B.pv[cidx] = P;
+              B.pv[B.nP + cidx] = w.V1;
+              B.pv[2 * B.nP + cidx] = w.V2;
+              B.pv[3 * B.nP + cidx] = w.V3;
+            }
             tsi_max = fmax2(tsi_max,
                             inverse_cfl_time(w, CS, w0, w1, w2, gxc[G_RW * LX + tx + 2],
                                              gyc[G_RW * LY + ty + 2], __ldg(GZ.RW + k + 2)));

@@ -155,6 +155,14 @@ class FluidBox:
         lib.call("gfx_fluid_set_tuning", self.h, int(z_chunk), int(adjoint_segment))
         self.tuning = (int(z_chunk), int(adjoint_segment))
 
+    def totals(self, U=None):
+        """sum U dV over the proper cells for the six conserved fields
+        (the conservation tallies), as a numpy array."""
+        out = np.zeros(6)
+        lib.call("gfx_fluid_totals", self.h, _ptr(self.U if U is None else U),
+                 out.ctypes.data_as(ctypes.c_void_p), _stream())
+        return out
+
     def check_state(self, U=None):
         """Raises GfxError (GFX_ERR_STATE) if a proper cell of U (default: the
         box's state) holds a non-finite value."""

@@ -229,6 +229,13 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config *cfg, double *U_dev, double dt
  * stream. */
 int gfx_fluid_check_state(gfx_fluid *h, const double *U_dev, void *stream);
 
+/* Volume integrals of the six conserved fields of U_dev over the proper
+ * cells, sum U dV (the conservation tallies of Current_ASC__Template.f90:
+ * 203-349 and VolumeIntegral_Form.f90:25-117, on the device): totals_host[6].
+ * Partial sums are added in a fixed order, so repeated calls agree bit for
+ * bit.  Synchronises the stream. */
+int gfx_fluid_totals(gfx_fluid *h, const double *U_dev, double *totals_host, void *stream);
+
 /* Speed knobs (set by genasis_b200/autotune.py).  The step's results do not
  * depend on them, bit for bit; the adjoint's change only by the rounding of
  * its atomic additions, whose order is not fixed in any case:

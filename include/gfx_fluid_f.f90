@@ -61,7 +61,8 @@ module GFX_Fluid_C
     gfx_fluid_set_tuning, gfx_fluid_batch_create, gfx_fluid_batch_destroy, &
     gfx_fluid_batch_set_clocks, gfx_fluid_batch_evolve, &
     gfx_fluid_batch_clocks, gfx_fluid_batch_kernel_launches, &
-    gfx_fluid_step_noalloc, gfx_fluid_check_state, gfx_fluid_last_error
+    gfx_fluid_step_noalloc, gfx_fluid_check_state, gfx_fluid_totals, &
+    gfx_fluid_last_error
 
   interface
 
@@ -277,6 +278,13 @@ module GFX_Fluid_C
       import
       type ( c_ptr ), value :: Handle, Conserved_dev, Stream
     end function gfx_fluid_check_state
+
+    integer ( c_int ) function gfx_fluid_totals ( Handle, Conserved_dev, Totals, Stream ) &
+      bind ( c, name = 'gfx_fluid_totals' )
+      import
+      type ( c_ptr ), value :: Handle, Conserved_dev, Stream
+      real ( c_double ), intent ( out ) :: Totals ( 6 )
+    end function gfx_fluid_totals
 
     integer ( c_int ) function gfx_fluid_last_error ( Buffer, Length ) &
       bind ( c, name = 'gfx_fluid_last_error' )
