@@ -45,7 +45,7 @@ __device__ __forceinline__ double limited_slope_branch(double vm, double v0, dou
   bm = p3 ? cden : bm;
   rm = p3 ? rcden : rm;
   const double q = markstein(am, bm, rm);
-  const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && quotient_in_range(am, rm);
+  const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && geo_quotient_in_range(am);
   branch = (s == 0.0) ? 0 : (p3 ? 3 : (p12 ? 1 : 2));
   if (s == 0.0) return 0.0;
   return fast ? s * q : limited_slope_ieee(dvl, dvr, dxl, dxr, sql, sqr, cden, theta);

@@ -66,15 +66,30 @@ __device__ __forceinline__ double markstein(double a, double b, double r) {
   return __fma_rn(e1, r, q1);
 }
 
-// |x| == 0 or 2^-900 <= |x| < 2^1001, from the exponent bits (integer pipe).
+// |x| == 0 or 2^-900 <= |x| < 2^1001 (NaN and infinities fail).
 __device__ __forceinline__ bool exp_in_range(double x) {
-  const unsigned hi = (unsigned)__double2hiint(x) & 0x7fffffffu;
-  const unsigned e = hi >> 20;
-  return (e - 123u) < 1901u || (hi | (unsigned)__double2loint(x)) == 0u;
+  const double ax = fabs(x);
+  return (ax >= 0x1p-900 && ax < 0x1p1001) || x == 0.0;
 }
 
 __device__ __forceinline__ bool quotient_in_range(double a, double r) {
   return exp_in_range(a) & exp_in_range(a * r);
+}
+
+// The same window for a divisor of the chart geometry (a width, a centre
+// difference, the limiter's central denominator or a cell volume), whose
+// rounded reciprocal r lies in [2^-300, 2^300] because every cell width lies
+// in [2^-98, 2^98] (checked when a brick is created): then 2^-600 <= |a| <
+// 2^700, or a == 0, puts both a and a r inside the window, and one test on
+// a suffices.
+__device__ __forceinline__ bool geo_quotient_in_range(double a) {
+  const double ax = fabs(a);
+  return (ax >= 0x1p-600 && ax < 0x1p700) || a == 0.0;
+}
+
+__device__ __forceinline__ double div_geo(double a, double b, double r) {
+  const double q = markstein(a, b, r);
+  return geo_quotient_in_range(a) ? q : div_ieee(a, b);
 }
 
 __device__ __forceinline__ double div_rn(double a, double b, double r) {
@@ -129,7 +144,7 @@ __device__ __forceinline__ double limited_slope(double vm, double v0, double vp,
   rm = p3 ? rcden : rm;
   const double q = markstein(am, bm, rm);
   // a zero candidate is the minimum whatever the ties
-  const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && quotient_in_range(am, rm);
+  const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && geo_quotient_in_range(am);
   if (s == 0.0) return 0.0;
   return fast ? s * q : limited_slope_ieee(dvl, dvr, dxl, dxr, sql, sqr, cden, theta);
 }
@@ -342,9 +357,9 @@ __device__ __forceinline__ void eos_cell(double N, double E, const Phys& ph, dou
 __device__ __forceinline__ double inverse_cfl_time(const Prim& w, double CS, double w0,
                                                    double w1, double w2, double r0, double r1,
                                                    double r2) {
-  return div_rn(fmax2(w.V1 + CS, -(w.V1 - CS)), w0, r0) +
-         div_rn(fmax2(w.V2 + CS, -(w.V2 - CS)), w1, r1) +
-         div_rn(fmax2(w.V3 + CS, -(w.V3 - CS)), w2, r2);
+  return div_geo(fmax2(w.V1 + CS, -(w.V1 - CS)), w0, r0) +
+         div_geo(fmax2(w.V2 + CS, -(w.V2 - CS)), w1, r1) +
+         div_geo(fmax2(w.V3 + CS, -(w.V3 - CS)), w2, r2);
 }
 
 // Total order of doubles as unsigned integers, for atomicMax reductions.

@@ -226,6 +226,10 @@ int validate(const gfx_fluid_config* c) {
                   c->n_cells[d]);
     if (!(c->max_coordinate[d] > c->min_coordinate[d]))
       return fail(GFX_ERR_ARGUMENT, "max_coordinate[%d] must exceed min_coordinate[%d]", d, d);
+    // the exact divisions by geometry values assume widths in [2^-98, 2^98]
+    const double w = (c->max_coordinate[d] - c->min_coordinate[d]) / c->n_cells[d];
+    if (!(w >= 0x1p-98 && w <= 0x1p98))
+      return fail(GFX_ERR_UNSUPPORTED, "axis %d: cell width %g outside [2^-98, 2^98]", d, w);
     for (int s = 0; s < 2; ++s)
       if (c->boundary[d][s] < GFX_BC_OUTFLOW || c->boundary[d][s] > GFX_BC_PERIODIC)
         return fail(GFX_ERR_ARGUMENT, "boundary[%d][%d] = %d is not a boundary condition", d,

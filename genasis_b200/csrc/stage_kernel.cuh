@@ -587,8 +587,8 @@ __global__ void __launch_bounds__(NT, 2)
           qx[u] = markstein(nx_[u], vol, rvol);
           qy[u] = markstein(ny_[u], vol, rvol);
           qz[u] = markstein(nz_[u], vol, rvol);
-          ok &= quotient_in_range(nx_[u], rvol) & quotient_in_range(ny_[u], rvol) &
-                quotient_in_range(nz_[u], rvol);
+          ok &= geo_quotient_in_range(nx_[u]) & geo_quotient_in_range(ny_[u]) &
+                geo_quotient_in_range(nz_[u]);
         }
         if (!ok) {
 #pragma unroll

@@ -14,16 +14,6 @@
 #define __forceinline__ inline
 #define __noinline__
 static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
-static inline int __double2hiint(double x) {
-  uint64_t u;
-  std::memcpy(&u, &x, 8);
-  return (int)(u >> 32);
-}
-static inline int __double2loint(double x) {
-  uint64_t u;
-  std::memcpy(&u, &x, 8);
-  return (int)(uint32_t)u;
-}
 static inline long long __double_as_longlong(double x) {
   long long u;
   std::memcpy(&u, &x, 8);
