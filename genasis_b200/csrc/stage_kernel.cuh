@@ -21,8 +21,9 @@
 namespace gfx {
 
 constexpr int TX = 32;          // tile width (x), one warp per row
-constexpr int TY = 8;           // tile rows (y)
+constexpr int TY = 16;          // tile rows (y)
 constexpr int NT = TX * TY;     // threads per CTA
+constexpr int kMinCtas = (NT >= 512) ? 1 : 2;  // CTAs per SM the registers allow
 constexpr int PW = TX + 4;      // plane pitch with the 2-cell halo
 constexpr int PH = TY + 4;
 constexpr int PS = PW * PH;     // doubles per plane per variable
@@ -388,7 +389,7 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
 // copied from `many` into shared memory.  Otherwise `single` describes the one
 // brick (read from the constant bank).
 template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, kMinCtas)
     stage_kernel(const __grid_constant__ BrickDesc single, const BrickDesc* __restrict__ many,
                  const WorkItem* __restrict__ items, int n_items, int* __restrict__ counter,
                  const __grid_constant__ Phys ph) {
