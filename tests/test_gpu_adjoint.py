@@ -170,5 +170,7 @@ def test_adjoint_recomputes_the_new_state_when_not_given():
     a = step_adjoint(box, U0, dts[0], lam, U_np1=U1, detect_features=False)
     b = step_adjoint(box, U0, dts[0], lam, U_np1=None, detect_features=False)
     torch.cuda.synchronize()
-    assert np.array_equal(to_np(a), to_np(b))
+    # equal up to the rounding of the adjoint's unordered atomic additions
+    A, Bv = to_np(a), to_np(b)
+    assert float(np.abs(A - Bv).max()) <= 1e-12 * float(np.abs(Bv).max())
     box.close()
