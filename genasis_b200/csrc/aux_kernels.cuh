@@ -143,6 +143,14 @@ __global__ void ghost_refresh_kernel(Box b, Phys ph, double* __restrict__ U) {
     ghost_refresh_value(b, ph, U, v);
 }
 
+// The same over the values [v0, v1) only (whole planes of a z slab).
+__global__ void ghost_refresh_range_kernel(Box b, Phys ph, double* __restrict__ U, long long v0,
+                                           long long v1) {
+  for (long long v = v0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; v < v1;
+       v += (long long)gridDim.x * blockDim.x)
+    ghost_refresh_value(b, ph, U, v);
+}
+
 // One brick of a batch for the element-wise kernels: its box, its state and
 // feature storage, and the offsets of its values in the batch's flat ranges.
 struct BatchBrick {
@@ -291,6 +299,21 @@ __device__ __forceinline__ void detect_flags_cell(const Box& b, const uint8_t* s
 __global__ void detect_flags_kernel(Box b, const uint8_t* __restrict__ sb,
                                     uint8_t* __restrict__ df) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
+       c += (long long)gridDim.x * blockDim.x)
+    detect_flags_cell(b, sb, df, c);
+}
+
+// Shock bits and flags of the proper cells [c0, c1) only (whole planes).
+__global__ void detect_shock_range_kernel(Box b, Phys ph, const double* __restrict__ U,
+                                          uint8_t* __restrict__ sb, long long c0, long long c1) {
+  for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1;
+       c += (long long)gridDim.x * blockDim.x)
+    detect_shock_cell(b, ph, U, nullptr, sb, c);
+}
+
+__global__ void detect_flags_range_kernel(Box b, const uint8_t* __restrict__ sb,
+                                          uint8_t* __restrict__ df, long long c0, long long c1) {
+  for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1;
        c += (long long)gridDim.x * blockDim.x)
     detect_flags_cell(b, sb, df, c);
 }

@@ -155,6 +155,10 @@ struct gfx_fluid {
   unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
   double* partials = nullptr;                  // per-block sums of gfx_fluid_totals
   double* pv = nullptr;  // [4][nP]: P and V of the state the last stage 2 wrote
+  // pipelined gfx_fluid_step_host: copy streams, per-slab events and counters
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_in[8] = {}, ev_out[8] = {}, ev_end = nullptr;
+  int* slab_counters = nullptr;  // [16]
 };
 
 namespace {
@@ -434,6 +438,149 @@ int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, bool in_prim, cudaStrea
 
 }  // namespace
 
+namespace {
+
+// gfx_fluid_step with U in host memory, pipelined over z slabs (whole
+// z chunks of the work list) on three streams: the copy of the inputs (the
+// five fields D, S1, S2, S3, G of every plane: DS is rewritten by the step and
+// never read), the compute, and the copy of the result (all six fields).
+// Shock detection and stage 1 of a slab start as soon as its planes and the
+// two above it have arrived; every slab is copied back as soon as its stage 2
+// and the x / y ghosts of its planes are done, while stage 2 of the next slab
+// runs; the z ghost planes, which reach across the brick, come last.  The
+// launches and their inputs are those of gfx_fluid_step, so the result is
+// the same bit for bit.  Returns GFX_ERR_UNSUPPORTED when the work list is too
+// short to pipeline (the caller then takes the unpipelined path).
+int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence_host) {
+  const Box& b = h->box;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  if (h->prims_pending) return GFX_ERR_UNSUPPORTED;
+  std::vector<WorkItem> items = make_items(b.n, 0, h->z_chunk);
+  const int cols = ((b.n[0] + TX - 1) / TX) * ((b.n[1] + TY - 1) / TY);
+  const int nchunks = (int)items.size() / cols;
+  const int len = items[0].z1 - items[0].z0;
+  if (nchunks < 2 || len < 2 || (int)items.size() != h->n_items)
+    return GFX_ERR_UNSUPPORTED;
+  const int S = std::min(8, nchunks);
+  int it[9], zs[9];
+  for (int j = 0; j <= S; ++j) {
+    const int c = (int)((long long)j * nchunks / S);
+    it[j] = c * cols;
+    zs[j] = (j == S) ? b.n[2] : items[(size_t)c * cols].z0;
+  }
+  if (!h->copy_in) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
+  if (!h->copy_out) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
+  for (int j = 0; j < 8; ++j) {
+    if (!h->ev_in[j]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_in[j], cudaEventDisableTiming));
+    if (!h->ev_out[j]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_out[j], cudaEventDisableTiming));
+  }
+  if (!h->ev_end) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_end, cudaEventDisableTiming));
+  if (!h->slab_counters && cudaMalloc(&h->slab_counters, 16 * sizeof(int)) != cudaSuccess)
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc slab counters");
+  cudaStream_t sc = h->host_stream, si = h->copy_in, so = h->copy_out;
+  double* U = h->U_stage;
+  const size_t nV = (size_t)b.nV, plane = (size_t)b.m[0] * b.m[1];
+  const long long cplane = (long long)b.n[0] * b.n[1];
+  const int n2 = b.n[2];
+  auto copy = [&](cudaStream_t st, int nf, int p0, int p1, cudaMemcpyKind kind) -> cudaError_t {
+    for (int q = 0; q < nf; ++q) {
+      const size_t off = q * nV + (size_t)p0 * plane;
+      double* dst = (kind == cudaMemcpyHostToDevice) ? U + off : U_host + off;
+      const double* src = (kind == cudaMemcpyHostToDevice) ? U_host + off : U + off;
+      cudaError_t e = cudaMemcpyAsync(dst, src, (size_t)(p1 - p0) * plane * sizeof(double),
+                                      kind, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  // inputs: the top planes first (a periodic z axis reads them from slab 0),
+  // then the slabs; plane index P = z + 2 of the ghost layout
+  CUDA_TRY(copy(si, 5, n2, n2 + 4, cudaMemcpyHostToDevice));
+  for (int j = 0; j < S; ++j) {
+    const int p0 = (j == 0) ? 0 : zs[j] + 2, p1 = std::min(zs[j + 1] + 2, n2);
+    CUDA_TRY(copy(si, 5, p0, p1, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaEventRecord(h->ev_in[j], si));
+  }
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  const bool grav = h->cfg.uniform_acceleration != 0.0;
+  const bool detect = hllc && h->features == FEAT_PENDING;
+  const int blk = 256;
+  double* fl = fluence_host ? U + 6 * nV : nullptr;
+  reset_bits_kernel<<<1, 32, 0, sc>>>(h->tsi_bits, 1, h->slab_counters, 2 * S);
+  set_scalar_kernel<<<1, 1, 0, sc>>>(h->dt_slot, dt);
+  CUDA_TRY(cudaGetLastError());
+  if (fl) CUDA_TRY(cudaMemsetAsync(fl, 0, sizeof(double) * 36 * h->face_size, sc));
+  long long launches = 2;
+  const uint8_t* df = hllc ? h->df : nullptr;
+  BrickDesc d1 = make_desc(h, U, nullptr, nullptr, nullptr, df, fl, h->dt_slot, 0.5, nullptr);
+  BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fl, h->dt_slot, 0.5, nullptr);
+  d2.pv = h->pv;
+  auto stage = [&](int mode, int j) -> cudaError_t {
+    ++launches;
+    return launch_stage(mode, mode == MODE_STAGE2, hllc, grav, mode == MODE_STAGE1 ? d1 : d2,
+                        nullptr, h->items + it[j], it[j + 1] - it[j],
+                        h->slab_counters + (mode == MODE_STAGE1 ? 0 : S) + j, h->ph, sc);
+  };
+  auto shock = [&](int j) {
+    const long long c0 = zs[j] * cplane, c1 = zs[j + 1] * cplane;
+    detect_shock_range_kernel<<<grid_for(c1 - c0, blk), blk, 0, sc>>>(b, h->ph, U, h->sb, c0,
+                                                                       c1);
+    ++launches;
+  };
+  auto flags = [&](int j) {
+    const long long c0 = zs[j] * cplane, c1 = zs[j + 1] * cplane;
+    detect_flags_range_kernel<<<grid_for(c1 - c0, blk), blk, 0, sc>>>(b, h->sb, h->df, c0, c1);
+    ++launches;
+  };
+  // slab j: its shock bits once its planes are in; the flags of slab j-1
+  // (which read the first plane of slab j); stage 1 of slab j-2 (which reads
+  // two planes into slab j-1 and the flags of its top face)
+  for (int j = 0; j < S; ++j) {
+    CUDA_TRY(cudaStreamWaitEvent(sc, h->ev_in[j], 0));
+    if (detect) shock(j);
+    if (detect && j >= 1) flags(j - 1);
+    if (j >= 2) CUDA_TRY(stage(MODE_STAGE1, j - 2));
+  }
+  if (detect) flags(S - 1);
+  CUDA_TRY(cudaGetLastError());
+  if (S >= 2) CUDA_TRY(stage(MODE_STAGE1, S - 2));
+  CUDA_TRY(stage(MODE_STAGE1, S - 1));
+  // stage 2 slab by slab, each slab's in-plane ghosts, then its copy back
+  for (int j = 0; j < S; ++j) {
+    CUDA_TRY(stage(MODE_STAGE2, j));
+    const long long v0 = (long long)(zs[j] + 2) * plane, v1 = (long long)(zs[j + 1] + 2) * plane;
+    ghost_refresh_range_kernel<<<grid_for(v1 - v0, blk), blk, 0, sc>>>(b, h->ph, U, v0, v1);
+    CUDA_TRY(cudaGetLastError());
+    ++launches;
+    CUDA_TRY(cudaEventRecord(h->ev_out[j], sc));
+    CUDA_TRY(cudaStreamWaitEvent(so, h->ev_out[j], 0));
+    CUDA_TRY(copy(so, 6, zs[j] + 2, zs[j + 1] + 2, cudaMemcpyDeviceToHost));
+  }
+  // the z ghost planes, then their copy back and the fluence
+  ghost_refresh_range_kernel<<<grid_for(2 * (long long)plane, blk), blk, 0, sc>>>(
+      b, h->ph, U, 0, 2 * (long long)plane);
+  ghost_refresh_range_kernel<<<grid_for(2 * (long long)plane, blk), blk, 0, sc>>>(
+      b, h->ph, U, (long long)(n2 + 2) * plane, (long long)(n2 + 4) * plane);
+  CUDA_TRY(cudaGetLastError());
+  launches += 2;
+  CUDA_TRY(cudaEventRecord(h->ev_end, sc));
+  CUDA_TRY(cudaStreamWaitEvent(so, h->ev_end, 0));
+  CUDA_TRY(copy(so, 6, 0, 2, cudaMemcpyDeviceToHost));
+  CUDA_TRY(copy(so, 6, n2 + 2, n2 + 4, cudaMemcpyDeviceToHost));
+  if (fluence_host)
+    CUDA_TRY(cudaMemcpyAsync(fluence_host, fl, 36 * h->face_size * sizeof(double),
+                             cudaMemcpyDeviceToHost, so));
+  CUDA_TRY(cudaStreamSynchronize(so));
+  CUDA_TRY(cudaStreamSynchronize(sc));
+  h->launches += launches;
+  h->prims_pending = false;
+  h->features = FEAT_PENDING;
+  h->features_src = U;
+  return GFX_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int gfx_fluid_config_default(gfx_fluid_config* c) {
@@ -566,6 +713,14 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->state_counts);
   cudaFree(h->partials);
   cudaFree(h->pv);
+  cudaFree(h->slab_counters);
+  for (int j = 0; j < 8; ++j) {
+    if (h->ev_in[j]) cudaEventDestroy(h->ev_in[j]);
+    if (h->ev_out[j]) cudaEventDestroy(h->ev_out[j]);
+  }
+  if (h->ev_end) cudaEventDestroy(h->ev_end);
+  if (h->copy_in) cudaStreamDestroy(h->copy_in);
+  if (h->copy_out) cudaStreamDestroy(h->copy_out);
   if (h->host_stream) cudaStreamDestroy(h->host_stream);
   delete h;
   return GFX_OK;
@@ -688,6 +843,8 @@ int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence
     if (cudaMalloc(&h->U_stage, bytes + 36 * h->face_size * sizeof(double)) != cudaSuccess)
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc host-step staging");
   }
+  int prc = step_host_pipelined(h, U_host, dt, fluence_host);
+  if (prc != GFX_ERR_UNSUPPORTED) return prc;
   cudaStream_t s = h->host_stream;
   double* fl = fluence_host ? h->U_stage + 6 * (size_t)h->box.nV : nullptr;
   CUDA_TRY(cudaMemcpyAsync(h->U_stage, U_host, bytes, cudaMemcpyHostToDevice, s));

@@ -125,8 +125,10 @@ int gfx_fluid_fluence_face_size(const gfx_fluid *h, size_t *face_size);
 int gfx_fluid_step(gfx_fluid *h, double *U_dev, double dt, double *fluence_dev,
                    void *stream);
 
-/* The same step with U in host memory: copies in, steps, copies out, and
- * returns after the result is back on the host. */
+/* The same step with U in host memory (pinned for speed): copies in, steps,
+ * copies out, and returns after the result is back on the host.  The copies
+ * and the compute overlap over z slabs (bit-identical to gfx_fluid_step); the
+ * DS field of U_host is not read. */
 int gfx_fluid_step_host(gfx_fluid *h, double *U_host, double dt, double *fluence_host);
 
 /* Integrator ComputeTimeStep (Integrator_Template.f90:896-939) on U_dev:

@@ -1,0 +1,57 @@
+"""gfx_fluid_step_host on host arrays: the pipelined path (z slabs copied in,
+computed and copied back on three streams) gives the device step's result
+bit for bit, state and boundary fluence, over consecutive steps, for every
+kind of z boundary."""
+import numpy as np
+import pytest
+
+from genasis_b200 import problems
+from genasis_b200.config import FluidConfig
+from tests.gpu_helpers import to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    kh_cfg, kh = problems.kelvin_helmholtz(16)
+    kh_cfg = FluidConfig(n_cells=(20, 16, 40), boundary=(("PERIODIC", "PERIODIC"),) * 3,
+                         riemann_solver="HLLC", courant_factor=0.8, n_ramp_cycles=1)
+    rt_cfg, rt = problems.rayleigh_taylor(shape=(16, 12, 36), seed=2)
+    mix = FluidConfig(n_cells=(18, 10, 30), riemann_solver="HLL", courant_factor=0.8,
+                      n_ramp_cycles=1,
+                      boundary=(("OUTFLOW", "REFLECTING"), ("PERIODIC", "PERIODIC"),
+                                ("OUTFLOW", "OUTFLOW")))
+    return {
+        "random_hllc_periodic": (kh_cfg, problems.random_state(kh_cfg, seed=12)),
+        "rt_hllc_gravity_reflecting": (rt_cfg, rt),
+        "random_hll_outflow": (mix, problems.random_state(mix, seed=13)),
+    }
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("z_chunk", [4, 0])
+def test_host_step_matches_the_device_step(name, z_chunk):
+    import torch
+
+    from genasis_b200.fluid import FluidBox
+
+    cfg, prim = CASES[name]
+    dev, hst = FluidBox(cfg), FluidBox(cfg)
+    for box in (dev, hst):
+        box.set_tuning(z_chunk, 0)
+        box.compute_from_primitive(prim)
+    host = dev.U.detach().cpu().pin_memory()
+    fl_dev = dev.new_fluence()
+    fl_host = torch.zeros(tuple(fl_dev.shape), dtype=torch.float64).pin_memory()
+    for i in range(4):
+        dt = dev.compute_time_step(i)
+        dev.step(dt, fl_dev)
+        hst.step_host(host, dt, fl_host)
+        torch.cuda.synchronize()
+        assert torch.equal(host, dev.U.cpu()), (name, z_chunk, i)
+        assert np.array_equal(fl_host.numpy(), to_np(fl_dev)), (name, z_chunk, i)
+    dev.close()
+    hst.close()
