@@ -1245,6 +1245,14 @@ int gfx_fluid_check_state(gfx_fluid* h, const double* U, void* stream) {
   return GFX_OK;
 }
 
+int gfx_fluid_resume(gfx_fluid* h, double* U) {
+  if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  h->prims_pending = false;
+  h->features = FEAT_PENDING;
+  h->features_src = U;
+  return GFX_OK;
+}
+
 int gfx_fluid_totals(gfx_fluid* h, const double* U, double* totals, void* stream) {
   if (!h || !U || !totals) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;

@@ -55,6 +55,7 @@ SIGNATURES = {
     "gfx_fluid_check_state": [P, P, P],
     "gfx_fluid_set_tuning": [P, I, I],
     "gfx_fluid_totals": [P, P, P, P],
+    "gfx_fluid_resume": [P, P],
     "gfx_fluid_last_error": [ctypes.c_char_p, SZ],
 }
 

@@ -231,6 +231,12 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config *cfg, double *U_dev, double dt
  * stream. */
 int gfx_fluid_check_state(gfx_fluid *h, const double *U_dev, void *stream);
 
+/* Restart (Integrator_Template.f90:476-502, 658-764): U_dev holds a state
+ * written by a step of this library (a checkpoint read back); the next step
+ * or evolve continues from it as an uninterrupted run would, detecting the
+ * shock features of U_dev first.  No device work. */
+int gfx_fluid_resume(gfx_fluid *h, double *U_dev);
+
 /* Volume integrals of the six conserved fields of U_dev over the proper
  * cells, sum U dV (the conservation tallies of Current_ASC__Template.f90:
  * 203-349 and VolumeIntegral_Form.f90:25-117, on the device): totals_host[6].

@@ -62,7 +62,7 @@ module GFX_Fluid_C
     gfx_fluid_batch_set_clocks, gfx_fluid_batch_evolve, &
     gfx_fluid_batch_clocks, gfx_fluid_batch_kernel_launches, &
     gfx_fluid_step_noalloc, gfx_fluid_check_state, gfx_fluid_totals, &
-    gfx_fluid_last_error
+    gfx_fluid_resume, gfx_fluid_last_error
 
   interface
 
@@ -285,6 +285,12 @@ module GFX_Fluid_C
       type ( c_ptr ), value :: Handle, Conserved_dev, Stream
       real ( c_double ), intent ( out ) :: Totals ( 6 )
     end function gfx_fluid_totals
+
+    integer ( c_int ) function gfx_fluid_resume ( Handle, Conserved_dev ) &
+      bind ( c, name = 'gfx_fluid_resume' )
+      import
+      type ( c_ptr ), value :: Handle, Conserved_dev
+    end function gfx_fluid_resume
 
     integer ( c_int ) function gfx_fluid_last_error ( Buffer, Length ) &
       bind ( c, name = 'gfx_fluid_last_error' )
