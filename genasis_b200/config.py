@@ -5,7 +5,8 @@ MinCoordinate -> min_coordinate, RiemannSolverType -> riemann_solver, ...);
 defaults are the reference defaults:
   ChartHeader_SL__Form.f90:345-366 (nGhostLayers 2), Chart_Template.f90:178-192
   ([0,1] per axis), Fluid_ASC__Form.f90:128-177 (HLLC, PRIMITIVE, limiter 1.4),
-  Fluid_P_I__Form.f90:210 (gamma 1.4), FluidFeatures_ASC__Form.f90:61-65
+  Fluid_P_I__Form.f90:210 (gamma 1.4), IncrementDivergence_FV__Form.f90:239
+  (ReconstructionType LINEAR), FluidFeatures_ASC__Form.f90:61-65
   (ShockThreshold 0.1), Integrator_C_PS__Form.f90:136 (Courant 0.7),
   IntegratorHeader_Form.f90:95 (nRampCycles 100).
 """
@@ -14,6 +15,7 @@ from dataclasses import dataclass, field
 
 BC = {"OUTFLOW": 0, "REFLECTING": 1, "PERIODIC": 2}
 RIEMANN = {"HLL": 0, "HLLC": 1}
+RECONSTRUCTION = {"LINEAR": 0, "PARABOLIC": 1}
 
 
 class GfxConfig(ctypes.Structure):
@@ -33,6 +35,7 @@ class GfxConfig(ctypes.Structure):
         ("baryon_density_min", ctypes.c_double),
         ("uniform_acceleration", ctypes.c_double),
         ("n_ramp_cycles", ctypes.c_int),
+        ("reconstruction", ctypes.c_int),
     ]
 
 
@@ -53,6 +56,7 @@ class FluidConfig:
     baryon_density_min: float = 0.0
     uniform_acceleration: float = 0.0
     n_ramp_cycles: int = 100
+    reconstruction: str = "LINEAR"  # ReconstructionType: LINEAR or PARABOLIC
 
     @property
     def shape(self):
@@ -90,4 +94,6 @@ class FluidConfig:
         c.baryon_density_min = float(self.baryon_density_min)
         c.uniform_acceleration = float(self.uniform_acceleration)
         c.n_ramp_cycles = int(self.n_ramp_cycles)
+        rc = self.reconstruction
+        c.reconstruction = RECONSTRUCTION[rc] if isinstance(rc, str) else int(rc)
         return c

@@ -28,6 +28,7 @@ struct Phys {
   double courant;
   int use_limiter;
   int n_ramp;
+  int parabolic;  // ReconstructionType PARABOLIC
 };
 
 // Fortran MAX / MIN with gfortran's argument order: the first argument wins ties.
@@ -147,6 +148,98 @@ __device__ __forceinline__ double limited_slope(double vm, double v0, double vp,
   const bool fast = (am == 0.0 || tr > tm * (1.0 + 0x1p-50)) && geo_quotient_in_range(am);
   if (s == 0.0) return 0.0;
   return fast ? s * q : limited_slope_ieee(dvl, dvr, dxl, dxr, sql, sqr, cden, theta);
+}
+
+// PARABOLIC reconstruction of one cell (IncrementDivergence_FV__Kernel.f90:
+// 296-596) with the cell averages XA = X and X2A = X**2 its caller passes
+// (IncrementDivergence_FV__Form.f90:850-927).  g holds per-axis tables over
+// the ghost-inclusive index (entry t of table q at g[q L + t]): the centre, its
+// square, the inner and outer edges, and each denominator of the scheme that
+// depends on the geometry only, with its correctly rounded reciprocal; every
+// division by them is exact (div_rn).  The extremum position divides by a
+// value-dependent quantity and uses the IEEE division.  SqrtTiny is
+// tiny(0.0), as the reference sets it.
+enum {
+  PG_XC, PG_X2, PG_XI, PG_XO,
+  PG_D1, PG_R1, PG_DA, PG_RA, PG_DB, PG_RB,
+  PG_D3, PG_R3, PG_D4A, PG_R4A, PG_D4B, PG_R4B,
+  PG_N
+};
+
+struct FaceVals {
+  double vI, vO;  // inner and outer face values of the cell
+};
+
+__device__ __noinline__ FaceVals parabolic_cell(double vM, double vC, double vP,
+                                                const double* __restrict__ g, int L, int t) {
+  const double SqrtTiny = kTiny;
+  const double xAM = __ldg(g + PG_XC * L + t - 1), xAC = __ldg(g + PG_XC * L + t),
+               xAP = __ldg(g + PG_XC * L + t + 1);
+  const double x2AM = __ldg(g + PG_X2 * L + t - 1), x2AC = __ldg(g + PG_X2 * L + t),
+               x2AP = __ldg(g + PG_X2 * L + t + 1);
+  const double xI = __ldg(g + PG_XI * L + t), xO = __ldg(g + PG_XO * L + t);
+  FaceVals r;
+  if ((vC - vM) * (vP - vC) <= 0.0) {
+    r.vI = vC;
+    r.vO = vC;
+    return r;
+  }
+  double D = __ldg(g + PG_D1 * L + t), R = __ldg(g + PG_R1 * L + t);
+  double c0 = div_rn(vP * (x2AM * xAC - x2AC * xAM) + vM * (x2AC * xAP - x2AP * xAC) +
+                         vC * (x2AP * xAM - x2AM * xAP),
+                     D, R);
+  double c1 = div_rn(vP * (x2AC - x2AM) + vC * (x2AM - x2AP) + vM * (x2AP - x2AC), D, R);
+  double c2 = div_rn(vP * (xAM - xAC) + vM * (xAC - xAP) + vC * (xAP - xAM), D, R);
+  double c2s = copysign(fmax2(fabs(c2), SqrtTiny), c2);
+  double xE = -div_ieee(c1, 2.0 * c2s);
+  double vI = c0 + c1 * xI + c2 * (xI * xI);
+  double vO = c0 + c1 * xO + c2 * (xO * xO);
+  if (xE > xAM && xE <= xAC) {
+    D = __ldg(g + PG_DA * L + t);
+    R = __ldg(g + PG_RA * L + t);
+    c0 = div_rn((vM * x2AC - vC * x2AM) + 2.0 * (vC * xAM - vM * xAC) * xAM, D, R);
+    c1 = -div_rn(2.0 * (vC - vM) * xAM, D, R);
+    c2 = div_rn(vC - vM, D, R);
+    vI = c0 + c1 * xI + c2 * (xI * xI);
+  } else if (xE > xAC && xE < xAP) {
+    D = __ldg(g + PG_DB * L + t);
+    R = __ldg(g + PG_RB * L + t);
+    c0 = div_rn((vP * x2AC - vC * x2AP) + 2.0 * (vC * xAP - vP * xAC) * xAP, D, R);
+    c1 = -div_rn(2.0 * (vC - vP) * xAP, D, R);
+    c2 = div_rn(vC - vP, D, R);
+    vO = c0 + c1 * xO + c2 * (xO * xO);
+  }
+  D = __ldg(g + PG_D3 * L + t);
+  R = __ldg(g + PG_R3 * L + t);
+  c0 = div_rn(vO * xI * (x2AC - xAC * xI) + vC * xI * xO * (xI - xO) +
+                  vI * xO * (xAC * xO - x2AC),
+              D, R);
+  c1 = div_rn(vO * (xI * xI - x2AC) + vI * (x2AC - xO * xO) + vC * (xO * xO - xI * xI), D, R);
+  c2 = div_rn(vO * (xAC - xI) + vC * (xI - xO) + vI * (xO - xAC), D, R);
+  c2s = copysign(fmax2(fabs(c2), SqrtTiny), c2);
+  xE = -div_ieee(c1, 2.0 * c2s);
+  const double vI2 = c0 + c1 * xI + c2 * (xI * xI);
+  const double vO2 = c0 + c1 * xO + c2 * (xO * xO);
+  vI = vI2;
+  vO = vO2;
+  if (xE > xI && xE <= xAC) {
+    D = __ldg(g + PG_D4A * L + t);
+    R = __ldg(g + PG_R4A * L + t);
+    c0 = div_rn((vO * x2AC - vC * (xO * xO)) + 2.0 * xI * (vC * xO - vO * xAC), D, R);
+    c1 = -div_rn(2.0 * (vC - vO) * xI, D, R);
+    c2 = div_rn(vC - vO, D, R);
+    vI = c0 + c1 * xI + c2 * (xI * xI);
+  } else if (xE > xAC && xE < xO) {
+    D = __ldg(g + PG_D4B * L + t);
+    R = __ldg(g + PG_R4B * L + t);
+    c0 = div_rn((vI * x2AC - vC * (xI * xI)) + 2.0 * xO * (vC * xI - vI * xAC), D, R);
+    c1 = -div_rn(2.0 * (vC - vI) * xO, D, R);
+    c2 = div_rn(vC - vI, D, R);
+    vO = c0 + c1 * xO + c2 * (xO * xO);
+  }
+  r.vI = vI;
+  r.vO = vO;
+  return r;
 }
 
 // State at one face after ComputeFromPrimitiveCommon (Fluid_P_I__Form.f90:509-601):

@@ -51,6 +51,7 @@ int fail(int code, const char* fmt, ...) {
 // the centres; the limiter's denominators of Gradient_Kernel.f90:176-180.
 struct HostAxis {
   std::vector<double> X, WL, WR, W, dXI, SQ, CDEN, RDXI, RCDEN, RW;
+  std::vector<double> PAR;  // PG_N tables of m + 1 (parabolic reconstruction)
 };
 
 HostAxis build_axis(int n, double mn, double mx, int g) {
@@ -94,6 +95,35 @@ HostAxis build_axis(int n, double mn, double mx, int g) {
   for (int t = 1; t < m; ++t) a.RDXI[t] = 1.0 / a.dXI[t];
   for (int t = 1; t + 1 < m; ++t) a.RCDEN[t] = 1.0 / a.CDEN[t];
   for (int t = 0; t < m; ++t) a.RW[t] = 1.0 / a.W[t];
+  // PARABOLIC: centre, its square, inner and outer edges, and the geometry
+  // denominators of IncrementDivergence_FV__Kernel.f90:382-575 for the cells
+  // that have both neighbours, with their rounded reciprocals
+  const int L = m + 1;
+  a.PAR.assign((size_t)PG_N * L, 0.0);
+  auto P = [&](int q, int t) -> double& { return a.PAR[(size_t)q * L + t]; };
+  for (int t = 0; t < m; ++t) {
+    P(PG_XC, t) = a.X[t];
+    P(PG_X2, t) = a.X[t] * a.X[t];
+    P(PG_XI, t) = a.X[t] - a.WL[t];
+    P(PG_XO, t) = a.X[t] + a.WR[t];
+  }
+  for (int t = 1; t + 1 < m; ++t) {
+    const double xAM = a.X[t - 1], xAC = a.X[t], xAP = a.X[t + 1];
+    const double x2AM = xAM * xAM, x2AC = xAC * xAC, x2AP = xAP * xAP;
+    const double xI = P(PG_XI, t), xO = P(PG_XO, t);
+    const double D[6] = {
+        (x2AM - x2AP) * xAC + (x2AP - x2AC) * xAM + (x2AC - x2AM) * xAP,
+        (x2AC - x2AM) + 2.0 * (xAM - xAC) * xAM,
+        (x2AC - x2AP) + 2.0 * (xAP - xAC) * xAP,
+        (xI - xO) * (x2AC + xI * xO - xAC * (xI + xO)),
+        (x2AC - xO * xO) + 2.0 * xI * (xO - xAC),
+        (x2AC - xI * xI) + 2.0 * xO * (xI - xAC)};
+    const int qd[6] = {PG_D1, PG_DA, PG_DB, PG_D3, PG_D4A, PG_D4B};
+    for (int e = 0; e < 6; ++e) {
+      P(qd[e], t) = D[e];
+      P(qd[e] + 1, t) = 1.0 / D[e];
+    }
+  }
   return a;
 }
 
@@ -163,14 +193,15 @@ struct gfx_fluid {
 
 namespace {
 
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED>
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED,
+          bool PARAB = false>
 cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
                            int n_items, int* counter, const Phys& ph, cudaStream_t s) {
   using SM = StageLayout<NF>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int per_sm = 1;
-  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BATCHED>;
+  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BATCHED, PARAB>;
   std::call_once(once, [&] {
     attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)SM::kBytes);
@@ -185,10 +216,40 @@ cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const Work
   return cudaGetLastError();
 }
 
+// The PARABOLIC variants (single bricks only).
+cudaError_t launch_stage_parabolic(int mode, bool in_prim, bool hllc, bool grav,
+                                   const BrickDesc& d, const WorkItem* items, int n_items,
+                                   int* counter, const Phys& ph, cudaStream_t s) {
+#define GFX_PSTAGE(M, IP, HC, GR, NF)                                                     \
+  if (mode == M && in_prim == IP && hllc == HC && grav == GR)                            \
+    return launch_stage_t<M, IP, HC, GR, NF, false, true>(d, nullptr, items, n_items,     \
+                                                          counter, ph, s);
+  GFX_PSTAGE(MODE_INCREMENT, false, false, false, 6)
+  GFX_PSTAGE(MODE_INCREMENT, false, true, false, 6)
+  GFX_PSTAGE(MODE_INCREMENT, true, false, false, 6)
+  GFX_PSTAGE(MODE_INCREMENT, true, true, false, 6)
+  GFX_PSTAGE(MODE_STAGE1, false, false, false, 5)
+  GFX_PSTAGE(MODE_STAGE1, false, true, false, 5)
+  GFX_PSTAGE(MODE_STAGE1, false, false, true, 5)
+  GFX_PSTAGE(MODE_STAGE1, false, true, true, 5)
+  GFX_PSTAGE(MODE_STAGE1, true, false, false, 5)
+  GFX_PSTAGE(MODE_STAGE1, true, true, false, 5)
+  GFX_PSTAGE(MODE_STAGE1, true, false, true, 5)
+  GFX_PSTAGE(MODE_STAGE1, true, true, true, 5)
+  GFX_PSTAGE(MODE_STAGE2, true, false, false, 5)
+  GFX_PSTAGE(MODE_STAGE2, true, true, false, 5)
+  GFX_PSTAGE(MODE_STAGE2, true, false, true, 5)
+  GFX_PSTAGE(MODE_STAGE2, true, true, true, 5)
+#undef GFX_PSTAGE
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const BrickDesc& d,
                          const BrickDesc* many, const WorkItem* items, int n_items,
                          int* counter, const Phys& ph, cudaStream_t s) {
   const bool bat = many != nullptr;
+  if (!bat && d.geo[0].PAR != nullptr && ph.parabolic)
+    return launch_stage_parabolic(mode, in_prim, hllc, grav, d, items, n_items, counter, ph, s);
 #define GFX_STAGE(M, IP, HC, GR, NF, BA)                                                  \
   if (mode == M && in_prim == IP && hllc == HC && grav == GR && bat == BA)              \
     return launch_stage_t<M, IP, HC, GR, NF, BA>(d, many, items, n_items, counter, ph, s);
@@ -248,6 +309,9 @@ int validate(const gfx_fluid_config* c) {
     return fail(GFX_ERR_ARGUMENT, "riemann_solver = %d", c->riemann_solver);
   if (!(c->adiabatic_index > 1.0)) return fail(GFX_ERR_ARGUMENT, "adiabatic_index must be > 1");
   if (c->n_ramp_cycles < 1) return fail(GFX_ERR_ARGUMENT, "n_ramp_cycles must be >= 1");
+  if (c->reconstruction != GFX_RECONSTRUCTION_LINEAR &&
+      c->reconstruction != GFX_RECONSTRUCTION_PARABOLIC)
+    return fail(GFX_ERR_ARGUMENT, "reconstruction = %d", c->reconstruction);
   if (!(c->courant_factor > 0.0)) return fail(GFX_ERR_ARGUMENT, "courant_factor must be > 0");
   return GFX_OK;
 }
@@ -602,6 +666,7 @@ int gfx_fluid_config_default(gfx_fluid_config* c) {
   c->baryon_density_min = 0.0;
   c->uniform_acceleration = 0.0;
   c->n_ramp_cycles = 100;
+  c->reconstruction = GFX_RECONSTRUCTION_LINEAR;
   return GFX_OK;
 }
 
@@ -624,6 +689,7 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
   ph.courant = cfg->courant_factor;
   ph.use_limiter = cfg->use_limiter ? 1 : 0;
   ph.n_ramp = cfg->n_ramp_cycles;
+  ph.parabolic = cfg->reconstruction == GFX_RECONSTRUCTION_PARABOLIC ? 1 : 0;
   Box& b = h->box;
   for (int d = 0; d < 3; ++d) {
     b.n[d] = cfg->n_cells[d];
@@ -640,9 +706,9 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
     gfx_fluid_destroy(h);
     return code;
   };
-  // geometry arena: 6 tables per axis, each m + 1 long
+  // geometry arena: 9 tables per axis, then the PG_N parabolic ones, each m + 1 long
   size_t geo_len = 0;
-  for (int d = 0; d < 3; ++d) geo_len += 9 * (size_t)(b.m[d] + 1);
+  for (int d = 0; d < 3; ++d) geo_len += (9 + PG_N) * (size_t)(b.m[d] + 1);
   if (cudaMalloc(&h->geo, geo_len * sizeof(double)) != cudaSuccess)
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc geometry"));
   {
@@ -662,6 +728,9 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
         *dst[q] = h->geo + off;
         off += L;
       }
+      std::copy(a.PAR.begin(), a.PAR.end(), host.begin() + off);
+      h->dgeo[d].PAR = h->geo + off;
+      off += (size_t)PG_N * L;
     }
     if (cudaMemcpy(h->geo, host.data(), geo_len * sizeof(double), cudaMemcpyHostToDevice) !=
         cudaSuccess)
@@ -1018,6 +1087,9 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
   }
   if (c0.uniform_acceleration != 0.0)
     return fail(GFX_ERR_UNSUPPORTED, "batched bricks with gravity are not built");
+  for (int b = 0; b < n; ++b)
+    if (handles[b]->cfg.reconstruction != GFX_RECONSTRUCTION_LINEAR)
+      return fail(GFX_ERR_UNSUPPORTED, "batched bricks: LINEAR reconstruction only");
   gfx_fluid_batch* B = new (std::nothrow) gfx_fluid_batch();
   if (!B) return fail(GFX_ERR_NO_MEMORY, "host allocation failed");
   auto cleanup = [&](int code) {
@@ -1464,6 +1536,8 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
   int rc = validate(cfg);
   if (rc) return rc;
   if (!U) return fail(GFX_ERR_ARGUMENT, "U_dev is NULL");
+  if (cfg->reconstruction != GFX_RECONSTRUCTION_LINEAR)
+    return fail(GFX_ERR_UNSUPPORTED, "the no-allocation step: LINEAR reconstruction only");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   // the parameters and chart of gfx_fluid_create, without the handle
   Phys ph;
@@ -1671,6 +1745,8 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
                            void* stream) {
   if (!h || !U_n || !lam_np1 || !lam_n) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (lam_n == lam_np1) return fail(GFX_ERR_ARGUMENT, "lam_n must not alias lam_np1");
+  if (h->cfg.reconstruction != GFX_RECONSTRUCTION_LINEAR)
+    return fail(GFX_ERR_UNSUPPORTED, "adjoint: LINEAR reconstruction only");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   cudaStream_t s = (cudaStream_t)stream;
   const Box& b = h->box;

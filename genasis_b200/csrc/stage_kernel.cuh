@@ -42,6 +42,7 @@ struct AxisGeo {
   const double* RDXI;   // RN(1 / dXI(t))
   const double* RCDEN;  // RN(1 / CDEN(t))
   const double* RW;     // RN(1 / W(t))
+  const double* PAR;    // PARABOLIC tables [PG_N][m + 1] (fluid_physics.cuh), or null
 };
 
 struct BrickDesc {
@@ -335,14 +336,9 @@ __device__ __forceinline__ void z_slope(const AxisGeo& GZ, const Phys& ph, int p
 // Flux through the z face between planes p-1 (values a, slopes sm_) and p
 // (values b, slopes sp) of the own column (gx, gy), with its boundary fluence.
 template <bool HLLC, int NF>
-__device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p,
-                                       const double* a, int sa, const double* sm_, int ssm,
-                                       const double* b, int sb, const double* sp, int ssp,
-                                       int gx, int gy, bool own, double dt, double* F) {
-  const AxisGeo& GZ = B.geo[2];
-  double l[5], r[5];
-  face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2), l,
-             r);
+__device__ __forceinline__ void z_face_lr(const BrickDesc& B, const Phys& ph, int p,
+                                          const double* l, const double* r, int gx, int gy,
+                                          bool own, double dt, double* F) {
   FaceState L, R;
   face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
   face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
@@ -353,12 +349,40 @@ __device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p
                                   B.weight * dt);
 }
 
+template <bool HLLC, int NF>
+__device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p,
+                                       const double* a, int sa, const double* sm_, int ssm,
+                                       const double* b, int sb, const double* sp, int ssp,
+                                       int gx, int gy, bool own, double dt, double* F) {
+  const AxisGeo& GZ = B.geo[2];
+  double l[5], r[5];
+  face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2), l,
+             r);
+  z_face_lr<HLLC, NF>(B, ph, p, l, r, gx, gy, own, dt, F);
+}
+
+// PARABOLIC: inner and outer face values of the 5 primitives of the own
+// column's cell at plane p from the values a (p-1), b (p), c (p+1).
+__device__ __forceinline__ void z_parabolic(const BrickDesc& B, int p, const double* a, int sa,
+                                            const double* b, int sb, const double* c, int sc,
+                                            double* vI, double* vO) {
+  const int L = B.m[2] + 1;
+#pragma unroll 1
+  for (int q = 0; q < 5; ++q) {
+    const FaceVals f = parabolic_cell(a[q * sa], b[q * sb], c[q * sc], B.geo[2].PAR, L, p + 2);
+    vI[q] = f.vI;
+    vO[q] = f.vO;
+  }
+}
+
 // Prologue of a work item (own column only): planes z0-2 .. z0+1, the z
 // slopes at z0-1 and z0 and the z face z0, left in zss / zfs and the centre
 // slots for the plane loop.  Out of line: it runs once per item, and a second
 // inlined copy of the slope and face code would only crowd the instruction
 // cache of the plane loop.
-template <bool IN_PRIM, bool HLLC, int NF>
+// PARABOLIC (PARAB): zss keeps the outer face values of plane z0 instead of
+// its slopes.
+template <bool IN_PRIM, bool HLLC, int NF, bool PARAB>
 __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, double* full,
                                             double* cen, double* zss, double* zfs, int tid,
                                             int tx, int ty, int gx, int gy, int z0, bool own,
@@ -368,13 +392,22 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
   load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 - 2);
   load_cell_col<IN_PRIM>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
   load_cell_col<IN_PRIM>(B, ph, cslot(z0), gx, gy, z0);
-  double s_m[5], s_0[5];
-  z_slope(B.geo[2], ph, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
+  double s_m[5], s_0[5], vI0[5];
+  if (PARAB)
+    z_parabolic(B, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, vI0, s_m);
+  else
+    z_slope(B.geo[2], ph, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
   load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 + 1);
-  z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, s_0);
+  if (PARAB)
+    z_parabolic(B, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, vI0, s_0);
+  else
+    z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, s_0);
   double F[NF];
-  z_face<HLLC, NF>(B, ph, z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, gx, gy, own, dt,
-                   F);
+  if (PARAB)
+    z_face_lr<HLLC, NF>(B, ph, z0, s_m, vI0, gx, gy, own, dt, F);
+  else
+    z_face<HLLC, NF>(B, ph, z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, gx, gy, own,
+                     dt, F);
 #pragma unroll
   for (int q = 0; q < 5; ++q) zss[q * NT + tid] = s_0[q];
 #pragma unroll
@@ -388,7 +421,9 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
 // BATCHED: the work items span many bricks; each item's brick descriptor is
 // copied from `many` into shared memory.  Otherwise `single` describes the one
 // brick (read from the constant bank).
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED>
+// PARAB: PARABOLIC reconstruction (single bricks): no slope phase; each face
+// reconstructs its two cells, the own column carries outer face values in z.
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED, bool PARAB = false>
 __global__ void __launch_bounds__(NT, kMinCtas)
     stage_kernel(const __grid_constant__ BrickDesc single, const BrickDesc* __restrict__ many,
                  const WorkItem* __restrict__ items, int n_items, int* __restrict__ counter,
@@ -447,8 +482,8 @@ __global__ void __launch_bounds__(NT, kMinCtas)
     // (centre slots) or PS (full plane)
     auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
     // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
-    stage_prologue<IN_PRIM, HLLC, NF>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx, gy, z0, own,
-                                      dt);
+    stage_prologue<IN_PRIM, HLLC, NF, PARAB>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx, gy,
+                                             z0, own, dt);
     __syncthreads();  // geometry caches
 
     for (int k = z0; k < z1; ++k) {
@@ -477,7 +512,7 @@ __global__ void __launch_bounds__(NT, kMinCtas)
       __syncthreads();
 
       // (2) slopes: x [TY][TX+2], y [TY+2][TX] of plane k
-      {
+      if (!PARAB) {
         constexpr int NXS = TY * (TX + 2), NYS = (TY + 2) * TX;
         constexpr int PXS = (NXS + 31) / 32 * 32;
         for (int i = tid; i < PXS + NYS; i += NT) {
@@ -525,8 +560,21 @@ __global__ void __launch_bounds__(NT, kMinCtas)
           const double wr = isx ? gxc[G_WR * LX + lx + 1] : gyc[G_WR * LY + ly + 1];
           const double wl = isx ? gxc[G_WL * LX + lx + 2] : gyc[G_WL * LY + ly + 2];
           double l[5], r[5];
-          face_prims(full + o - step, sl, PS, full + o, sl + sstep, PS, sstride, sstride, wr,
-                     wl, l, r);
+          if (PARAB) {
+            // V_IL = outer value of the cell before, V_IR = inner value of the cell after
+            const double* g = isx ? B.geo[0].PAR : B.geo[1].PAR;
+            const int L = (isx ? B.m[0] : B.m[1]) + 1;
+            const int tm = (isx ? cx : cy) + 1;  // ghost-layout index of the cell before
+#pragma unroll 1
+            for (int q = 0; q < 5; ++q) {
+              const double* v = full + q * PS + o - step;
+              l[q] = parabolic_cell(v[-step], v[0], v[step], g, L, tm).vO;
+              r[q] = parabolic_cell(v[0], v[step], v[2 * step], g, L, tm + 1).vI;
+            }
+          } else {
+            face_prims(full + o - step, sl, PS, full + o, sl + sstep, PS, sstride, sstride, wr,
+                       wl, l, r);
+          }
           FaceState L, R;
           face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
           face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
@@ -559,9 +607,19 @@ __global__ void __launch_bounds__(NT, kMinCtas)
 
       // (4) z slope at k+1 and z face k+1 of the own column
       double zsn[5], zfn[NF];
-      z_slope(GZ, ph, k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
-      z_face<HLLC, NF>(B, ph, k + 1, full + c_off, PS, zss + tid, NT, cslot(k + 1), NT, zsn, 1,
-                       gx, gy, own, dt, zfn);
+      if (PARAB) {
+        // zsn: the outer values of plane k+1; the face takes the outer
+        // values of plane k (zss) and the inner ones of plane k+1
+        double zI[5], zl[5];
+        z_parabolic(B, k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zI, zsn);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) zl[q] = zss[q * NT + tid];
+        z_face_lr<HLLC, NF>(B, ph, k + 1, zl, zI, gx, gy, own, dt, zfn);
+      } else {
+        z_slope(GZ, ph, k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
+        z_face<HLLC, NF>(B, ph, k + 1, full + c_off, PS, zss + tid, NT, cslot(k + 1), NT, zsn,
+                         1, gx, gy, own, dt, zfn);
+      }
       __syncthreads();
 
       // (5) cell update and stage epilogue

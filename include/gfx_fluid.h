@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define GFX_FLUID_ABI_VERSION 1
+#define GFX_FLUID_ABI_VERSION 2
 
 enum gfx_status {
   GFX_OK = 0,
@@ -45,6 +45,9 @@ enum gfx_status {
 enum { GFX_BC_OUTFLOW = 0, GFX_BC_REFLECTING = 1, GFX_BC_PERIODIC = 2 };
 /* Fluid_ASC RiemannSolverType (Fluid_ASC__Form.f90:128-137) */
 enum { GFX_RIEMANN_HLL = 0, GFX_RIEMANN_HLLC = 1 };
+/* IncrementDivergence_FV ReconstructionType (IncrementDivergence_FV__Form.f90:
+ * 239, 637-655): PLM with the limiter, or PARABOLIC (Kernel.f90:296-596) */
+enum { GFX_RECONSTRUCTION_LINEAR = 0, GFX_RECONSTRUCTION_PARABOLIC = 1 };
 
 /* Parameters of one single-brick chart + Fluid_P_I + Step_RK2 + Integrator.
  * Names follow the reference's GetParameter names; gfx_fluid_config_default
@@ -64,6 +67,9 @@ typedef struct gfx_fluid_config {
   double baryon_density_min;    /* BaryonDensityMin (0) */
   double uniform_acceleration;  /* UniformAcceleration along z (0 = no gravity) */
   int    n_ramp_cycles;         /* nRampCycles (100) */
+  int    reconstruction;        /* ReconstructionType (LINEAR); PARABOLIC for single
+                                   bricks' step and increment (not batch, adjoint,
+                                   no-allocation step) */
 } gfx_fluid_config;
 
 typedef struct gfx_fluid gfx_fluid;

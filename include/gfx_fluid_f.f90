@@ -29,7 +29,9 @@ module GFX_Fluid_C
     GFX_BC_REFLECTING = 1, &
     GFX_BC_PERIODIC = 2, &
     GFX_RIEMANN_HLL = 0, &
-    GFX_RIEMANN_HLLC = 1
+    GFX_RIEMANN_HLLC = 1, &
+    GFX_RECONSTRUCTION_LINEAR = 0, &
+    GFX_RECONSTRUCTION_PARABOLIC = 1
 
   !-- gfx_fluid_config; Boundary ( iSide, iDimension ) is the C
   !   boundary[iDimension][iSide] (row-major there, column-major here)
@@ -48,6 +50,7 @@ module GFX_Fluid_C
     real ( c_double ) :: BaryonDensityMin
     real ( c_double ) :: UniformAcceleration
     integer ( c_int ) :: nRampCycles
+    integer ( c_int ) :: ReconstructionType  !-- GFX_RECONSTRUCTION_*
   end type GFX_FluidConfig
 
   public :: &

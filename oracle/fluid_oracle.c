@@ -84,6 +84,7 @@ struct ora_fluid {
   double *DF[3], *SHOCK, *SHOCK_I[3];
   /* scratch of the divergence increment */
   double *dX_I, *dV_I, *dVdX[NPRIM], *F_I[NCONS];
+  double *VO[NPRIM]; /* PARABOLIC: outer face value of each cell (dVdX holds the inner) */
   /* RK storages */
   double *Sol[NCONS], *Y[NCONS], *K[2][NCONS];
 };
@@ -167,7 +168,10 @@ ora_fluid *ora_create(const ora_config *cfg) {
   }
   f->SHOCK = alloc_field(nV);
   f->dX_I = alloc_field(nV); f->dV_I = alloc_field(nV);
-  for (int v = 0; v < NPRIM; ++v) f->dVdX[v] = alloc_field(nV);
+  for (int v = 0; v < NPRIM; ++v) {
+    f->dVdX[v] = alloc_field(nV);
+    f->VO[v] = alloc_field(nV);
+  }
   for (int v = 0; v < NCONS; ++v) {
     f->F_I[v] = alloc_field(nV);
     f->Sol[v] = alloc_field(nV); f->Y[v] = alloc_field(nV);
@@ -185,7 +189,10 @@ void ora_destroy(ora_fluid *f) {
   }
   free(f->N); free(f->E); free(f->D); free(f->Gc); free(f->DS); free(f->P);
   free(f->SB); free(f->CS); free(f->SHOCK); free(f->dX_I); free(f->dV_I);
-  for (int v = 0; v < NPRIM; ++v) free(f->dVdX[v]);
+  for (int v = 0; v < NPRIM; ++v) {
+    free(f->dVdX[v]);
+    free(f->VO[v]);
+  }
   for (int v = 0; v < NCONS; ++v) {
     free(f->F_I[v]); free(f->Sol[v]); free(f->Y[v]); free(f->K[0][v]); free(f->K[1][v]);
   }
@@ -484,6 +491,77 @@ static inline void face_flux(const ora_fluid *f, const face_state *L, const face
 /* IncrementDivergence_FV % Compute (IncrementDivergence_FV__Form.f90:344-412) */
 /* ---------------------------------------------------------------------- */
 
+/* ComputeReconstructionParabolic_CSL_Kernel (IncrementDivergence_FV__Kernel.f90:
+ * 296-596) for one cell, with the cell averages XA = X and X2A = X**2 that its
+ * caller passes (IncrementDivergence_FV__Form.f90:850-927): a parabola through
+ * the three cell values, adjusted where it has an extremum inside the cell
+ * pair, then a second parabola through the face values and the cell value,
+ * adjusted likewise.  Fortran's left-to-right evaluation and x**2 = x*x are
+ * kept; SqrtTiny is tiny(0.0) as the reference sets it.  Returns the inner
+ * (vI) and outer (vO) face values of the cell. */
+static void parabolic_cell(double vM, double vC, double vP, double xM, double xC, double xP,
+                           double xI, double xO, double *pvI, double *pvO) {
+  const double SqrtTiny = DBL_MIN;
+  const double xAM = xM, xAC = xC, xAP = xP;
+  const double x2AM = xM * xM, x2AC = xC * xC, x2AP = xP * xP;
+  double vI, vO, D, c0, c1, c2, c2_Safe, xE;
+  if ((vC - vM) * (vP - vC) <= 0.0) {
+    vI = vC;
+    vO = vC;
+  } else {
+    /* first parabola */
+    D = (x2AM - x2AP) * xAC + (x2AP - x2AC) * xAM + (x2AC - x2AM) * xAP;
+    c0 = (vP * (x2AM * xAC - x2AC * xAM) + vM * (x2AC * xAP - x2AP * xAC) +
+          vC * (x2AP * xAM - x2AM * xAP)) / D;
+    c1 = (vP * (x2AC - x2AM) + vC * (x2AM - x2AP) + vM * (x2AP - x2AC)) / D;
+    c2 = (vP * (xAM - xAC) + vM * (xAC - xAP) + vC * (xAP - xAM)) / D;
+    c2_Safe = copysign(fmax2(fabs(c2), SqrtTiny), c2);
+    xE = -(c1 / (2.0 * c2_Safe));
+    vI = c0 + c1 * xI + c2 * (xI * xI);
+    vO = c0 + c1 * xO + c2 * (xO * xO);
+    /* extremum of the first parabola inside (xM, xC] or (xC, xP) */
+    if (xE > xM && xE <= xC) {
+      D = (x2AC - x2AM) + 2.0 * (xAM - xAC) * xAM;
+      c0 = ((vM * x2AC - vC * x2AM) + 2.0 * (vC * xAM - vM * xAC) * xAM) / D;
+      c1 = -(2.0 * (vC - vM) * xAM / D);
+      c2 = (vC - vM) / D;
+      vI = c0 + c1 * xI + c2 * (xI * xI);
+    } else if (xE > xC && xE < xP) {
+      D = (x2AC - x2AP) + 2.0 * (xAP - xAC) * xAP;
+      c0 = ((vP * x2AC - vC * x2AP) + 2.0 * (vC * xAP - vP * xAC) * xAP) / D;
+      c1 = -(2.0 * (vC - vP) * xAP / D);
+      c2 = (vC - vP) / D;
+      vO = c0 + c1 * xO + c2 * (xO * xO);
+    }
+    /* second parabola, through vI, vC (as the average) and vO */
+    D = (xI - xO) * (x2AC + xI * xO - xAC * (xI + xO));
+    c0 = (vO * xI * (x2AC - xAC * xI) + vC * xI * xO * (xI - xO) + vI * xO * (xAC * xO - x2AC)) /
+         D;
+    c1 = (vO * (xI * xI - x2AC) + vI * (x2AC - xO * xO) + vC * (xO * xO - xI * xI)) / D;
+    c2 = (vO * (xAC - xI) + vC * (xI - xO) + vI * (xO - xAC)) / D;
+    c2_Safe = copysign(fmax2(fabs(c2), SqrtTiny), c2);
+    xE = -(c1 / (2.0 * c2_Safe));
+    vI = c0 + c1 * xI + c2 * (xI * xI);
+    vO = c0 + c1 * xO + c2 * (xO * xO);
+    /* extremum of the second parabola inside (xI, xC] or (xC, xO) */
+    if (xE > xI && xE <= xC) {
+      D = (x2AC - xO * xO) + 2.0 * xI * (xO - xAC);
+      c0 = ((vO * x2AC - vC * (xO * xO)) + 2.0 * xI * (vC * xO - vO * xAC)) / D;
+      c1 = -(2.0 * (vC - vO) * xI / D);
+      c2 = (vC - vO) / D;
+      vI = c0 + c1 * xI + c2 * (xI * xI);
+    } else if (xE > xC && xE < xO) {
+      D = (x2AC - xI * xI) + 2.0 * xO * (xI - xAC);
+      c0 = ((vI * x2AC - vC * (xI * xI)) + 2.0 * xO * (vC * xI - vI * xAC)) / D;
+      c1 = -(2.0 * (vC - vI) * xO / D);
+      c2 = (vC - vI) / D;
+      vO = c0 + c1 * xO + c2 * (xO * xO);
+    }
+  }
+  *pvI = vI;
+  *pvO = vO;
+}
+
 static void compute_direction(ora_fluid *f, int d, double **dU, double dT, double weight,
                               double *fluence) {
   const int g = f->g;
@@ -525,6 +603,23 @@ static void compute_direction(ora_fluid *f, int d, double **dU, double dT, doubl
     if (v < 0) continue;
     h3[d] = f->m[d] - 2;
     double *slope = f->dVdX[v];
+    if (f->c.reconstruction == ORA_PARABOLIC) {
+      /* inner face values into dVdX, outer ones into VO */
+      double *outer = f->VO[v];
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int k = l3[2]; k <= h3[2]; ++k)
+        for (int j = l3[1]; j <= h3[1]; ++j)
+          for (int i = l3[0]; i <= h3[0]; ++i) {
+            int t[3] = {i, j, k};
+            size_t iV = idx3(f, i, j, k);
+            const int c = t[d];
+            const double xC = f->X[d][c];
+            parabolic_cell(src[iV - sd], src[iV], src[iV + sd], f->X[d][c - 1], xC,
+                           f->X[d][c + 1], xC - f->WL[d][c], xC + f->WR[d][c], &slope[iV],
+                           &outer[iV]);
+          }
+      continue;
+    }
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = l3[2]; k <= h3[2]; ++k)
       for (int j = l3[1]; j <= h3[1]; ++j)
@@ -556,9 +651,17 @@ static void compute_direction(ora_fluid *f, int d, double **dU, double dT, doubl
           int t[3] = {i, j, k};
           size_t iV = idx3(f, i, j, k), iM = iV - sd;
           double pl[NPRIM], pr[NPRIM];
-          for (int v = 0; v < NPRIM; ++v) {
-            pl[v] = prim[v][iM] + f->WR[d][t[d] - 1] * f->dVdX[v][iM];
-            pr[v] = prim[v][iV] - f->WL[d][t[d]] * f->dVdX[v][iV];
+          if (f->c.reconstruction == ORA_PARABOLIC) {
+            /* V_IL(i) = vO(i-1), V_IR(i) = vI(i) (Kernel.f90:588-589) */
+            for (int v = 0; v < NPRIM; ++v) {
+              pl[v] = f->VO[v][iM];
+              pr[v] = f->dVdX[v][iV];
+            }
+          } else {
+            for (int v = 0; v < NPRIM; ++v) {
+              pl[v] = prim[v][iM] + f->WR[d][t[d] - 1] * f->dVdX[v][iM];
+              pr[v] = prim[v][iV] - f->WL[d][t[d]] * f->dVdX[v][iV];
+            }
           }
           face_state L, R;
           prim_to_cons(f, pl, d, &L);

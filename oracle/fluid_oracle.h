@@ -24,6 +24,7 @@ extern "C" {
 
 enum { ORA_BC_OUTFLOW = 0, ORA_BC_REFLECTING = 1, ORA_BC_PERIODIC = 2 };
 enum { ORA_HLL = 0, ORA_HLLC = 1 };
+enum { ORA_LINEAR = 0, ORA_PARABOLIC = 1 };
 
 typedef struct ora_config {
   int    n_cells[3];
@@ -40,6 +41,7 @@ typedef struct ora_config {
   double baryon_density_min;
   double uniform_acceleration;
   int    n_ramp_cycles;
+  int    reconstruction;  /* 0 = LINEAR (PLM), 1 = PARABOLIC */
 } ora_config;
 
 typedef struct ora_fluid ora_fluid;

@@ -18,6 +18,7 @@ _lib = None
 
 BC = {"OUTFLOW": 0, "REFLECTING": 1, "PERIODIC": 2}
 RIEMANN = {"HLL": 0, "HLLC": 1}
+RECONSTRUCTION = {"LINEAR": 0, "PARABOLIC": 1}
 
 
 class OraConfig(ctypes.Structure):
@@ -36,6 +37,7 @@ class OraConfig(ctypes.Structure):
         ("baryon_density_min", ctypes.c_double),
         ("uniform_acceleration", ctypes.c_double),
         ("n_ramp_cycles", ctypes.c_int),
+        ("reconstruction", ctypes.c_int),
     ]
 
 
@@ -100,6 +102,8 @@ def make_config(cfg):
     c.baryon_density_min = float(cfg.baryon_density_min)
     c.uniform_acceleration = float(cfg.uniform_acceleration)
     c.n_ramp_cycles = int(cfg.n_ramp_cycles)
+    rc = getattr(cfg, "reconstruction", "LINEAR")
+    c.reconstruction = RECONSTRUCTION[rc] if isinstance(rc, str) else int(rc)
     return c
 
 

@@ -14,6 +14,10 @@
 #define __forceinline__ inline
 #define __noinline__
 static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
+template <class T>
+static inline T __ldg(const T* p) {
+  return *p;
+}
 static inline long long __double_as_longlong(double x) {
   long long u;
   std::memcpy(&u, &x, 8);

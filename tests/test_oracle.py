@@ -291,3 +291,73 @@ def test_time_step_ramp():
     assert o.timestep(4) == pytest.approx(0.5 * full, rel=1e-15)
     tsi = o.inverse_timestep()
     assert full == cfg.courant_factor * (1.0 / tsi)
+
+
+# ---- PARABOLIC reconstruction (IncrementDivergence_FV__Kernel.f90:296-596) ----
+
+def test_parabolic_reconstructs_a_linear_profile_exactly():
+    n = 24
+    cfg = FluidConfig(n_cells=(n, 4, 4), riemann_solver="HLL", reconstruction="PARABOLIC")
+    X, Y, Z = problems.centers(cfg)
+    prim = np.zeros((5,) + cfg.shape)
+    prim[0] = 1.0 + 0.5 * X
+    prim[1] = 1.0
+    prim[4] = 2.5
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    dt = 1e-3
+    K = o.increment(dt)
+    kd = K[0][cfg.proper][:, :, 3:-3]
+    assert np.allclose(kd, -dt * 0.5, rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("rs", ["HLL", "HLLC"])
+def test_parabolic_periodic_totals_are_conserved(rs):
+    cfg, prim = problems.sine_wave(16, riemann_solver=rs)
+    cfg.reconstruction = "PARABOLIC"
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    U0 = o.conserved()
+    for i in range(4):
+        o.step(o.timestep(i))
+    U1 = o.conserved()
+    p = cfg.proper
+    for f in range(5):
+        scale = np.abs(U0[f][p]).sum() + 1.0
+        assert abs(U1[f][p].sum() - U0[f][p].sum()) <= 1e-13 * scale
+
+
+def test_parabolic_is_more_accurate_than_linear_on_the_sine_wave():
+    errs = {}
+    for rec in ("LINEAR", "PARABOLIC"):
+        cfg, prim = problems.sine_wave(24)
+        cfg.reconstruction = rec
+        o = Oracle(cfg)
+        o.set_primitive(prim)
+        t, i = 0.0, 0
+        while t < 0.1:
+            dt = o.timestep(i)
+            o.step(dt)
+            t += dt
+            i += 1
+        errs[rec] = problems.l1_error(o.primitive()[0], problems.sine_density(cfg, t), cfg)
+    assert errs["PARABOLIC"] < 0.8 * errs["LINEAR"], errs
+
+
+def test_parabolic_keeps_sod_close_to_the_exact_solution():
+    n = 96
+    cfg = FluidConfig(n_cells=(n, 4, 4), riemann_solver="HLL", courant_factor=0.8,
+                      n_ramp_cycles=1, reconstruction="PARABOLIC")
+    prim = problems.riemann(cfg, 1.0, 1.0, (0, 0, 0), 0.125, 0.1, (0, 0, 0), (0.5, 0, 0),
+                            (1.0, 0, 0))
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    t, i = 0.0, 0
+    while t < 0.15 - 1e-14:
+        dt = min(o.timestep(i), 0.15 - t)
+        o.step(dt)
+        t += dt
+        i += 1
+    x = problems.axis_geometry(n, 0.0, 1.0)[0][2:-2]
+    rho = o.conserved()[0][cfg.proper][2, 2, :]
+    assert np.abs(rho - _exact_sod_density(x, t)).mean() < 0.02
