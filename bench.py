@@ -233,11 +233,13 @@ def run_ours(args):
 
     world, rank, local = dist_init()
     from genasis_b200 import problems
-    from genasis_b200.fluid import FluidBox
 
     cfg, prim = problems.sine_wave(args.n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
     cells = cfg.n_proper
-    box = FluidBox(cfg, device="cuda:%d" % local)
+    # the pencil length from the autotuner's table (tuned here if absent)
+    from genasis_b200 import autotune
+
+    box = autotune.tuned_box(cfg, adjoint=False)
     box.compute_from_primitive(prim)
     del prim
     stream = torch.cuda.current_stream()
@@ -343,7 +345,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (state %.0f MB)" % (
                            6 * box.n_values * 8 / 1e6),
                        "l1_density_error": l1, "sim_time": t_sim,
-                       "full_crossing": crossing},
+                       "full_crossing": crossing, "tuning": {"z_chunk": box.tuning[0]}},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -567,14 +569,14 @@ def run_rt(args):
     recomputation) against the forward time of the same steps."""
     import torch
 
-    from genasis_b200 import problems
+    from genasis_b200 import autotune, problems
     from genasis_b200.adjoint import cell_volumes, run_adjoint, run_forward
-    from genasis_b200.fluid import FluidBox
 
     torch.cuda.set_device(0)
     cfg, prim = problems.rayleigh_taylor()
     cells = cfg.n_proper
-    box = FluidBox(cfg)
+
+    box = autotune.tuned_box(cfg, adjoint=False)
     box.compute_from_primitive(prim)
     del prim
     dv = cell_volumes(box)
@@ -676,7 +678,7 @@ def run_adjoint_workload(args):
     import numpy as np
     import torch
 
-    from genasis_b200 import problems
+    from genasis_b200 import autotune, problems
     from genasis_b200.adjoint import cell_volumes, run_adjoint, run_forward
     from genasis_b200.fluid import FluidBox
 
@@ -687,7 +689,7 @@ def run_adjoint_workload(args):
         cfg, prim = problems.kelvin_helmholtz(n)
         if variant == "noisy":
             prim = problems.noisy(prim, amp=2e-2, seed=20261205)
-        box = FluidBox(cfg)
+        box = autotune.tuned_box(cfg)
         box.compute_from_primitive(prim)
         box.compute_from_conserved()
         U0 = box.U.clone()
