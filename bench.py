@@ -345,7 +345,8 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (state %.0f MB)" % (
                            6 * box.n_values * 8 / 1e6),
                        "l1_density_error": l1, "sim_time": t_sim,
-                       "full_crossing": crossing, "tuning": {"z_chunk": box.tuning[0]}},
+                       "full_crossing": crossing,
+                       "tuning": {"z_chunk": box.tuning[0], "tile": "32x%d" % box.tuning[2]}},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -423,8 +424,9 @@ def run_bricks(args):
         "plain_loop": {"value": cells * K / t_plain, "ms_per_step": 1000.0 * t_plain / K,
                        "gpu_launches": launches_plain},
         "speedup_vs_plain_loop": t_plain / t_batch,
-        "autotune": {"z_chunk": z_chunk, "ms_per_cycle_by_candidate": tune_ms,
-                     "from_cache": from_cache, "tuning_s": t_tune},
+        "autotune": {"tile": "32x%d" % z_chunk[0], "z_chunk": z_chunk[1],
+                     "ms_per_cycle_by_candidate": tune_ms, "from_cache": from_cache,
+                     "tuning_s": t_tune},
         "bitwise_equal_to_plain": same,
         "gpu_launches": launches_batch,
     }

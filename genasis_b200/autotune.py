@@ -3,6 +3,10 @@
 for the adjoint).
 
 Knobs (gfx_fluid_set_tuning):
+  tile_rows        rows of the 32-wide tile of a CTA, 8 or 16: taller tiles
+                   recompute fewer y slopes and halo cells per plane, shorter
+                   ones waste fewer lanes on bricks whose y extent is not a
+                   multiple of 16;
   z_chunk          z length of the cell pencils a CTA of the stage kernel
                    marches: longer pencils pay fewer prologues (the two
                    planes of slopes below the pencil), shorter ones give the
@@ -25,6 +29,7 @@ from . import problems
 from .fluid import FluidBox, _torch
 
 Z_CANDIDATES = (0, 8, 16, 32, 64)
+ROW_CANDIDATES = (8, 16)
 SEGMENT_CANDIDATES = (4, 8, 16, 32)
 BATCH_Z_CANDIDATES = (8, 16, 24, 32, 48, 64, 96)
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -94,31 +99,33 @@ def tune_brick(cfg, reps=3, adjoint=True, seed=1):
     box.compute_from_conserved()
     U0 = box.U.clone()
     dt = box.compute_time_step(0)
+    rows = ROW_CANDIDATES if cfg.reconstruction == "LINEAR" else (16,)
     ms_z = {}
-    for z in Z_CANDIDATES:
-        box.set_tuning(z, 0)
+    for r in rows:
+        for z in Z_CANDIDATES:
+            box.set_tuning(z, 0, r)
 
-        def step():
-            box.U.copy_(U0)
-            box.step(dt)
+            def step():
+                box.U.copy_(U0)
+                box.step(dt)
 
-        ms_z[z] = _time(step, reps)
-    best_z = min(ms_z, key=ms_z.get)
-    box.set_tuning(best_z, 0)
+            ms_z[(r, z)] = _time(step, reps)
+    best_r, best_z = min(ms_z, key=ms_z.get)
+    box.set_tuning(best_z, 0, best_r)
     best_seg, ms_s = 0, {}
-    if adjoint:
+    if adjoint and cfg.reconstruction == "LINEAR":
         box.U.copy_(U0)
         box.step(dt)
         U1 = box.U.clone()
         lam = torch.ones_like(U1)
         out = torch.empty_like(U1)
         for seg in SEGMENT_CANDIDATES:
-            box.set_tuning(best_z, seg)
+            box.set_tuning(best_z, seg, best_r)
             ms_s[seg] = _time(lambda: step_adjoint(box, U0, dt, lam, out, U1, False), reps)
         best_seg = min(ms_s, key=ms_s.get)
     box.close()
-    return {"z_chunk": best_z, "adjoint_segment": best_seg,
-            "ms": {"step": {str(k): v for k, v in ms_z.items()},
+    return {"z_chunk": best_z, "tile_rows": best_r, "adjoint_segment": best_seg,
+            "ms": {"step": {"%dx%d" % k: v for k, v in ms_z.items()},
                    "adjoint": {str(k): v for k, v in ms_s.items()}}}
 
 
@@ -126,38 +133,42 @@ def tuned_box(cfg, retune=False, adjoint=True):
     """A FluidBox with the cached (or freshly tuned) knobs of cfg's bucket."""
     cache = load_cache()
     key = brick_key(cfg)
-    if retune or key not in cache:
+    if retune or "tile_rows" not in cache.get(key, {}):
         cache[key] = tune_brick(cfg, adjoint=adjoint)
         save_cache(cache)
     box = FluidBox(cfg)
-    box.set_tuning(cache[key]["z_chunk"], cache[key]["adjoint_segment"])
+    e = cache[key]
+    box.set_tuning(e["z_chunk"], e["adjoint_segment"], e["tile_rows"])
     return box
 
 
 def tune_batch(batch, prims, cycles=3, retune=False):
-    """Chooses the batch's pencil length by timing whole batched cycles for
-    every candidate (the persistent grid's balance depends on all bricks at
-    once, not on one brick alone); applies and caches it.  The bricks'
-    states are reset from prims afterwards.  Returns (z_chunk, ms per cycle
-    by candidate, from_cache)."""
+    """Chooses the batch's tile rows and pencil length by timing whole
+    batched cycles for every candidate pair (the persistent grid's balance
+    depends on all bricks at once, not on one brick alone); applies and
+    caches them.  The bricks' states are reset from prims afterwards.
+    Returns ((tile_rows, z_chunk), ms per cycle by candidate, from_cache)."""
     cache = load_cache()
     key = batch_key([b.config for b in batch.boxes])
-    if not retune and key in cache:
-        batch.set_pencil_length(cache[key]["z_chunk"])
+    e = cache.get(key, {})
+    if not retune and "tile_rows" in e:
+        batch.set_pencil_length(e["z_chunk"], e["tile_rows"])
         batch.set_primitives(prims)
         batch.set_clocks(0.0, 0)
-        return cache[key]["z_chunk"], cache[key]["ms"], True
+        return (e["tile_rows"], e["z_chunk"]), e["ms"], True
     ms = {}
     batch.set_primitives(prims)
-    for z in BATCH_Z_CANDIDATES:
-        # the states keep evolving from candidate to candidate: the work of a
-        # cycle does not depend on them
-        batch.set_pencil_length(z)
-        ms[str(z)] = _time(lambda: batch.evolve(n_cycles=cycles), 2) / cycles
-    best = int(min(ms, key=ms.get))
-    cache[key] = {"z_chunk": best, "ms": ms}
+    for r in ROW_CANDIDATES:
+        for z in BATCH_Z_CANDIDATES:
+            # the states keep evolving from candidate to candidate: the work
+            # of a cycle does not depend on them
+            batch.set_pencil_length(z, r)
+            ms["%dx%d" % (r, z)] = _time(lambda: batch.evolve(n_cycles=cycles), 2) / cycles
+    best = min(ms, key=ms.get)
+    best_r, best_z = (int(v) for v in best.split("x"))
+    cache[key] = {"z_chunk": best_z, "tile_rows": best_r, "ms": ms}
     save_cache(cache)
-    batch.set_pencil_length(best)
+    batch.set_pencil_length(best_z, best_r)
     batch.set_primitives(prims)
     batch.set_clocks(0.0, 0)
-    return best, ms, False
+    return (best_r, best_z), ms, False

@@ -18,11 +18,13 @@ class FluidBatch:
         self.boxes = [FluidBox(c, device=device) for c in configs]
         self.h = None
 
-    def set_pencil_length(self, z_chunk):
+    def set_pencil_length(self, z_chunk, tile_rows=None):
         """The z length of the cell pencils of every brick's work items (0 =
-        32 planes); rebuilds the batch's work list on its next use."""
+        32 planes) and, if given, the tile rows (8 or 16); rebuilds the
+        batch's work list on its next use."""
         for b in self.boxes:
-            b.set_tuning(z_chunk, getattr(b, "tuning", (0, 0))[1])
+            _, seg, rows = getattr(b, "tuning", (0, 0, 0))
+            b.set_tuning(z_chunk, seg, rows if tile_rows is None else tile_rows)
         if self.h is not None:
             lib.load().gfx_fluid_batch_destroy(self.h)
             self.h = None

@@ -182,6 +182,7 @@ struct gfx_fluid {
   // tuning (gfx_fluid_set_tuning; 0 = built-in default)
   int z_chunk = 0;
   int adjoint_segment = 0;
+  int tile_y = kTileY;  // tile rows of the work list (8 or 16)
   unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
   double* partials = nullptr;                  // per-block sums of gfx_fluid_totals
   double* pv = nullptr;  // [4][nP]: P and V of the state the last stage 2 wrote
@@ -194,25 +195,26 @@ struct gfx_fluid {
 namespace {
 
 template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED,
-          bool PARAB = false>
+          bool PARAB = false, int TYt = kTileY>
 cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
                            int n_items, int* counter, const Phys& ph, cudaStream_t s) {
-  using SM = StageLayout<NF>;
+  using SM = StageLayout<NF, TYt>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int per_sm = 1;
-  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BATCHED, PARAB>;
+  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BATCHED, PARAB, TYt>;
   std::call_once(once, [&] {
     attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)SM::kBytes);
     if (attr_err == cudaSuccess)
-      attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, SM::kBytes);
+      attr_err =
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SM::NT, SM::kBytes);
     if (per_sm < 1) per_sm = 1;
   });
   if (attr_err != cudaSuccess) return attr_err;
   // persistent grid: every resident CTA slot pulls work items
   const int grid = std::max(1, std::min(n_items, num_sms() * per_sm));
-  kern<<<grid, NT, SM::kBytes, s>>>(d, many, items, n_items, counter, ph);
+  kern<<<grid, SM::NT, SM::kBytes, s>>>(d, many, items, n_items, counter, ph);
   return cudaGetLastError();
 }
 
@@ -244,15 +246,17 @@ cudaError_t launch_stage_parabolic(int mode, bool in_prim, bool hllc, bool grav,
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const BrickDesc& d,
-                         const BrickDesc* many, const WorkItem* items, int n_items,
-                         int* counter, const Phys& ph, cudaStream_t s) {
+// The LINEAR variants for tile height TYt.
+template <int TYt>
+cudaError_t launch_stage_linear(int mode, bool in_prim, bool hllc, bool grav,
+                                const BrickDesc& d, const BrickDesc* many,
+                                const WorkItem* items, int n_items, int* counter,
+                                const Phys& ph, cudaStream_t s) {
   const bool bat = many != nullptr;
-  if (!bat && d.geo[0].PAR != nullptr && ph.parabolic)
-    return launch_stage_parabolic(mode, in_prim, hllc, grav, d, items, n_items, counter, ph, s);
 #define GFX_STAGE(M, IP, HC, GR, NF, BA)                                                  \
   if (mode == M && in_prim == IP && hllc == HC && grav == GR && bat == BA)              \
-    return launch_stage_t<M, IP, HC, GR, NF, BA>(d, many, items, n_items, counter, ph, s);
+    return launch_stage_t<M, IP, HC, GR, NF, BA, false, TYt>(d, many, items, n_items,     \
+                                                             counter, ph, s);
 #define GFX_STAGE_B(M, IP, HC, GR, NF) \
   GFX_STAGE(M, IP, HC, GR, NF, false)  \
   GFX_STAGE(M, IP, HC, GR, NF, true)
@@ -274,6 +278,27 @@ cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const Bri
   GFX_STAGE(MODE_STAGE2, true, true, true, 5, false)
 #undef GFX_STAGE_B
 #undef GFX_STAGE
+  return cudaErrorInvalidValue;
+}
+
+// The stage launch of a brick (or, with many, of a batch): PARABOLIC single
+// bricks at the default tile height, LINEAR at the tile height of the work
+// list (d.tile_y).
+cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const BrickDesc& d,
+                         const BrickDesc* many, const WorkItem* items, int n_items,
+                         int* counter, const Phys& ph, cudaStream_t s) {
+  const bool bat = many != nullptr;
+  const int ty = d.tile_y ? d.tile_y : kTileY;
+  if (!bat && d.geo[0].PAR != nullptr && ph.parabolic)
+    return ty == kTileY ? launch_stage_parabolic(mode, in_prim, hllc, grav, d, items, n_items,
+                                                 counter, ph, s)
+                        : cudaErrorInvalidValue;
+  if (ty == 8)
+    return launch_stage_linear<8>(mode, in_prim, hllc, grav, d, many, items, n_items, counter,
+                                  ph, s);
+  if (ty == kTileY)
+    return launch_stage_linear<kTileY>(mode, in_prim, hllc, grav, d, many, items, n_items,
+                                       counter, ph, s);
   return cudaErrorInvalidValue;
 }
 
@@ -316,11 +341,12 @@ int validate(const gfx_fluid_config* c) {
   return GFX_OK;
 }
 
-// Work list of one brick: TX x TY columns, cut along z into chunks so that the
+// Work list of one brick: TX x ty columns, cut along z into chunks so that the
 // persistent grid has several items per SM.
 // z_chunk > 0 fixes the pencil length instead (the autotuner's knob).
-std::vector<WorkItem> make_items(const int n[3], int brick, int z_chunk = 0) {
-  const int cx = (n[0] + TX - 1) / TX, cy = (n[1] + TY - 1) / TY;
+std::vector<WorkItem> make_items(const int n[3], int brick, int z_chunk = 0,
+                                 int ty = kTileY) {
+  const int cx = (n[0] + TX - 1) / TX, cy = (n[1] + ty - 1) / ty;
   const long long cols = (long long)cx * cy;
   const long long want = 16LL * num_sms();
   int chunks = (int)std::max(1LL, std::min<long long>(n[2] / 16, (want + cols - 1) / cols));
@@ -330,7 +356,7 @@ std::vector<WorkItem> make_items(const int n[3], int brick, int z_chunk = 0) {
   std::vector<WorkItem> v;
   for (int z = 0; z < n[2]; z += len)
     for (int y = 0; y < cy; ++y)
-      for (int x = 0; x < cx; ++x) v.push_back({brick, x * TX, y * TY, z, std::min(n[2], z + len)});
+      for (int x = 0; x < cx; ++x) v.push_back({brick, x * TX, y * ty, z, std::min(n[2], z + len)});
   return v;
 }
 
@@ -361,6 +387,7 @@ BrickDesc make_desc(gfx_fluid* h, const double* U_in, double* U_out, double* K,
   d.weight = weight;
   d.tsi_bits = h->tsi_bits;
   d.skip = skip;
+  d.tile_y = h->tile_y;
   return d;
 }
 
@@ -465,6 +492,7 @@ struct gfx_fluid_batch {
   cudaGraphExec_t graph = nullptr;
   long long graph_kernels = 0;
   long long launches = 0;
+  int tile_y = kTileY;
 };
 
 namespace {
@@ -487,6 +515,7 @@ int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, bool in_prim, cudaStrea
   }
   BrickDesc none;
   memset(&none, 0, sizeof(none));
+  none.tile_y = B->tile_y;
   CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, B->hllc, false, none, in_prim ? B->d1p : B->d1,
                         B->items, B->n_items, B->counters, B->ph, s));
   CUDA_TRY(launch_stage(MODE_STAGE2, true, B->hllc, false, none, B->d2, B->items, B->n_items,
@@ -519,8 +548,8 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   const Box& b = h->box;
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   if (h->prims_pending) return GFX_ERR_UNSUPPORTED;
-  std::vector<WorkItem> items = make_items(b.n, 0, h->z_chunk);
-  const int cols = ((b.n[0] + TX - 1) / TX) * ((b.n[1] + TY - 1) / TY);
+  std::vector<WorkItem> items = make_items(b.n, 0, h->z_chunk, h->tile_y);
+  const int cols = ((b.n[0] + TX - 1) / TX) * ((b.n[1] + h->tile_y - 1) / h->tile_y);
   const int nchunks = (int)items.size() / cols;
   const int len = items[0].z1 - items[0].z0;
   if (nchunks < 2 || len < 2 || (int)items.size() != h->n_items)
@@ -1097,6 +1126,10 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
     return code;
   };
   B->n = n;
+  B->tile_y = handles[0]->tile_y;
+  for (int b = 1; b < n; ++b)
+    if (handles[b]->tile_y != B->tile_y)
+      return cleanup(fail(GFX_ERR_ARGUMENT, "brick %d: tile rows differ from brick 0", b));
   B->h.assign(handles, handles + n);
   B->U.assign(U, U + n);
   B->ph = handles[0]->ph;
@@ -1135,11 +1168,12 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
     // brick's tuned pencil length
     const int* nn = h->box.n;
     const int len = std::min(nn[2], h->z_chunk > 0 ? h->z_chunk : 32);
+    const int ty = B->tile_y;
     for (int z = 0; z < nn[2]; z += len)
-      for (int y = 0; y < nn[1]; y += TY)
+      for (int y = 0; y < nn[1]; y += ty)
         for (int x = 0; x < nn[0]; x += TX) {
           items.push_back({b, x, y, z, std::min(nn[2], z + len)});
-          work.push_back((long long)std::min(TX, nn[0] - x) * std::min(TY, nn[1] - y) *
+          work.push_back((long long)std::min(TX, nn[0] - x) * std::min(ty, nn[1] - y) *
                          (std::min(nn[2], z + len) - z));
         }
   }
@@ -1348,13 +1382,18 @@ int gfx_fluid_totals(gfx_fluid* h, const double* U, double* totals, void* stream
   return GFX_OK;
 }
 
-int gfx_fluid_set_tuning(gfx_fluid* h, int z_chunk, int adjoint_segment) {
+int gfx_fluid_set_tuning(gfx_fluid* h, int z_chunk, int adjoint_segment, int tile_rows) {
   if (!h) return fail(GFX_ERR_ARGUMENT, "NULL handle");
   if (z_chunk < 0 || adjoint_segment < 0 || adjoint_segment > 4096)
     return fail(GFX_ERR_ARGUMENT, "z_chunk = %d, adjoint_segment = %d", z_chunk,
                 adjoint_segment);
-  if (z_chunk != h->z_chunk) {
-    std::vector<WorkItem> items = make_items(h->box.n, 0, z_chunk);
+  if (tile_rows == 0) tile_rows = kTileY;
+  if (tile_rows != 8 && tile_rows != kTileY)
+    return fail(GFX_ERR_ARGUMENT, "tile_rows = %d: 8 or %d", tile_rows, kTileY);
+  if (tile_rows != kTileY && h->cfg.reconstruction != GFX_RECONSTRUCTION_LINEAR)
+    return fail(GFX_ERR_UNSUPPORTED, "PARABOLIC runs on %d-row tiles only", kTileY);
+  if (z_chunk != h->z_chunk || tile_rows != h->tile_y) {
+    std::vector<WorkItem> items = make_items(h->box.n, 0, z_chunk, tile_rows);
     WorkItem* d = nullptr;
     if (cudaMalloc(&d, items.size() * sizeof(WorkItem)) != cudaSuccess)
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc work items");
@@ -1373,6 +1412,7 @@ int gfx_fluid_set_tuning(gfx_fluid* h, int z_chunk, int adjoint_segment) {
       h->graph = nullptr;
     }
     h->z_chunk = z_chunk;
+    h->tile_y = tile_rows;
   }
   h->adjoint_segment = adjoint_segment;
   return GFX_OK;
@@ -1472,7 +1512,7 @@ __global__ void noalloc_setup_kernel(NoAllocSetup p) {
   for (int i = threadIdx.x; i < p.n_items; i += blockDim.x) {
     const int x = i % p.cx, y = (i / p.cx) % p.cy, zc = i / (p.cx * p.cy);
     const int z0 = zc * p.len;
-    p.items[i] = {0, x * TX, y * TY, z0, min(p.n[2], z0 + p.len)};
+    p.items[i] = {0, x * TX, y * kTileY, z0, min(p.n[2], z0 + p.len)};
   }
   if (threadIdx.x == 0) {
     p.bits[0] = 0x0010000000000000ull;  // ordered_bits(-DBL_MAX), as reset_bits_kernel
@@ -1566,7 +1606,7 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
                                         (long long)b.n[0] * b.n[2],
                                         (long long)b.n[0] * b.n[1]});
   // work list shape: the cut of make_items
-  const int cx = (b.n[0] + TX - 1) / TX, cy = (b.n[1] + TY - 1) / TY;
+  const int cx = (b.n[0] + TX - 1) / TX, cy = (b.n[1] + kTileY - 1) / kTileY;
   const long long cols = (long long)cx * cy;
   const long long want = 16LL * num_sms();
   const int chunks =

@@ -21,12 +21,21 @@
 namespace gfx {
 
 constexpr int TX = 32;          // tile width (x), one warp per row
-constexpr int TY = 16;          // tile rows (y)
-constexpr int NT = TX * TY;     // threads per CTA
-constexpr int kMinCtas = (NT >= 512) ? 1 : 2;  // CTAs per SM the registers allow
-constexpr int PW = TX + 4;      // plane pitch with the 2-cell halo
-constexpr int PH = TY + 4;
-constexpr int PS = PW * PH;     // doubles per plane per variable
+constexpr int kTileY = 16;      // default tile rows; 8 is the other height built
+
+// The tile shape TX x TYt and what follows from it: NT threads per CTA, the
+// plane pitch PW and height PH with the 2-cell halo, PS doubles per plane and
+// variable.  Functions that depend on the tile take TYt as a template
+// parameter and open with GFX_TILE(TYt).
+#define GFX_TILE(TYt)                          \
+  constexpr int TY = (TYt);                    \
+  constexpr int NT = TX * TY;                  \
+  constexpr int PW = TX + 4;                   \
+  constexpr int PH = TY + 4;                   \
+  constexpr int PS = PW * PH;                  \
+  (void)TY; (void)NT; (void)PW; (void)PH; (void)PS
+// CTAs per SM the registers allow at 128 registers per thread
+constexpr int tile_min_ctas(int ty) { return (TX * ty >= 512) ? 1 : 2; }
 
 enum { MODE_INCREMENT = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
 enum { BC_OUTFLOW = 0, BC_REFLECTING = 1, BC_PERIODIC = 2 };
@@ -65,6 +74,8 @@ struct BrickDesc {
   unsigned long long* tsi_bits;  // max inverse CFL time, ordered bits
   const int* skip;       // device flag: nonzero = do nothing (finished evolve)
   double* pv;            // stage 2: P, V1, V2, V3 of the new state, compact (or null)
+  int tile_y;            // host side: tile rows of the work list (0 = kTileY)
+  int pad_;
   AxisGeo geo[3];
 };
 
@@ -95,9 +106,10 @@ __device__ __forceinline__ int bc_map(int g, int n, int bc_lo, int bc_hi, bool& 
 
 // Loads the primitives of cell (gx, gy) of plane gz (all possibly ghosts) into
 // a ring plane at local (ly, lx).
-template <bool IN_PRIM>
+template <bool IN_PRIM, int TYt>
 __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, double* plane,
                                           int lx, int ly, int gx, int gy, int gz) {
+  GFX_TILE(TYt);
   bool nx, ny, nz;
   const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
   const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
@@ -135,9 +147,10 @@ __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, do
 }
 
 // Loads the primitives of one cell into a column slot (5 values at stride NT).
-template <bool IN_PRIM>
+template <bool IN_PRIM, int TYt>
 __device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph, double* dst,
                                               int gx, int gy, int gz) {
+  GFX_TILE(TYt);
   bool nx, ny, nz;
   const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
   const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
@@ -276,8 +289,10 @@ __device__ __forceinline__ void face_prims(const double* vm, const double* sm_, 
 // Per-tile copy of the geometry tables of one axis, entries t0 .. t0 + L - 1.
 enum { G_W, G_WL, G_WR, G_DXI, G_SQ, G_CDEN, G_RDXI, G_RCDEN, G_RW, G_NTAB };
 
+template <int TYt>
 __device__ __forceinline__ void fill_geo(const AxisGeo& G, int m, int t0, int L, double* dst,
                                          int tid) {
+  GFX_TILE(TYt);
   const double* tabs[G_NTAB] = {G.W, G.WL, G.WR, G.dXI, G.SQ, G.CDEN, G.RDXI, G.RCDEN, G.RW};
   for (int i = tid; i < G_NTAB * L; i += NT) {
     const int q = i / L, j = i % L, t = t0 + j;
@@ -285,8 +300,9 @@ __device__ __forceinline__ void fill_geo(const AxisGeo& G, int m, int t0, int L,
   }
 }
 
-template <int NF>
+template <int NF, int TYt>
 struct StageLayout {
+  static constexpr int TY = TYt, NT = TX * TYt, PW = TX + 4, PH = TYt + 4, PS = PW * PH;
   static constexpr int kFull = 5 * PS;            // plane k with its x / y halo
   static constexpr int kCen = 2 * 5 * NT;         // centres of planes k+1, k+2
   static constexpr int kZs = 5 * NT;              // z slope of plane k (own column)
@@ -382,22 +398,23 @@ __device__ __forceinline__ void z_parabolic(const BrickDesc& B, int p, const dou
 // cache of the plane loop.
 // PARABOLIC (PARAB): zss keeps the outer face values of plane z0 instead of
 // its slopes.
-template <bool IN_PRIM, bool HLLC, int NF, bool PARAB>
+template <bool IN_PRIM, bool HLLC, int NF, bool PARAB, int TYt>
 __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, double* full,
                                             double* cen, double* zss, double* zfs, int tid,
                                             int tx, int ty, int gx, int gy, int z0, bool own,
                                             double dt) {
+  GFX_TILE(TYt);
   auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
   double* fc = full + (ty + 2) * PW + (tx + 2);
-  load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 - 2);
-  load_cell_col<IN_PRIM>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
-  load_cell_col<IN_PRIM>(B, ph, cslot(z0), gx, gy, z0);
+  load_cell<IN_PRIM, TYt>(B, ph, full, tx, ty, gx, gy, z0 - 2);
+  load_cell_col<IN_PRIM, TYt>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
+  load_cell_col<IN_PRIM, TYt>(B, ph, cslot(z0), gx, gy, z0);
   double s_m[5], s_0[5], vI0[5];
   if (PARAB)
     z_parabolic(B, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, vI0, s_m);
   else
     z_slope(B.geo[2], ph, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
-  load_cell<IN_PRIM>(B, ph, full, tx, ty, gx, gy, z0 + 1);
+  load_cell<IN_PRIM, TYt>(B, ph, full, tx, ty, gx, gy, z0 + 1);
   if (PARAB)
     z_parabolic(B, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, vI0, s_0);
   else
@@ -423,12 +440,14 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
 // brick (read from the constant bank).
 // PARAB: PARABOLIC reconstruction (single bricks): no slope phase; each face
 // reconstructs its two cells, the own column carries outer face values in z.
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED, bool PARAB = false>
-__global__ void __launch_bounds__(NT, kMinCtas)
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED, bool PARAB = false,
+          int TYt = kTileY>
+__global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
     stage_kernel(const __grid_constant__ BrickDesc single, const BrickDesc* __restrict__ many,
                  const WorkItem* __restrict__ items, int n_items, int* __restrict__ counter,
                  const __grid_constant__ Phys ph) {
-  using SL = StageLayout<NF>;
+  GFX_TILE(TYt);
+  using SL = StageLayout<NF, TYt>;
   extern __shared__ double smem[];
   double* full = smem;
   double* cen = full + SL::kFull;
@@ -475,15 +494,15 @@ __global__ void __launch_bounds__(NT, kMinCtas)
     const int gx = x0 + tx, gy = y0 + ty;
     const bool own = (gx < n0) && (gy < n1);
     double tsi_max = -DBL_MAX;
-    fill_geo(B.geo[0], B.m[0], x0, LX, gxc, tid);
-    fill_geo(B.geo[1], B.m[1], y0, LY, gyc, tid);
+    fill_geo<TYt>(B.geo[0], B.m[0], x0, LX, gxc, tid);
+    fill_geo<TYt>(B.geo[1], B.m[1], y0, LY, gyc, tid);
 
     // own column helpers: a "column pointer" addresses 5 values at stride NT
     // (centre slots) or PS (full plane)
     auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
     // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
-    stage_prologue<IN_PRIM, HLLC, NF, PARAB>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx, gy,
-                                             z0, own, dt);
+    stage_prologue<IN_PRIM, HLLC, NF, PARAB, TYt>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx,
+                                                  gy, z0, own, dt);
     __syncthreads();  // geometry caches
 
     for (int k = z0; k < z1; ++k) {
@@ -494,7 +513,7 @@ __global__ void __launch_bounds__(NT, kMinCtas)
 #pragma unroll
         for (int q = 0; q < 5; ++q) full[q * PS + c_off] = src[q * NT];
       }
-      load_cell_col<IN_PRIM>(B, ph, cslot(k + 2), gx, gy, k + 2);
+      load_cell_col<IN_PRIM, TYt>(B, ph, cslot(k + 2), gx, gy, k + 2);
       if (tid < 4 * TX + 4 * TY) {
         // the halo: two rows below and above the tile, two columns left and right
         int lx, ly;
@@ -507,7 +526,7 @@ __global__ void __launch_bounds__(NT, kMinCtas)
           ly = j / 4;
           lx = (s < 2) ? s - 2 : TX + s - 2;
         }
-        load_cell<IN_PRIM>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
+        load_cell<IN_PRIM, TYt>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
       }
       __syncthreads();
 

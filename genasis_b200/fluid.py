@@ -150,10 +150,12 @@ class FluidBox:
                  ms, _stream())
         return tuple(ms)
 
-    def set_tuning(self, z_chunk=0, adjoint_segment=0):
-        """Speed knobs that leave results unchanged (genasis_b200.autotune)."""
-        lib.call("gfx_fluid_set_tuning", self.h, int(z_chunk), int(adjoint_segment))
-        self.tuning = (int(z_chunk), int(adjoint_segment))
+    def set_tuning(self, z_chunk=0, adjoint_segment=0, tile_rows=0):
+        """Speed knobs that leave results unchanged (genasis_b200.autotune):
+        pencil length, adjoint sweep segment, tile rows (8 or 16)."""
+        lib.call("gfx_fluid_set_tuning", self.h, int(z_chunk), int(adjoint_segment),
+                 int(tile_rows))
+        self.tuning = (int(z_chunk), int(adjoint_segment), int(tile_rows))
 
     def totals(self, U=None):
         """sum U dV over the proper cells for the six conserved fields

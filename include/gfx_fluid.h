@@ -256,8 +256,11 @@ int gfx_fluid_totals(gfx_fluid *h, const double *U_dev, double *totals_host, voi
  * z_chunk = z length of the cell pencils a CTA marches in the stage kernel
  * (0 = default: enough items for 16 per SM; a batch created afterwards takes
  * it per brick, default 32); adjoint_segment = faces per thread in the
- * adjoint's reverse sweep (0 = 8).  No counterpart in the reference. */
-int gfx_fluid_set_tuning(gfx_fluid *h, int z_chunk, int adjoint_segment);
+ * adjoint's reverse sweep (0 = 8); tile_rows = rows of the 32-wide tile of a
+ * CTA, 8 (256 threads, 2 CTAs per SM) or 16 (512 threads, 1 CTA per SM; 0 =
+ * 16; PARABOLIC runs on 16 only; the bricks of a batch must agree).  No
+ * counterpart in the reference. */
+int gfx_fluid_set_tuning(gfx_fluid *h, int z_chunk, int adjoint_segment, int tile_rows);
 
 int gfx_fluid_last_error(char *buf, size_t len);
 

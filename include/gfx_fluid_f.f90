@@ -216,11 +216,12 @@ module GFX_Fluid_C
       integer ( c_int ), value :: DetectFeatures
     end function gfx_fluid_step_adjoint
 
-    integer ( c_int ) function gfx_fluid_set_tuning ( Handle, zChunk, AdjointSegment ) &
+    integer ( c_int ) function gfx_fluid_set_tuning &
+      ( Handle, zChunk, AdjointSegment, TileRows ) &
       bind ( c, name = 'gfx_fluid_set_tuning' )
       import
       type ( c_ptr ), value :: Handle
-      integer ( c_int ), value :: zChunk, AdjointSegment
+      integer ( c_int ), value :: zChunk, AdjointSegment, TileRows
     end function gfx_fluid_set_tuning
 
     integer ( c_int ) function gfx_fluid_batch_create ( nBricks, Handles, Conserved_dev, Batch ) &

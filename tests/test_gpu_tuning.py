@@ -23,9 +23,9 @@ def test_pencil_length_and_segment_leave_results_unchanged():
                                 ("OUTFLOW", "OUTFLOW")))
     prim = problems.random_state(cfg, seed=4)
     ref_U = ref_lam = None
-    for z, seg in [(0, 0), (5, 3), (16, 8), (37, 32), (64, 1)]:
+    for z, seg, rows in [(0, 0, 16), (5, 3, 8), (16, 8, 16), (37, 32, 8), (64, 1, 8)]:
         box = FluidBox(cfg)
-        box.set_tuning(z, seg)
+        box.set_tuning(z, seg, rows)
         box.compute_from_primitive(prim)
         dts = []
         for i in range(3):
@@ -39,11 +39,11 @@ def test_pencil_length_and_segment_leave_results_unchanged():
         if ref_U is None:
             ref_U, ref_lam = U, L
         else:
-            assert np.array_equal(U, ref_U), (z, seg)
+            assert np.array_equal(U, ref_U), (z, seg, rows)
             # the adjoint adds into cells shared by two segments atomically, in
             # no fixed order: equal up to rounding
             scale = float(np.abs(ref_lam).max())
-            assert float(np.abs(L - ref_lam).max()) <= 1e-12 * scale, (z, seg)
+            assert float(np.abs(L - ref_lam).max()) <= 1e-12 * scale, (z, seg, rows)
         box.close()
 
 
@@ -56,14 +56,15 @@ def test_batch_tuner_picks_a_candidate_and_keeps_results(tmp_path, monkeypatch):
     cfgs = [c for c, _ in bricks]
     prims = [p for _, p in bricks]
     batch = FluidBatch(cfgs)
-    z, ms, cached = autotune.tune_batch(batch, prims, cycles=2)
-    assert z in autotune.BATCH_Z_CANDIDATES and not cached
-    assert set(ms) == {str(c) for c in autotune.BATCH_Z_CANDIDATES}
+    (rows, z), ms, cached = autotune.tune_batch(batch, prims, cycles=2)
+    assert z in autotune.BATCH_Z_CANDIDATES and rows in autotune.ROW_CANDIDATES and not cached
+    assert set(ms) == {"%dx%d" % (r, c) for r in autotune.ROW_CANDIDATES
+                       for c in autotune.BATCH_Z_CANDIDATES}
     batch.evolve(n_cycles=3)
     tuned = [to_np(b.U) for b in batch.boxes]
-    z2, _, cached2 = autotune.tune_batch(batch, prims)
-    assert cached2 and z2 == z
-    batch.set_pencil_length(0)
+    (rows2, z2), _, cached2 = autotune.tune_batch(batch, prims)
+    assert cached2 and (rows2, z2) == (rows, z)
+    batch.set_pencil_length(0, 16)
     batch.set_primitives(prims)
     batch.set_clocks(0.0, 0)
     batch.evolve(n_cycles=3)
