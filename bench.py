@@ -216,16 +216,28 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def traffic_per_launch(kernel, cells):
-    """DRAM bytes per launch of the stage kernel from the committed ncu summary
-    (bytes per cell measured on a smaller case, scaled by the cells)."""
+def _stage_profile(kernel):
     path = os.path.join(ROOT, "profiles", "stage_traffic.json")
     try:
         with open(path) as f:
-            per_cell = json.load(f)[kernel]["dram_bytes_per_cell"]
-        return per_cell * cells
+            return json.load(f)[kernel]
     except Exception:  # noqa: BLE001
-        return None
+        return {}
+
+
+def traffic_per_launch(kernel, cells):
+    """DRAM bytes per launch of the stage kernel from the committed ncu summary
+    (bytes per cell measured on a smaller case, scaled by the cells)."""
+    per_cell = _stage_profile(kernel).get("dram_bytes_per_cell")
+    return per_cell * cells if per_cell is not None else None
+
+
+def pipe_use(kernel):
+    """FP64 pipe and issue activity of the stage kernel from the committed
+    ncu capture: what bounds it instead of HBM."""
+    p = _stage_profile(kernel)
+    return {"fp64_pipe_active": p.get("fp64_pipe_active"), "issue_active": p.get("issue_active"),
+            "source": "profiles/stage_kernel_sine160.md (ncu, 160^3)"}
 
 
 def run_ours(args):
@@ -303,7 +315,8 @@ def run_ours(args):
                 "algorithmic_bytes_per_cell": STAGE_BYTES[dom],
                 "avg_launch_ms": avg[dom],
                 "kernel_ms": avg,
-                "step_hbm_frac": STEP_BYTES * value / world / 1e9 / peak}
+                "step_hbm_frac": STEP_BYTES * value / world / 1e9 / peak,
+                "ncu_pipes": pipe_use(dom)}
 
 
     # end to end: H2D of the state from pinned host memory, the step, D2H
