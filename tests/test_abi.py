@@ -125,3 +125,38 @@ def test_fortran_config_type_has_the_c_layout():
     c_fields = [f[0] for f in GfxConfig._fields_]
     assert len(fields) == len(c_fields)
     assert offsets == [getattr(GfxConfig, f).offset for f in c_fields]
+
+
+def _calls(text, name):
+    """Argument lists (top-level comma count + 1) of every call to name."""
+    out = []
+    for m in re.finditer(r"\b%s\s*\(" % name, text):
+        i, depth, args, nonempty = m.end(), 1, 1, False
+        while depth:
+            c = text[i]
+            if c == "(":
+                depth += 1
+            elif c == ")":
+                depth -= 1
+            elif c == "," and depth == 1:
+                args += 1
+            elif not c.isspace() and c != "&":
+                nonempty = True
+            i += 1
+        out.append(args if nonempty else 0)
+    return out
+
+
+def test_genasis_wrapper_calls_match_the_header():
+    """include/gfx_fluid_genasis.f90 (the GenASiS-side wrapper) calls each C
+    function with the header's number of arguments."""
+    text = open(os.path.join(ROOT, "include", "gfx_fluid_genasis.f90")).read()
+    text = "\n".join(l.split("!")[0] for l in text.splitlines())  # drop comments
+    text = re.sub(r"&\s*\n\s*", " ", text)  # join continuation lines
+    h = header_arg_counts()
+    used = 0
+    for name, n in h.items():
+        for got in _calls(text, name):
+            assert got == n, (name, got, n)
+            used += 1
+    assert used >= 6
