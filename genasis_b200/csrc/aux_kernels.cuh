@@ -12,6 +12,17 @@ struct Box {
   long long nV, nP;
 };
 
+// Coordinates (i, j, k) of the linear index v over an a x b x ... box, x
+// fastest.  Every brick has fewer than 2^31 values (gfx_fluid_create checks),
+// so 32-bit division suffices; the 64-bit one would be emulated.
+__device__ __forceinline__ void decode3(long long v, int a, int b, int& i, int& j, int& k) {
+  const unsigned u = (unsigned)v, ua = (unsigned)a, ub = (unsigned)b;
+  const unsigned r = u / ua;
+  i = (int)(u - r * ua);
+  k = (int)(r / ub);
+  j = (int)(r - (unsigned)k * ub);
+}
+
 __device__ __forceinline__ bool periodic_reachable(const Box& b, int i, int j, int k, int& si,
                                                    int& sj, int& sk) {
   // A ghost value is written by the single-brick exchange (faces and edges,
@@ -43,9 +54,8 @@ __global__ void from_primitive_kernel(Box b, Phys ph, const double* __restrict__
   const long long nV = b.nV;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
        v += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(v % b.m[0]);
-    const int j = (int)((v / b.m[0]) % b.m[1]);
-    const int k = (int)(v / ((long long)b.m[0] * b.m[1]));
+    int i, j, k;
+    decode3(v, b.m[0], b.m[1], i, j, k);
     int si, sj, sk;
     long long src = v;
     if (periodic_reachable(b, i, j, k, si, sj, sk))
@@ -111,9 +121,8 @@ __global__ void to_primitive_kernel(Box b, Phys ph, double* __restrict__ U,
 __device__ __forceinline__ void ghost_refresh_value(const Box& b, const Phys& ph, double* U,
                                                     long long v) {
   const long long nV = b.nV;
-  const int i = (int)(v % b.m[0]);
-  const int j = (int)((v / b.m[0]) % b.m[1]);
-  const int k = (int)(v / ((long long)b.m[0] * b.m[1]));
+  int i, j, k;
+  decode3(v, b.m[0], b.m[1], i, j, k);
   const bool ghost =
       i < 2 || j < 2 || k < 2 || i >= b.n[0] + 2 || j >= b.n[1] + 2 || k >= b.n[2] + 2;
   if (!ghost) return;
@@ -211,9 +220,8 @@ __device__ __forceinline__ void cell_p_v(const Box& b, const Phys& ph, const dou
 // cells: bit e of sb[c] = shock along e at c (compared with c - e_e).
 __device__ __forceinline__ void detect_shock_cell(const Box& b, const Phys& ph, const double* U,
                                                   const double* Pst, uint8_t* sb, long long c) {
-  const int i = (int)(c % b.n[0]);
-  const int j = (int)((c / b.n[0]) % b.n[1]);
-  const int k = (int)(c / ((long long)b.n[0] * b.n[1]));
+  int i, j, k;
+  decode3(c, b.n[0], b.n[1], i, j, k);
   double P0, v0[3];
   cell_p_v(b, ph, U, Pst, i, j, k, P0, v0);
   uint8_t bits = 0;
@@ -240,8 +248,8 @@ __global__ void detect_shock_pv_kernel(Box b, Phys ph, const double* __restrict_
   const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
        c += (long long)gridDim.x * blockDim.x) {
-    const int t[3] = {(int)(c % b.n[0]), (int)((c / b.n[0]) % b.n[1]),
-                      (int)(c / ((long long)b.n[0] * b.n[1]))};
+    int t[3];
+    decode3(c, b.n[0], b.n[1], t[0], t[1], t[2]);
     const double P0 = pv[c];
     uint8_t bits = 0;
 #pragma unroll
@@ -272,8 +280,8 @@ __global__ void detect_shock_kernel(Box b, Phys ph, const double* __restrict__ U
 // or x + e_e - e_d (the positions DetectShocks_CSL_Kernel writes).
 __device__ __forceinline__ void detect_flags_cell(const Box& b, const uint8_t* sb, uint8_t* df,
                                                   long long c) {
-  const int t[3] = {(int)(c % b.n[0]), (int)((c / b.n[0]) % b.n[1]),
-                    (int)(c / ((long long)b.n[0] * b.n[1]))};
+  int t[3];
+  decode3(c, b.n[0], b.n[1], t[0], t[1], t[2]);
   uint8_t bits = 0;
   bool interior = true;
 #pragma unroll
@@ -349,9 +357,8 @@ __global__ void inverse_timestep_kernel(Box b, Phys ph, const double* __restrict
   double m = -DBL_MAX;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
        c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % b.n[0]);
-    const int j = (int)((c / b.n[0]) % b.n[1]);
-    const int k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    int i, j, k;
+    decode3(c, b.n[0], b.n[1], i, j, k);
     Prim w;
     if (Pst) {
       w.N = Pst[c];
@@ -435,8 +442,8 @@ __global__ void totals_kernel(Box b, const double* __restrict__ U, AxisGeo G0, A
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const long long c0 = blockIdx.x * chunk, c1 = min(b.nP, c0 + chunk);
   for (long long c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-    const int i = (int)(c % b.n[0]), j = (int)((c / b.n[0]) % b.n[1]),
-              k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    int i, j, k;
+    decode3(c, b.n[0], b.n[1], i, j, k);
     const long long g = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
     const double dv = G0.W[i + 2] * G1.W[j + 2] * G2.W[k + 2];
 #pragma unroll
@@ -465,8 +472,8 @@ __global__ void check_state_kernel(Box b, Phys ph, const double* __restrict__ U,
   unsigned long long bad = 0, floor = 0;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
        c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % b.n[0]), j = (int)((c / b.n[0]) % b.n[1]),
-              k = (int)(c / ((long long)b.n[0] * b.n[1]));
+    int i, j, k;
+    decode3(c, b.n[0], b.n[1], i, j, k);
     const long long g = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
     bool finite = true;
 #pragma unroll

@@ -327,6 +327,8 @@ int validate(const gfx_fluid_config* c) {
     if ((c->boundary[d][0] == GFX_BC_PERIODIC) != (c->boundary[d][1] == GFX_BC_PERIODIC))
       return fail(GFX_ERR_ARGUMENT, "axis %d: PERIODIC must be set on both faces", d);
   }
+  if ((long long)(c->n_cells[0] + 4) * (c->n_cells[1] + 4) * (c->n_cells[2] + 4) >= (1LL << 31))
+    return fail(GFX_ERR_UNSUPPORTED, "a brick of 2^31 or more values (with ghosts)");
   if (c->n_ghost_layers != 2)
     return fail(GFX_ERR_UNSUPPORTED, "n_ghost_layers = %d: only 2 (the reference default)",
                 c->n_ghost_layers);
@@ -398,9 +400,11 @@ __global__ void scatter_flags_kernel(Box b, const uint8_t* __restrict__ df,
                                      uint8_t* __restrict__ out) {
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < b.nV;
        v += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(v % b.m[0]) - 2;
-    const int j = (int)((v / b.m[0]) % b.m[1]) - 2;
-    const int k = (int)(v / ((long long)b.m[0] * b.m[1])) - 2;
+    int i, j, k;
+    decode3(v, b.m[0], b.m[1], i, j, k);
+    i -= 2;
+    j -= 2;
+    k -= 2;
     uint8_t f = 0;
     if (i >= 0 && j >= 0 && k >= 0 && i < b.n[0] && j < b.n[1] && k < b.n[2])
       f = df[i + (long long)b.n[0] * (j + (long long)b.n[1] * k)];
