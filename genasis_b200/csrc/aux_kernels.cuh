@@ -152,6 +152,35 @@ __global__ void ghost_refresh_kernel(Box b, Phys ph, double* __restrict__ U) {
     ghost_refresh_value(b, ph, U, v);
 }
 
+// The same, visiting only the ghost shell: the two z ghost planes at each
+// end, then the y ghost rows and the x ghost columns of the proper planes.
+__global__ void ghost_refresh_shell_kernel(Box b, Phys ph, double* __restrict__ U) {
+  const long long m0 = b.m[0], m1 = b.m[1], m2 = b.m[2];
+  const long long n1 = b.n[1], n2 = b.n[2];
+  const long long gz = 4 * m0 * m1, gy = 4 * m0 * n2, gx = 4 * n1 * n2;
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < gz + gy + gx;
+       u += (long long)gridDim.x * blockDim.x) {
+    long long i, j, k;
+    if (u < gz) {  // planes k = 0, 1, m2 - 2, m2 - 1
+      const long long s = u / (m0 * m1), r = u - s * m0 * m1;
+      k = (s < 2) ? s : m2 - 4 + s;
+      j = r / m0;
+      i = r - j * m0;
+    } else if (u < gz + gy) {  // rows j = 0, 1, m1 - 2, m1 - 1 of planes 2 .. m2 - 3
+      const long long w = u - gz, s = w / (m0 * n2), r = w - s * m0 * n2;
+      j = (s < 2) ? s : m1 - 4 + s;
+      k = 2 + r / m0;
+      i = r - (k - 2) * m0;
+    } else {  // columns i = 0, 1, m0 - 2, m0 - 1 of rows 2 .. m1 - 3
+      const long long w = u - gz - gy, s = w / (n1 * n2), r = w - s * n1 * n2;
+      i = (s < 2) ? s : m0 - 4 + s;
+      k = 2 + r / n1;
+      j = 2 + (r - (k - 2) * n1);
+    }
+    ghost_refresh_value(b, ph, U, i + m0 * (j + m1 * k));
+  }
+}
+
 // The same over the values [v0, v1) only (whole planes of a z slab).
 __global__ void ghost_refresh_range_kernel(Box b, Phys ph, double* __restrict__ U, long long v0,
                                            long long v1) {

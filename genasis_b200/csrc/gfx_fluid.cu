@@ -468,7 +468,9 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
                         h->counters + 1, h->ph, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[3], s));
   const int blk = 256;
-  ghost_refresh_kernel<<<grid_for(h->box.nV, blk), blk, 0, s>>>(h->box, h->ph, U);
+  const Box& bx = h->box;
+  const long long shell = bx.nV - bx.nP;
+  ghost_refresh_shell_kernel<<<grid_for(shell, blk), blk, 0, s>>>(bx, h->ph, U);
   CUDA_TRY(cudaGetLastError());
   if (ev) CUDA_TRY(cudaEventRecord(ev[4], s));
   h->launches += 3;
