@@ -269,33 +269,6 @@ __device__ __forceinline__ void detect_shock_cell(const Box& b, const Phys& ph, 
   sb[c] = bits;
 }
 
-// The same shock bits from the pressure and velocities that the previous
-// step's stage 2 stored for its new state (pv = [P, V1, V2, V3][nP]): the
-// values cell_p_v would recover from that state, without the recovery.
-__global__ void detect_shock_pv_kernel(Box b, Phys ph, const double* __restrict__ pv,
-                                       uint8_t* __restrict__ sb) {
-  const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
-       c += (long long)gridDim.x * blockDim.x) {
-    int t[3];
-    decode3(c, b.n[0], b.n[1], t[0], t[1], t[2]);
-    const double P0 = pv[c];
-    uint8_t bits = 0;
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-      if (t[e] < 1) continue;
-      const long long cm = c - st[e];
-      const double P1 = pv[cm];
-      const double dP = fabs(P0 - P1);
-      const double pmin = (P0 < P1) ? P0 : P1;
-      const double dLnP = dP / fmax2(pmin, kSqrtTiny);
-      const double dV = pv[(1 + e) * b.nP + c] - pv[(1 + e) * b.nP + cm];
-      if (dLnP > ph.shock_threshold && dV <= 0.0) bits |= (uint8_t)(1u << e);
-    }
-    sb[c] = bits;
-  }
-}
-
 __global__ void detect_shock_kernel(Box b, Phys ph, const double* __restrict__ U,
                                     const double* __restrict__ Pst, uint8_t* __restrict__ sb) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;

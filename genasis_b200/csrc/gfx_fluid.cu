@@ -185,7 +185,7 @@ struct gfx_fluid {
   int tile_y = kTileY;  // tile rows of the work list (8 or 16)
   unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
   double* partials = nullptr;                  // per-block sums of gfx_fluid_totals
-  double* pv = nullptr;  // [4][nP]: P and V of the state the last stage 2 wrote
+  double* wn = nullptr;  // [5][nP]: the primitives of the state the last stage 2 wrote
   // pipelined gfx_fluid_step_host: copy streams, per-slab events and counters
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[8] = {}, ev_out[8] = {}, ev_end = nullptr;
@@ -422,12 +422,13 @@ int run_features(gfx_fluid* h, const double* U, const double* Pst, cudaStream_t 
   return GFX_OK;
 }
 
-// Shock flags of the state the previous step's stage 2 wrote, from its
-// stored pressure and velocities (valid only between the steps of one
-// evolve, where nothing else touches the state).
-int run_features_pv(gfx_fluid* h, cudaStream_t s) {
+// Shock flags of the state the previous step's stage 2 wrote, from the
+// primitives it stored (valid only between the steps of one evolve, where
+// nothing else touches the state; the same values the recovery from the
+// stored, floored state gives).
+int run_features_wn(gfx_fluid* h, const double* U, cudaStream_t s) {
   const int blk = 256;
-  detect_shock_pv_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->ph, h->pv, h->sb);
+  detect_shock_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->ph, U, h->wn, h->sb);
   CUDA_TRY(cudaGetLastError());
   detect_flags_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->sb, h->df);
   CUDA_TRY(cudaGetLastError());
@@ -438,10 +439,12 @@ int run_features_pv(gfx_fluid* h, cudaStream_t s) {
 // The launches of one RK2 step on U (in place).  dt_ptr, skip: device scalars.
 // detect: whether the shock flags must be recomputed from U first.  ev (may
 // be null): 5 events recorded between the phases for gfx_fluid_step_timed.
-// from_pv: detect from the pressure and velocities of the previous stage 2.
+// from_wn: the step follows a step of the same evolve, whose stage 2 stored
+// the primitives of U: shock detection and stage 1 read them instead of
+// recovering them from U.
 int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
                  double* fluence, bool detect, cudaStream_t s, cudaEvent_t* ev = nullptr,
-                 bool from_pv = false) {
+                 bool from_wn = false) {
   const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
   const bool grav = h->cfg.uniform_acceleration != 0.0;
   reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
@@ -451,19 +454,20 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
     CUDA_TRY(cudaMemsetAsync(fluence, 0, sizeof(double) * 36 * h->face_size, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[0], s));
   if (hllc && detect) {
-    int rc = from_pv ? run_features_pv(h, s) : run_features(h, U, nullptr, s);
+    int rc = from_wn ? run_features_wn(h, U, s) : run_features(h, U, nullptr, s);
     if (rc) return rc;
   }
   if (ev) CUDA_TRY(cudaEventRecord(ev[1], s));
   const uint8_t* df = hllc ? h->df : nullptr;
-  const bool in_prim = h->prims_pending;
-  BrickDesc d1 = make_desc(h, U, nullptr, nullptr, in_prim ? h->Pst : nullptr, df, fluence,
+  const bool in_prim = from_wn || h->prims_pending;
+  BrickDesc d1 = make_desc(h, U, nullptr, nullptr,
+                           from_wn ? h->wn : (h->prims_pending ? h->Pst : nullptr), df, fluence,
                            dt_ptr, 0.5, skip);
   CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, hllc, grav, d1, nullptr, h->items, h->n_items,
                         h->counters, h->ph, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[2], s));
   BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fluence, dt_ptr, 0.5, skip);
-  d2.pv = h->pv;
+  d2.wn = h->wn;
   CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
                         h->counters + 1, h->ph, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[3], s));
@@ -613,7 +617,7 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   const uint8_t* df = hllc ? h->df : nullptr;
   BrickDesc d1 = make_desc(h, U, nullptr, nullptr, nullptr, df, fl, h->dt_slot, 0.5, nullptr);
   BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fl, h->dt_slot, 0.5, nullptr);
-  d2.pv = h->pv;
+  d2.wn = h->wn;
   auto stage = [&](int mode, int j) -> cudaError_t {
     ++launches;
     return launch_stage(mode, mode == MODE_STAGE2, hllc, grav, mode == MODE_STAGE1 ? d1 : d2,
@@ -780,7 +784,7 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
       cudaMalloc(&h->counters, 4 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&h->clock, 2 * sizeof(Clock)) != cudaSuccess ||
       cudaMalloc(&h->dt_slot, sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->pv, 4 * nP * sizeof(double)) != cudaSuccess)
+      cudaMalloc(&h->wn, 5 * nP * sizeof(double)) != cudaSuccess)
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc of the stage scratch (%zu cells)", nP));
   if (cudaMemset(h->df, 0, nP) != cudaSuccess)
     return cleanup(fail(GFX_ERR_CUDA, "clear features"));
@@ -816,7 +820,7 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->adj_U);
   cudaFree(h->state_counts);
   cudaFree(h->partials);
-  cudaFree(h->pv);
+  cudaFree(h->wn);
   cudaFree(h->slab_counters);
   for (int j = 0; j < 8; ++j) {
     if (h->ev_in[j]) cudaEventDestroy(h->ev_in[j]);
@@ -1034,8 +1038,8 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
       cudaGraph_t g;
       const long long before = h->launches;
       CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      // every captured cycle follows a step of this evolve: its flags come
-      // from the pressure and velocities that step's stage 2 stored
+      // every captured cycle follows a step of this evolve: its flags and its
+      // stage 1 read the primitives that step's stage 2 stored
       int rc2 = enqueue_step(h, U, &dc->dt, &dc->done, nullptr, true, cs, nullptr, true);
       advance_clock_kernel<<<1, 1, 0, cs>>>(dc, 1);
       finalize_dt_kernel<<<1, 1, 0, cs>>>(h->ph, h->tsi_bits, dc, 1, 1);

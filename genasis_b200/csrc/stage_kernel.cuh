@@ -73,7 +73,8 @@ struct BrickDesc {
   double weight;         // Runge-Kutta weight of the stage (fluence)
   unsigned long long* tsi_bits;  // max inverse CFL time, ordered bits
   const int* skip;       // device flag: nonzero = do nothing (finished evolve)
-  double* pv;            // stage 2: P, V1, V2, V3 of the new state, compact (or null)
+  double* wn;            // stage 2: primitives N, V1, V2, V3, E of the new state, compact
+                         // (or null)
   int tile_y;            // host side: tile rows of the work list (0 = kTileY)
   int pad_;
   AxisGeo geo[3];
@@ -746,11 +747,12 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             U[3 * B.nV + gidx] = u.S3;
             U[4 * B.nV + gidx] = u.G;
             U[5 * B.nV + gidx] = SB * w.N;
-            if (B.pv) {
-              B.pv[cidx] = P;
-              B.pv[B.nP + cidx] = w.V1;
-              B.pv[2 * B.nP + cidx] = w.V2;
-              B.pv[3 * B.nP + cidx] = w.V3;
+            if (B.wn) {
+              B.wn[cidx] = w.N;
+              B.wn[B.nP + cidx] = w.V1;
+              B.wn[2 * B.nP + cidx] = w.V2;
+              B.wn[3 * B.nP + cidx] = w.V3;
+              B.wn[4 * B.nP + cidx] = w.E;
             }
             tsi_max = fmax2(tsi_max,
                             inverse_cfl_time(w, CS, w0, w1, w2, gxc[G_RW * LX + tx + 2],
