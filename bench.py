@@ -58,6 +58,10 @@ def parse():
                     help="rt workload: steps of the adjoint run at the end")
     ap.add_argument("--full-crossing", action="store_true",
                     help="sine workload: also run to t = 1 (one crossing) for the L1 error")
+    ap.add_argument("--tile-rows", type=int, default=0,
+                    help="sine workload: tile rows (8 or 16) instead of the autotuner's choice")
+    ap.add_argument("--z-chunk", type=int, default=0,
+                    help="sine workload: pencil length instead of the autotuner's choice")
     ap.add_argument("--bricks", type=int, default=512)
     return ap.parse_args()
 
@@ -248,10 +252,17 @@ def run_ours(args):
 
     cfg, prim = problems.sine_wave(args.n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
     cells = cfg.n_proper
-    # the pencil length from the autotuner's table (tuned here if absent)
+    # tile and pencil from the autotuner's table (tuned here if absent), or
+    # as given on the command line
     from genasis_b200 import autotune
 
-    box = autotune.tuned_box(cfg, adjoint=False)
+    if args.tile_rows or args.z_chunk:
+        from genasis_b200.fluid import FluidBox
+
+        box = FluidBox(cfg)
+        box.set_tuning(args.z_chunk, 0, args.tile_rows)
+    else:
+        box = autotune.tuned_box(cfg, adjoint=False)
     box.compute_from_primitive(prim)
     del prim
     stream = torch.cuda.current_stream()

@@ -260,20 +260,9 @@ __device__ __forceinline__ void detect_shock_cell(const Box& b, const Phys& ph, 
     if (t[e] < 1) continue;
     double P1, v1[3];
     cell_p_v(b, ph, U, Pst, i - (e == 0), j - (e == 1), k - (e == 2), P1, v1);
-    const double dP = fabs(P0 - P1);
-    const double pmin = (P0 < P1) ? P0 : P1;  // Fortran MIN: ties give either
-    const double dLnP = dP / fmax2(pmin, kSqrtTiny);
-    const double dV = v0[e] - v1[e];
-    if (dLnP > ph.shock_threshold && dV <= 0.0) bits |= (uint8_t)(1u << e);
+    if (shock_between(P0, P1, v0[e] - v1[e], ph.shock_threshold)) bits |= (uint8_t)(1u << e);
   }
   sb[c] = bits;
-}
-
-__global__ void detect_shock_kernel(Box b, Phys ph, const double* __restrict__ U,
-                                    const double* __restrict__ Pst, uint8_t* __restrict__ sb) {
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
-       c += (long long)gridDim.x * blockDim.x)
-    detect_shock_cell(b, ph, U, Pst, sb, c);
 }
 
 // DIFFUSIVE_FLUX_I flags after ClearBoundary_CSL_Kernel (FluidFeatures_P__Kernel.f90:
@@ -306,26 +295,136 @@ __device__ __forceinline__ void detect_flags_cell(const Box& b, const uint8_t* s
   df[c] = bits;
 }
 
-__global__ void detect_flags_kernel(Box b, const uint8_t* __restrict__ sb,
-                                    uint8_t* __restrict__ df) {
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < b.nP;
-       c += (long long)gridDim.x * blockDim.x)
-    detect_flags_cell(b, sb, df, c);
+// Tiles of the feature detection over the planes [k0, k1): 32 x 8 cells of a
+// plane per CTA, marching through up to kDetKZ planes of z.  The CTA has one
+// thread per cell of the tile with a one-cell halo (34 x 10, in 12 warps).
+constexpr int kDetTX = 32, kDetTY = 8, kDetKZ = 16;
+constexpr int kDetRX = kDetTX + 2, kDetRY = kDetTY + 2, kDetNR = kDetRX * kDetRY;
+constexpr int kDetThreads = (kDetNR + 31) / 32 * 32;
+
+inline dim3 detect_grid(const Box& b, int k0, int k1) {
+  return dim3((b.n[0] + kDetTX - 1) / kDetTX, (b.n[1] + kDetTY - 1) / kDetTY,
+              (k1 - k0 + kDetKZ - 1) / kDetKZ);
 }
 
-// Shock bits and flags of the proper cells [c0, c1) only (whole planes).
-__global__ void detect_shock_range_kernel(Box b, Phys ph, const double* __restrict__ U,
-                                          uint8_t* __restrict__ sb, long long c0, long long c1) {
-  for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1;
-       c += (long long)gridDim.x * blockDim.x)
-    detect_shock_cell(b, ph, U, nullptr, sb, c);
-}
-
-__global__ void detect_flags_range_kernel(Box b, const uint8_t* __restrict__ sb,
-                                          uint8_t* __restrict__ df, long long c0, long long c1) {
-  for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1;
-       c += (long long)gridDim.x * blockDim.x)
-    detect_flags_cell(b, sb, df, c);
+// Shock bits (detect_shock_cell) and DIFFUSIVE_FLUX_I flags (detect_flags_cell)
+// of the proper cells of planes [k0, k1) in one pass, from the conserved state
+// U or (PST) from the compact primitives Pst (N, V1, V2, V3, E).  For every
+// plane kk each thread recovers pressure and velocities of its halo-tile
+// cell (its loads for plane kk + 1 are issued before the CTA synchronises),
+// forms the cell's shock bits from the -x and -y neighbours in shared memory
+// and the -z neighbour kept in registers, and the CTA keeps three planes of
+// bits in a ring; the flags of plane kk - 1 (threads 0-255, one per tile
+// cell) then read bits of planes kk - 2 to kk only.  A bit that no flag reads
+// (x at the left halo column, y at the bottom halo row, z at the first
+// plane) is left zero, and so is every bit outside the brick, which only
+// cells without flags would read.  Reads the state of planes k0 - 1 to k1
+// (those that exist); writes df of planes [k0, k1).
+template <bool PST>
+__global__ void __launch_bounds__(kDetThreads, 3)
+    detect_features_kernel(Box b, Phys ph, const double* __restrict__ U,
+                           const double* __restrict__ Pst, uint8_t* __restrict__ df, int k0,
+                           int k1) {
+  constexpr int RX = kDetRX, NR = kDetNR;
+  __shared__ double sP[NR], sV1[NR], sV2[NR];
+  __shared__ uint8_t sS[3][NR];
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * kDetTX, j0 = blockIdx.y * kDetTY;
+  const int kb = k0 + blockIdx.z * kDetKZ;
+  const int ke = min(kb + kDetKZ, k1);
+  const double thr = ph.shock_threshold;
+  // the input fields (N is not needed from Pst) and their layout: compact
+  // proper cells, or the ghost layout of U; offsets fit in 32 bits (every
+  // brick has fewer than 2^31 values)
+  const long long fs = PST ? b.nP : b.nV;
+  const double* F0 = PST ? Pst + 4 * fs : U;  // E, or D
+  const double* F1 = (PST ? Pst : U) + fs;
+  const double* F2 = F1 + fs;
+  const double* F3 = F2 + fs;
+  const double* F4 = F3 + fs;  // G (U only)
+  const int plane = PST ? b.n[0] * b.n[1] : b.m[0] * b.m[1];
+  // the halo-tile cell of this thread
+  const int rx = tid % RX, ry = tid / RX;
+  const int gi = i0 - 1 + rx, gj = j0 - 1 + ry;
+  const bool ok = tid < NR && gi >= 0 && gj >= 0 && gi < b.n[0] && gj < b.n[1];
+  const bool has_xm = rx >= 1 && gi >= 1, has_ym = ry >= 1 && gj >= 1;
+  const int gh = PST ? 0 : 2;
+  int off = (gi + gh) + (PST ? b.n[0] : b.m[0]) * (gj + gh) + plane * (kb - 1 + gh);
+  double raw[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  auto fetch = [&](int kk) {
+    if (ok && kk >= 0 && kk < b.n[2]) {
+      raw[0] = F0[off];
+      raw[1] = F1[off];
+      raw[2] = F2[off];
+      raw[3] = F3[off];
+      if (!PST) raw[4] = F4[off];
+    }
+  };
+  fetch(kb - 1);
+  double Pz = 0.0, Vz = 0.0;  // the plane below
+  // the output cell of this thread (threads 0-255)
+  const int ox = tid % kDetTX, oy = tid / kDetTX;
+  const int i = i0 + ox, j = j0 + oy, ro = (ox + 1) + RX * (oy + 1);
+  const bool out_in = tid < kDetTX * kDetTY && i < b.n[0] && j < b.n[1];
+  const bool inner_xy = i >= 1 && j >= 1 && i <= b.n[0] - 2 && j <= b.n[1] - 2;
+  for (int kk = kb - 1; kk <= ke; ++kk) {
+    const bool live = ok && kk >= 0 && kk < b.n[2];
+    double P = 0.0, V1 = 0.0, V2 = 0.0, V3 = 0.0;
+    if (live) {
+      if (PST) {
+        P = ph.gm1 * raw[0];
+        V1 = raw[1];
+        V2 = raw[2];
+        V3 = raw[3];
+      } else {
+        Cons u{raw[0], raw[1], raw[2], raw[3], raw[4]};
+        Prim w;
+        cons_to_prim(u, w, ph.nmin);
+        P = ph.gm1 * w.E;
+        V1 = w.V1;
+        V2 = w.V2;
+        V3 = w.V3;
+      }
+    }
+    off += plane;
+    if (kk < ke) fetch(kk + 1);
+    if (tid < NR) {
+      sP[tid] = P;
+      sV1[tid] = V1;
+      sV2[tid] = V2;
+    }
+    __syncthreads();
+    if (tid < NR) {
+      uint8_t bits = 0;
+      if (live) {
+        if (has_xm && shock_between(P, sP[tid - 1], V1 - sV1[tid - 1], thr)) bits |= 1;
+        if (has_ym && shock_between(P, sP[tid - RX], V2 - sV2[tid - RX], thr)) bits |= 2;
+        if (kk >= 1 && kk >= kb && shock_between(P, Pz, V3 - Vz, thr)) bits |= 4;
+      }
+      sS[(kk + 3) % 3][tid] = bits;
+    }
+    Pz = P;
+    Vz = V3;
+    __syncthreads();
+    const int k = kk - 1;
+    if (k >= kb && out_in) {
+      uint8_t bits = 0;
+      if (inner_xy && k >= 1 && k <= b.n[2] - 2) {
+        const uint8_t* m = sS[(k + 2) % 3];  // plane k - 1
+        const uint8_t* c = sS[k % 3];
+        const uint8_t* p = sS[(k + 1) % 3];
+        const unsigned s0 = c[ro], sxp = c[ro + 1], sxm = c[ro - 1], syp = c[ro + RX],
+                       sym = c[ro - RX], szp = p[ro], szm = m[ro];
+        const unsigned sxp_ym = c[ro + 1 - RX], syp_xm = c[ro + RX - 1], sxp_zm = m[ro + 1],
+                       syp_zm = m[ro + RX], szp_xm = p[ro - 1], szp_ym = p[ro - RX];
+        // flag d from bit e at c, c + e_e, c - e_d and c + e_e - e_d (e != d)
+        if (((s0 | syp | sxm | syp_xm) & 2) || ((s0 | szp | sxm | szp_xm) & 4)) bits |= 1;
+        if (((s0 | sxp | sym | sxp_ym) & 1) || ((s0 | szp | sym | szp_ym) & 4)) bits |= 2;
+        if (((s0 | sxp | szm | sxp_zm) & 1) || ((s0 | syp | szm | syp_zm) & 2)) bits |= 4;
+      }
+      df[i + (long long)b.n[0] * (j + (long long)b.n[1] * k)] = bits;
+    }
+  }
 }
 
 __global__ void batch_detect_shock_kernel(const BatchBrick* __restrict__ bb, int n,

@@ -431,6 +431,30 @@ __device__ __forceinline__ Cons floored_cons(const Cons& u, const Prim& w, doubl
   return f;
 }
 
+// RN(a / m) > t, exactly, for a >= 0 (or NaN) and m > 0.  The product
+// p = RN(t m) carries a relative error of at most 2^-53 when it is normal, so
+// a > RN(p (1 + 2^-50)) implies a / m > t (1 + 2^-51) >= t + ulp(t), and
+// a < RN(p (1 - 2^-50)) implies a / m < t (1 - 2^-51) <= pred(t): the
+// rounded quotient is then above t, resp. not above it.  Only between the two
+// bounds (or out of the exponent window) is the division carried out.
+__device__ __forceinline__ bool quotient_exceeds(double a, double m, double t) {
+  const double p = t * m;
+  if (t >= 0x1p-1000 && t <= 0x1p1000 && p >= 0x1p-960 && p <= 0x1p960) {
+    if (a > p * (1.0 + 0x1p-50)) return true;
+    if (a < p * (1.0 - 0x1p-50)) return false;
+  }
+  return a / m > t;
+}
+
+// The shock test of DetectShocks_CSL_Kernel (FluidFeatures_P__Kernel.f90:
+// 12-186) between a cell (pressure P0) and its lower neighbour along one
+// axis (P1), dV the difference of their normal velocities.
+__device__ __forceinline__ bool shock_between(double P0, double P1, double dV, double thr) {
+  const double dP = fabs(P0 - P1);
+  const double pmin = (P0 < P1) ? P0 : P1;  // Fortran MIN: ties give either
+  return quotient_exceeds(dP, fmax2(pmin, kSqrtTiny), thr) && dV <= 0.0;
+}
+
 // Apply_EOS_I_E_Kernel for a cell value: pressure, sound speed and (when
 // asked) the entropy per baryon.
 __device__ __forceinline__ void eos_cell(double N, double E, const Phys& ph, double& P,

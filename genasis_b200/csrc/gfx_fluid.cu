@@ -412,13 +412,23 @@ __global__ void scatter_flags_kernel(Box b, const uint8_t* __restrict__ df,
   }
 }
 
+// DIFFUSIVE_FLUX_I flags of the planes [k0, k1), from U or from the compact
+// primitives Pst when given (reads the state of planes k0 - 1 to k1).
+cudaError_t launch_features(const Box& b, const Phys& ph, const double* U, const double* Pst,
+                            uint8_t* df, int k0, int k1, cudaStream_t s) {
+  if (k1 <= k0) return cudaSuccess;
+  if (Pst)
+    detect_features_kernel<true>
+        <<<detect_grid(b, k0, k1), kDetThreads, 0, s>>>(b, ph, U, Pst, df, k0, k1);
+  else
+    detect_features_kernel<false>
+        <<<detect_grid(b, k0, k1), kDetThreads, 0, s>>>(b, ph, U, Pst, df, k0, k1);
+  return cudaGetLastError();
+}
+
 int run_features(gfx_fluid* h, const double* U, const double* Pst, cudaStream_t s) {
-  const int blk = 256;
-  detect_shock_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->ph, U, Pst, h->sb);
-  CUDA_TRY(cudaGetLastError());
-  detect_flags_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->sb, h->df);
-  CUDA_TRY(cudaGetLastError());
-  h->launches += 2;
+  CUDA_TRY(launch_features(h->box, h->ph, U, Pst, h->df, 0, h->box.n[2], s));
+  h->launches += 1;
   return GFX_OK;
 }
 
@@ -427,13 +437,7 @@ int run_features(gfx_fluid* h, const double* U, const double* Pst, cudaStream_t 
 // nothing else touches the state; the same values the recovery from the
 // stored, floored state gives).
 int run_features_wn(gfx_fluid* h, const double* U, cudaStream_t s) {
-  const int blk = 256;
-  detect_shock_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->ph, U, h->wn, h->sb);
-  CUDA_TRY(cudaGetLastError());
-  detect_flags_kernel<<<grid_for(h->box.nP, blk), blk, 0, s>>>(h->box, h->sb, h->df);
-  CUDA_TRY(cudaGetLastError());
-  h->launches += 2;
-  return GFX_OK;
+  return run_features(h, U, h->wn, s);
 }
 
 // The launches of one RK2 step on U (in place).  dt_ptr, skip: device scalars.
@@ -583,7 +587,6 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   cudaStream_t sc = h->host_stream, si = h->copy_in, so = h->copy_out;
   double* U = h->U_stage;
   const size_t nV = (size_t)b.nV, plane = (size_t)b.m[0] * b.m[1];
-  const long long cplane = (long long)b.n[0] * b.n[1];
   const int n2 = b.n[2];
   auto copy = [&](cudaStream_t st, int nf, int p0, int p1, cudaMemcpyKind kind) -> cudaError_t {
     for (int q = 0; q < nf; ++q) {
@@ -624,28 +627,19 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
                         nullptr, h->items + it[j], it[j + 1] - it[j],
                         h->slab_counters + (mode == MODE_STAGE1 ? 0 : S) + j, h->ph, sc);
   };
-  auto shock = [&](int j) {
-    const long long c0 = zs[j] * cplane, c1 = zs[j + 1] * cplane;
-    detect_shock_range_kernel<<<grid_for(c1 - c0, blk), blk, 0, sc>>>(b, h->ph, U, h->sb, c0,
-                                                                       c1);
+  auto flags = [&](int j) -> cudaError_t {
     ++launches;
+    return launch_features(b, h->ph, U, nullptr, h->df, zs[j], zs[j + 1], sc);
   };
-  auto flags = [&](int j) {
-    const long long c0 = zs[j] * cplane, c1 = zs[j + 1] * cplane;
-    detect_flags_range_kernel<<<grid_for(c1 - c0, blk), blk, 0, sc>>>(b, h->sb, h->df, c0, c1);
-    ++launches;
-  };
-  // slab j: its shock bits once its planes are in; the flags of slab j-1
-  // (which read the first plane of slab j); stage 1 of slab j-2 (which reads
-  // two planes into slab j-1 and the flags of its top face)
+  // once slab j is in: the flags of slab j-1 (which read the first plane of
+  // slab j), then stage 1 of slab j-2 (which reads two planes into slab j-1
+  // and the flags of its top face)
   for (int j = 0; j < S; ++j) {
     CUDA_TRY(cudaStreamWaitEvent(sc, h->ev_in[j], 0));
-    if (detect) shock(j);
-    if (detect && j >= 1) flags(j - 1);
+    if (detect && j >= 1) CUDA_TRY(flags(j - 1));
     if (j >= 2) CUDA_TRY(stage(MODE_STAGE1, j - 2));
   }
-  if (detect) flags(S - 1);
-  CUDA_TRY(cudaGetLastError());
+  if (detect) CUDA_TRY(flags(S - 1));
   if (S >= 2) CUDA_TRY(stage(MODE_STAGE1, S - 2));
   CUDA_TRY(stage(MODE_STAGE1, S - 1));
   // stage 2 slab by slab, each slab's in-plane ghosts, then its copy back
@@ -1480,7 +1474,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Byte offsets of the step's buffers inside the scratch array.
 struct NoAllocLayout {
-  size_t geo[3], edge[3], yp, h, df, sb, bits, counters, dt, items, total;
+  size_t geo[3], edge[3], yp, h, df, bits, counters, dt, items, total;
 };
 
 // Parameters of the set-up kernel: the chart of the brick, the work list's
@@ -1639,8 +1633,6 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
   off = align256(off + 5 * nP * sizeof(double));
   L.df = off;
   off = align256(off + nP);
-  L.sb = off;
-  off = align256(off + nP);
   L.bits = off;
   off = align256(off + 2 * sizeof(unsigned long long));
   L.counters = off;
@@ -1653,7 +1645,7 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
   if (L.total > kNoAllocScratchBytes)
     return fail(GFX_ERR_ARGUMENT,
                 "brick %d x %d x %d needs %zu bytes of scratch; the no-allocation step has "
-                "%zu: about 82 bytes per proper cell plus the chart tables, so up to about 50000 "
+                "%zu: about 81 bytes per proper cell plus the chart tables, so up to about 50000 "
                 "proper cells (37^3 fits, 38^3 does not)",
                 b.n[0], b.n[1], b.n[2], L.total, kNoAllocScratchBytes);
   unsigned char* base = nullptr;
@@ -1694,14 +1686,7 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
   const bool hllc = cfg->riemann_solver == GFX_RIEMANN_HLLC;
   const bool grav = cfg->uniform_acceleration != 0.0;
   uint8_t* df = (uint8_t*)(base + L.df);
-  uint8_t* sb = (uint8_t*)(base + L.sb);
-  const int blk = 256;
-  if (hllc && detect_features) {
-    detect_shock_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, ph, U, nullptr, sb);
-    CUDA_TRY(cudaGetLastError());
-    detect_flags_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, sb, df);
-    CUDA_TRY(cudaGetLastError());
-  }
+  if (hllc && detect_features) CUDA_TRY(launch_features(b, ph, U, nullptr, df, 0, b.n[2], s));
   const uint8_t* feat = (hllc && detect_features) ? df : nullptr;
   BrickDesc d;
   memset(&d, 0, sizeof(d));
@@ -1733,7 +1718,7 @@ int gfx_fluid_step_noalloc(const gfx_fluid_config* cfg, double* U, double dt,
   d2.P_in = d.Yp;
   CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, p.items, p.n_items,
                         p.counters + 1, ph, s));
-  ghost_refresh_kernel<<<grid_for(b.nV, blk), blk, 0, s>>>(b, ph, U);
+  ghost_refresh_kernel<<<grid_for(b.nV, 256), 256, 0, s>>>(b, ph, U);
   CUDA_TRY(cudaGetLastError());
   return GFX_OK;
 }
@@ -1806,7 +1791,7 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
   if (!h->adj) {
     if (cudaMalloc(&h->adj, 20 * nP * sizeof(double)) != cudaSuccess)
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
-    if (cudaMalloc(&h->adj_flags, 2 * nP) != cudaSuccess)
+    if (cudaMalloc(&h->adj_flags, nP) != cudaSuccess)
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
   }
   if (!U_np1 && !h->adj_U) {
@@ -1818,17 +1803,14 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
   double* lamW = lamZ + 5 * nP;
   double* lamK1 = lamW + 5 * nP;
   uint8_t* df = h->adj_flags;
-  uint8_t* sb = df + nP;
   const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
   const bool grav = h->cfg.uniform_acceleration != 0.0;
   const int blk = 256;
   // features of U^n (zero for the first step after initialisation)
   const uint8_t* feat = nullptr;
   if (hllc && detect_features) {
-    detect_shock_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, U_n, nullptr, sb);
-    detect_flags_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, sb, df);
-    CUDA_TRY(cudaGetLastError());
-    h->launches += 2;
+    CUDA_TRY(launch_features(b, h->ph, U_n, nullptr, df, 0, b.n[2], s));
+    h->launches += 1;
     feat = df;
   }
   // forward recomputation from the checkpoint: W0, stage 1 (W1 into Yp) and,

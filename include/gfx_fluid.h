@@ -218,7 +218,7 @@ int gfx_fluid_step_adjoint(gfx_fluid *h, const double *U_n_dev, double dt,
  * It allocates nothing: its tables and stage buffers live in one fixed
  * array of GFX_FLUID_NOALLOC_SCRATCH_BYTES of device memory inside the
  * library, which every GPU that loads the library holds until exit.  That
- * bounds the brick at about 82 bytes per proper cell plus the chart tables
+ * bounds the brick at about 81 bytes per proper cell plus the chart tables
  * (37^3 proper cells fit, 38^3 do not); larger bricks get GFX_ERR_ARGUMENT.
  * The first call on a device looks up the array's device address (and sets
  * up the stage kernels' launch attributes if no step ran before); make that
