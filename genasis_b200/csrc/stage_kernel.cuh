@@ -187,6 +187,36 @@ __device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph
   dst[4 * NT] = w.E;
 }
 
+// Asynchronous 8-byte copies from global to shared memory (cp.async, which
+// needs no registers and lets the thread go on until cp_async_wait_all).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Starts the asynchronous copy of the stored primitives of cell (gx, gy, gz)
+// (possibly ghosts) into 5 shared slots at stride `stride`, unless the
+// boundary map reverses a velocity there: then it starts nothing and returns
+// false, and the caller loads the cell with load_cell / load_cell_col.
+__device__ __forceinline__ bool copy_prim_async(const BrickDesc& B, double* dst, int stride,
+                                                int gx, int gy, int gz) {
+  bool nx, ny, nz;
+  const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
+  const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
+  const int sz = bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
+  if (nx || ny || nz) return false;
+  const double* p = B.P_in + (sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz));
+#pragma unroll
+  for (int q = 0; q < 5; ++q) cp_async8(dst + q * stride, p + q * B.nP);
+  return true;
+}
+
 // Reconstructed face states of the face between cells (im) and (ip) along one
 // axis, IncrementDivergence_FV__Kernel.f90:70-90: V_IL = V(i-1) + dXR(i-1) dVdX(i-1),
 // V_IR = V(i) - dXL(i) dVdX(i).
@@ -314,7 +344,10 @@ struct StageLayout {
   static constexpr int kFy = NF * (TY + 1) * TX;
   static constexpr int kGx = G_NTAB * (TX + 4);
   static constexpr int kGy = G_NTAB * (TY + 4);
-  static constexpr int kDoubles = kFull + kCen + kZs + kZf + kSx + kSy + kFx + kFy + kGx + kGy;
+  static constexpr int kNH = 4 * TX + 4 * TY;  // x / y halo cells of a plane
+  static constexpr int kHalo = 5 * kNH;        // halo of plane k+1 in flight
+  static constexpr int kDoubles =
+      kFull + kCen + kZs + kZf + kSx + kSy + kFx + kFy + kGx + kGy + kHalo;
   static constexpr size_t kBytes = sizeof(double) * kDoubles;
 };
 
@@ -460,6 +493,8 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
   double* fys = fxs + SL::kFx;
   double* gxc = fys + SL::kFy;
   double* gyc = gxc + SL::kGx;
+  double* hbuf = gyc + SL::kGy;
+  constexpr int NH = SL::kNH;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
   __shared__ BrickDesc s_desc;
@@ -506,29 +541,45 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
                                                   gy, z0, own, dt);
     __syncthreads();  // geometry caches
 
+    // the halo cell of this thread (threads below NH): two rows below and
+    // above the tile, two columns left and right
+    int hx = 0, hy = 0;
+    if (tid < 4 * TX) {
+      const int s = tid / TX;
+      hx = tid % TX;
+      hy = (s < 2) ? s - 2 : TY + s - 2;
+    } else if (tid < NH) {
+      const int j = tid - 4 * TX, s = j % 4;
+      hy = j / 4;
+      hx = (s < 2) ? s - 2 : TX + s - 2;
+    }
+    // with stored primitives as input (IN_PRIM) the halo of plane k+1 and the
+    // own column's plane k+2 are copied asynchronously during plane k;
+    // halo_ready: this thread's halo cell of plane k is in hbuf
+    bool halo_ready = false;
+
     for (int k = z0; k < z1; ++k) {
       // (1) plane k into the full buffer: own centre from its slot, the
-      // x / y halo loaded; plane k+2 into the freed slot
+      // x / y halo from hbuf or loaded; plane k+2 into the freed slot
       {
         double* src = cslot(k);
 #pragma unroll
         for (int q = 0; q < 5; ++q) full[q * PS + c_off] = src[q * NT];
       }
-      load_cell_col<IN_PRIM, TYt>(B, ph, cslot(k + 2), gx, gy, k + 2);
-      if (tid < 4 * TX + 4 * TY) {
-        // the halo: two rows below and above the tile, two columns left and right
-        int lx, ly;
-        if (tid < 4 * TX) {
-          const int s = tid / TX;
-          lx = tid % TX;
-          ly = (s < 2) ? s - 2 : TY + s - 2;
+      if (!(IN_PRIM && copy_prim_async(B, cslot(k + 2), NT, gx, gy, k + 2)))
+        load_cell_col<IN_PRIM, TYt>(B, ph, cslot(k + 2), gx, gy, k + 2);
+      if (tid < NH) {
+        if (halo_ready) {
+          const int o = (hy + 2) * PW + (hx + 2);
+#pragma unroll
+          for (int q = 0; q < 5; ++q) full[q * PS + o] = hbuf[q * NH + tid];
         } else {
-          const int j = tid - 4 * TX, s = j % 4;
-          ly = j / 4;
-          lx = (s < 2) ? s - 2 : TX + s - 2;
+          load_cell<IN_PRIM, TYt>(B, ph, full, hx, hy, x0 + hx, y0 + hy, k);
         }
-        load_cell<IN_PRIM, TYt>(B, ph, full, lx, ly, x0 + lx, y0 + ly, k);
+        halo_ready = IN_PRIM && k + 1 < z1 &&
+                     copy_prim_async(B, hbuf + tid, NH, x0 + hx, y0 + hy, k + 1);
       }
+      if (IN_PRIM) cp_async_commit();
       __syncthreads();
 
       // (2) slopes: x [TY][TX+2], y [TY+2][TX] of plane k
@@ -625,7 +676,9 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         }
       }
 
-      // (4) z slope at k+1 and z face k+1 of the own column
+      // (4) z slope at k+1 and z face k+1 of the own column (after this
+      // thread's copies of plane k+2 and of the halo of plane k+1 landed)
+      if (IN_PRIM) cp_async_wait_all();
       double zsn[5], zfn[NF];
       if (PARAB) {
         // zsn: the outer values of plane k+1; the face takes the outer
@@ -764,7 +817,10 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       for (int q = 0; q < 5; ++q) zss[q * NT + tid] = zsn[q];
 #pragma unroll
       for (int u = 0; u < NF; ++u) zfs[u * NT + tid] = zfn[u];
-      __syncthreads();
+      // no barrier here: the next plane's phase (1) writes only this
+      // thread's centre and slots and the halo cells, none of which the
+      // update above reads from other threads (it reads their x / y fluxes,
+      // rewritten only after two more barriers)
     }
 
     if (MODE == MODE_STAGE2) {
