@@ -144,6 +144,9 @@ int num_sms() {
 
 }  // namespace
 
+// z slabs of the pipelined gfx_fluid_step_host
+constexpr int kMaxSlabs = 16;
+
 struct gfx_fluid {
   gfx_fluid_config cfg;
   Phys ph;
@@ -188,8 +191,10 @@ struct gfx_fluid {
   double* wn = nullptr;  // [5][nP]: the primitives of the state the last stage 2 wrote
   // pipelined gfx_fluid_step_host: copy streams, per-slab events and counters
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
-  cudaEvent_t ev_in[8] = {}, ev_out[8] = {}, ev_end = nullptr;
-  int* slab_counters = nullptr;  // [16]
+  cudaEvent_t ev_in[kMaxSlabs] = {}, ev_out[kMaxSlabs] = {}, ev_end = nullptr;
+  int* slab_counters = nullptr;  // [2 * kMaxSlabs]
+  WorkItem* host_items = nullptr;  // the work list of the slabs, z chunks of host_chunk
+  int host_n_items = 0, host_chunk = 0, host_tile_y = 0;
 };
 
 namespace {
@@ -552,9 +557,11 @@ namespace {
 // five fields D, S1, S2, S3, G of every plane: DS is rewritten by the step and
 // never read), the compute, and the copy of the result (all six fields).
 // Shock detection and stage 1 of a slab start as soon as its planes and the
-// two above it have arrived; every slab is copied back as soon as its stage 2
-// and the x / y ghosts of its planes are done, while stage 2 of the next slab
-// runs; the z ghost planes, which reach across the brick, come last.  The
+// two above it have arrived; stage 2 of a slab as soon as stage 1 of the slab
+// above it is done, and every slab is copied back as soon as its stage 2 and
+// the x / y ghosts of its planes are done, so that the copies back overlap
+// the copies in of later slabs; the z ghost planes, which reach across the
+// brick, come last.  The
 // launches and their inputs are those of gfx_fluid_step, so the result is
 // the same bit for bit.  Returns GFX_ERR_UNSUPPORTED when the work list is too
 // short to pipeline (the caller then takes the unpipelined path).
@@ -562,32 +569,48 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   const Box& b = h->box;
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   if (h->prims_pending) return GFX_ERR_UNSUPPORTED;
-  std::vector<WorkItem> items = make_items(b.n, 0, h->z_chunk, h->tile_y);
+  // the slabs' own work list: z chunks of the tuned length, shortened so
+  // that the brick has up to kMaxSlabs of them (at least 2 planes each)
+  const int n2 = b.n[2];
+  const WorkItem first = make_items(b.n, 0, h->z_chunk, h->tile_y)[0];
+  const int len0 = first.z1 - first.z0;
+  const int len = std::min(len0, std::max(2, (n2 + kMaxSlabs - 1) / kMaxSlabs));
+  const int nchunks = (n2 + len - 1) / len;
+  if (nchunks < 2 || n2 - (nchunks - 1) * len < 2) return GFX_ERR_UNSUPPORTED;
+  if (h->host_chunk != len || h->host_tile_y != h->tile_y) {
+    std::vector<WorkItem> items = make_items(b.n, 0, len, h->tile_y);
+    cudaFree(h->host_items);
+    h->host_items = nullptr;
+    h->host_chunk = 0;
+    if (cudaMalloc(&h->host_items, items.size() * sizeof(WorkItem)) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc slab work items");
+    CUDA_TRY(cudaMemcpy(h->host_items, items.data(), items.size() * sizeof(WorkItem),
+                        cudaMemcpyHostToDevice));
+    h->host_n_items = (int)items.size();
+    h->host_chunk = len;
+    h->host_tile_y = h->tile_y;
+  }
   const int cols = ((b.n[0] + TX - 1) / TX) * ((b.n[1] + h->tile_y - 1) / h->tile_y);
-  const int nchunks = (int)items.size() / cols;
-  const int len = items[0].z1 - items[0].z0;
-  if (nchunks < 2 || len < 2 || (int)items.size() != h->n_items)
-    return GFX_ERR_UNSUPPORTED;
-  const int S = std::min(8, nchunks);
-  int it[9], zs[9];
+  const int S = std::min(kMaxSlabs, nchunks);
+  int it[kMaxSlabs + 1], zs[kMaxSlabs + 1];
   for (int j = 0; j <= S; ++j) {
     const int c = (int)((long long)j * nchunks / S);
     it[j] = c * cols;
-    zs[j] = (j == S) ? b.n[2] : items[(size_t)c * cols].z0;
+    zs[j] = (j == S) ? n2 : c * len;
   }
   if (!h->copy_in) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
   if (!h->copy_out) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < kMaxSlabs; ++j) {
     if (!h->ev_in[j]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_in[j], cudaEventDisableTiming));
     if (!h->ev_out[j]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_out[j], cudaEventDisableTiming));
   }
   if (!h->ev_end) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_end, cudaEventDisableTiming));
-  if (!h->slab_counters && cudaMalloc(&h->slab_counters, 16 * sizeof(int)) != cudaSuccess)
+  if (!h->slab_counters &&
+      cudaMalloc(&h->slab_counters, 2 * kMaxSlabs * sizeof(int)) != cudaSuccess)
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc slab counters");
   cudaStream_t sc = h->host_stream, si = h->copy_in, so = h->copy_out;
   double* U = h->U_stage;
   const size_t nV = (size_t)b.nV, plane = (size_t)b.m[0] * b.m[1];
-  const int n2 = b.n[2];
   auto copy = [&](cudaStream_t st, int nf, int p0, int p1, cudaMemcpyKind kind) -> cudaError_t {
     for (int q = 0; q < nf; ++q) {
       const size_t off = q * nV + (size_t)p0 * plane;
@@ -624,35 +647,50 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   auto stage = [&](int mode, int j) -> cudaError_t {
     ++launches;
     return launch_stage(mode, mode == MODE_STAGE2, hllc, grav, mode == MODE_STAGE1 ? d1 : d2,
-                        nullptr, h->items + it[j], it[j + 1] - it[j],
+                        nullptr, h->host_items + it[j], it[j + 1] - it[j],
                         h->slab_counters + (mode == MODE_STAGE1 ? 0 : S) + j, h->ph, sc);
   };
+  // the flags of planes [g(j), g(j+1)) with g(j) = zs[j] + 1 inside the
+  // brick: those of slab j shifted up one plane, so that they include the
+  // first plane of slab j+1 (whose flags stage 1 of slab j reads) and need the
+  // state up to the second plane of slab j+1 only
+  auto g = [&](int j) { return (j == 0) ? 0 : (j == S) ? n2 : zs[j] + 1; };
   auto flags = [&](int j) -> cudaError_t {
     ++launches;
-    return launch_features(b, h->ph, U, nullptr, h->df, zs[j], zs[j + 1], sc);
+    return launch_features(b, h->ph, U, nullptr, h->df, g(j), g(j + 1), sc);
   };
-  // once slab j is in: the flags of slab j-1 (which read the first plane of
-  // slab j), then stage 1 of slab j-2 (which reads two planes into slab j-1
-  // and the flags of its top face)
-  for (int j = 0; j < S; ++j) {
-    CUDA_TRY(cudaStreamWaitEvent(sc, h->ev_in[j], 0));
-    if (detect && j >= 1) CUDA_TRY(flags(j - 1));
-    if (j >= 2) CUDA_TRY(stage(MODE_STAGE1, j - 2));
-  }
-  if (detect) CUDA_TRY(flags(S - 1));
-  if (S >= 2) CUDA_TRY(stage(MODE_STAGE1, S - 2));
-  CUDA_TRY(stage(MODE_STAGE1, S - 1));
-  // stage 2 slab by slab, each slab's in-plane ghosts, then its copy back
-  for (int j = 0; j < S; ++j) {
-    CUDA_TRY(stage(MODE_STAGE2, j));
+  // stage 2 of slab j, the x / y ghosts of its planes, then its copy back
+  auto finish = [&](int j) -> cudaError_t {
+    cudaError_t e = stage(MODE_STAGE2, j);
+    if (e != cudaSuccess) return e;
     const long long v0 = (long long)(zs[j] + 2) * plane, v1 = (long long)(zs[j + 1] + 2) * plane;
     ghost_refresh_range_kernel<<<grid_for(v1 - v0, blk), blk, 0, sc>>>(b, h->ph, U, v0, v1);
-    CUDA_TRY(cudaGetLastError());
     ++launches;
-    CUDA_TRY(cudaEventRecord(h->ev_out[j], sc));
-    CUDA_TRY(cudaStreamWaitEvent(so, h->ev_out[j], 0));
-    CUDA_TRY(copy(so, 6, zs[j] + 2, zs[j + 1] + 2, cudaMemcpyDeviceToHost));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(h->ev_out[j], sc)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(so, h->ev_out[j], 0)) != cudaSuccess) return e;
+    return copy(so, 6, zs[j] + 2, zs[j + 1] + 2, cudaMemcpyDeviceToHost);
+  };
+  // Once slab j is in: the flags of range j-1 and stage 1 of slab j-1 (which
+  // reads two planes into slab j); then stage 2 of slab j-2, whose state no
+  // later detection or stage 1 reads, so that its copy back overlaps the
+  // copy in of the slabs still to come.  On a periodic z axis stage 1 of the
+  // last slab reads the first planes of slab 0, which is therefore finished
+  // last.
+  const bool zper = b.bc[2][0] == BC_PERIODIC;
+  int fin = zper ? 1 : 0;  // the next slab to finish
+  for (int j = 0; j < S; ++j) {
+    CUDA_TRY(cudaStreamWaitEvent(sc, h->ev_in[j], 0));
+    if (j >= 1) {
+      if (detect) CUDA_TRY(flags(j - 1));
+      CUDA_TRY(stage(MODE_STAGE1, j - 1));
+    }
+    while (fin <= j - 2) CUDA_TRY(finish(fin++));
   }
+  if (detect) CUDA_TRY(flags(S - 1));
+  CUDA_TRY(stage(MODE_STAGE1, S - 1));
+  while (fin < S) CUDA_TRY(finish(fin++));
+  if (zper) CUDA_TRY(finish(0));
   // the z ghost planes, then their copy back and the fluence
   ghost_refresh_range_kernel<<<grid_for(2 * (long long)plane, blk), blk, 0, sc>>>(
       b, h->ph, U, 0, 2 * (long long)plane);
@@ -816,7 +854,8 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->partials);
   cudaFree(h->wn);
   cudaFree(h->slab_counters);
-  for (int j = 0; j < 8; ++j) {
+  cudaFree(h->host_items);
+  for (int j = 0; j < kMaxSlabs; ++j) {
     if (h->ev_in[j]) cudaEventDestroy(h->ev_in[j]);
     if (h->ev_out[j]) cudaEventDestroy(h->ev_out[j]);
   }
