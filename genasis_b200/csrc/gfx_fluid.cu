@@ -500,6 +500,7 @@ struct gfx_fluid_batch {
   bool hllc = false, grav = false;
   BrickDesc* d1 = nullptr;   // stage 1 from conserved input, per brick
   BrickDesc* d1p = nullptr;  // stage 1 from kept primitives, per brick
+  BrickDesc* d1w = nullptr;  // stage 1 from the primitives the last stage 2 stored
   BrickDesc* d2 = nullptr;   // stage 2, per brick
   WorkItem* items = nullptr;
   int n_items = 0;
@@ -517,8 +518,10 @@ struct gfx_fluid_batch {
 namespace {
 
 // The launches of one batched cycle: shock flags (HLLC), the two stages for
-// every brick, ghosts, then each brick's clock and next time step.
-int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, bool in_prim, cudaStream_t s) {
+// every brick, ghosts, then each brick's clock and next time step.  d1: the
+// stage-1 descriptors (input from primitives when in_prim).
+int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, const BrickDesc* d1, bool in_prim,
+                        cudaStream_t s) {
   const int blk = 256;
   reset_bits_kernel<<<grid_for(std::max(B->n, 4), blk), blk, 0, s>>>(B->tsi_bits, B->n,
                                                                       B->counters, 4);
@@ -535,8 +538,8 @@ int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, bool in_prim, cudaStrea
   BrickDesc none;
   memset(&none, 0, sizeof(none));
   none.tile_y = B->tile_y;
-  CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, B->hllc, false, none, in_prim ? B->d1p : B->d1,
-                        B->items, B->n_items, B->counters, B->ph, s));
+  CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, B->hllc, false, none, d1, B->items, B->n_items,
+                        B->counters, B->ph, s));
   CUDA_TRY(launch_stage(MODE_STAGE2, true, B->hllc, false, none, B->d2, B->items, B->n_items,
                         B->counters + 1, B->ph, s));
   batch_ghost_refresh_kernel<<<grid_for(B->total_v, blk), blk, 0, s>>>(B->bb, B->n,
@@ -1182,10 +1185,11 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
       cudaMalloc(&B->counters, 4 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&B->d1, n * sizeof(BrickDesc)) != cudaSuccess ||
       cudaMalloc(&B->d1p, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&B->d1w, n * sizeof(BrickDesc)) != cudaSuccess ||
       cudaMalloc(&B->d2, n * sizeof(BrickDesc)) != cudaSuccess ||
       cudaMalloc(&B->bb, n * sizeof(BatchBrick)) != cudaSuccess)
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch tables"));
-  std::vector<BrickDesc> d1(n), d1p(n), d2(n);
+  std::vector<BrickDesc> d1(n), d1p(n), d1w(n), d2(n);
   std::vector<BatchBrick> bb(n);
   std::vector<WorkItem> items;
   std::vector<long long> work;
@@ -1196,8 +1200,10 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
     const int* skip = &B->clocks[b].done;
     d1[b] = make_desc(h, U[b], nullptr, nullptr, nullptr, df, nullptr, dt, 0.5, skip);
     d1p[b] = make_desc(h, U[b], nullptr, nullptr, h->Pst, df, nullptr, dt, 0.5, skip);
+    d1w[b] = make_desc(h, U[b], nullptr, nullptr, h->wn, df, nullptr, dt, 0.5, skip);
     d2[b] = make_desc(h, U[b], U[b], nullptr, h->Yp, df, nullptr, dt, 0.5, skip);
-    d1[b].tsi_bits = d1p[b].tsi_bits = d2[b].tsi_bits = B->tsi_bits + b;
+    d2[b].wn = h->wn;
+    d1[b].tsi_bits = d1p[b].tsi_bits = d1w[b].tsi_bits = d2[b].tsi_bits = B->tsi_bits + b;
     bb[b].box = h->box;
     bb[b].U = U[b];
     bb[b].sb = h->sb;
@@ -1231,6 +1237,7 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch work items"));
   if (cudaMemcpy(B->d1, d1.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
       cudaMemcpy(B->d1p, d1p.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(B->d1w, d1w.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
       cudaMemcpy(B->d2, d2.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
       cudaMemcpy(B->bb, bb.data(), n * sizeof(BatchBrick), cudaMemcpyHostToDevice) ||
       cudaMemcpy(B->items, sorted.data(), sorted.size() * sizeof(WorkItem),
@@ -1256,6 +1263,7 @@ int gfx_fluid_batch_destroy(gfx_fluid_batch* B) {
   cudaFree(B->counters);
   cudaFree(B->d1);
   cudaFree(B->d1p);
+  cudaFree(B->d1w);
   cudaFree(B->d2);
   cudaFree(B->bb);
   cudaFree(B->items);
@@ -1321,7 +1329,8 @@ int gfx_fluid_batch_evolve(gfx_fluid_batch* B, double finish_time, int n_cycles,
   CUDA_TRY(cudaGetLastError());
   B->launches += B->n + 1;
   // first cycle eagerly (its primitives and features follow the handles' state)
-  int rc = enqueue_batch_cycle(B, B->hllc && feat_pending == B->n, in_prim, s);
+  int rc = enqueue_batch_cycle(B, B->hllc && feat_pending == B->n, in_prim ? B->d1p : B->d1,
+                               in_prim, s);
   if (rc) return rc;
   for (gfx_fluid* h : B->h) {
     h->prims_pending = false;
@@ -1335,7 +1344,9 @@ int gfx_fluid_batch_evolve(gfx_fluid_batch* B, double finish_time, int n_cycles,
       cudaGraph_t g;
       const long long before = B->launches;
       CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      int rc2 = enqueue_batch_cycle(B, true, false, cs);
+      // the replayed cycles follow a stage 2 of this evolve: stage 1 reads
+      // the primitives it stored
+      int rc2 = enqueue_batch_cycle(B, true, B->d1w, true, cs);
       cudaError_t ce = cudaStreamEndCapture(cs, &g);
       cudaStreamDestroy(cs);
       B->graph_kernels = B->launches - before;
