@@ -147,11 +147,10 @@ __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, do
   plane[4 * PS + o] = w.E;
 }
 
-// Loads the primitives of one cell into a column slot (5 values at stride NT).
-template <bool IN_PRIM, int TYt>
-__device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph, double* dst,
-                                              int gx, int gy, int gz) {
-  GFX_TILE(TYt);
+// Loads the primitives of one cell into 5 shared slots at stride `stride`.
+template <bool IN_PRIM>
+__device__ __forceinline__ void load_cell_to(const BrickDesc& B, const Phys& ph, double* dst,
+                                             int stride, int gx, int gy, int gz) {
   bool nx, ny, nz;
   const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
   const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
@@ -181,10 +180,18 @@ __device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph
   if (ny) w.V2 = -w.V2;
   if (nz) w.V3 = -w.V3;
   dst[0] = w.N;
-  dst[NT] = w.V1;
-  dst[2 * NT] = w.V2;
-  dst[3 * NT] = w.V3;
-  dst[4 * NT] = w.E;
+  dst[stride] = w.V1;
+  dst[2 * stride] = w.V2;
+  dst[3 * stride] = w.V3;
+  dst[4 * stride] = w.E;
+}
+
+// Loads the primitives of one cell into a column slot (5 values at stride NT).
+template <bool IN_PRIM, int TYt>
+__device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph, double* dst,
+                                              int gx, int gy, int gz) {
+  GFX_TILE(TYt);
+  load_cell_to<IN_PRIM>(B, ph, dst, NT, gx, gy, gz);
 }
 
 // Asynchronous 8-byte copies from global to shared memory (cp.async, which
@@ -338,16 +345,23 @@ struct StageLayout {
   static constexpr int kCen = 2 * 5 * NT;         // centres of planes k+1, k+2
   static constexpr int kZs = 5 * NT;              // z slope of plane k (own column)
   static constexpr int kZf = NF * NT;             // z flux of face k (own column)
-  static constexpr int kSx = 5 * TY * (TX + 2);
-  static constexpr int kSy = 5 * (TY + 2) * TX;
+  // HS: the slopes of the x / y halo cells of plane k+1 are formed during
+  // plane k (from the halo copied ahead) into a double-buffered array, so
+  // that the slope phase holds the tile's own cells only; 16-row tiles (with
+  // 8-row tiles two CTAs share an SM and the extra space does not fit)
+  static constexpr bool HS = TYt >= 16;
+  static constexpr int kNHS = 2 * TX + 2 * TYt;  // halo slopes of a plane
+  static constexpr int kSx = HS ? 5 * NT : 5 * TY * (TX + 2);
+  static constexpr int kSy = HS ? 5 * NT : 5 * (TY + 2) * TX;
   static constexpr int kFx = NF * TY * (TX + 1);
   static constexpr int kFy = NF * (TY + 1) * TX;
   static constexpr int kGx = G_NTAB * (TX + 4);
   static constexpr int kGy = G_NTAB * (TY + 4);
   static constexpr int kNH = 4 * TX + 4 * TY;  // x / y halo cells of a plane
-  static constexpr int kHalo = 5 * kNH;        // halo of plane k+1 in flight
+  static constexpr int kHalo = 5 * kNH;        // halo of plane k+1
+  static constexpr int kHs = HS ? 2 * 5 * kNHS : 0;
   static constexpr int kDoubles =
-      kFull + kCen + kZs + kZf + kSx + kSy + kFx + kFy + kGx + kGy + kHalo;
+      kFull + kCen + kZs + kZf + kSx + kSy + kFx + kFy + kGx + kGy + kHalo + kHs;
   static constexpr size_t kBytes = sizeof(double) * kDoubles;
 };
 
@@ -494,7 +508,9 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
   double* gxc = fys + SL::kFy;
   double* gyc = gxc + SL::kGx;
   double* hbuf = gyc + SL::kGy;
-  constexpr int NH = SL::kNH;
+  double* hsl = hbuf + SL::kHalo;
+  constexpr int NH = SL::kNH, NHS = SL::kNHS;
+  constexpr bool HS = SL::HS && !PARAB;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
   __shared__ BrickDesc s_desc;
@@ -539,10 +555,10 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
     // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
     stage_prologue<IN_PRIM, HLLC, NF, PARAB, TYt>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx,
                                                   gy, z0, own, dt);
-    __syncthreads();  // geometry caches
-
     // the halo cell of this thread (threads below NH): two rows below and
-    // above the tile, two columns left and right
+    // above the tile, two columns left and right; hbuf holds it for the next
+    // plane (copied asynchronously from stored primitives where no boundary
+    // map reverses a velocity, loaded otherwise), starting with plane z0
     int hx = 0, hy = 0;
     if (tid < 4 * TX) {
       const int s = tid / TX;
@@ -553,14 +569,74 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       hy = j / 4;
       hx = (s < 2) ? s - 2 : TX + s - 2;
     }
-    // with stored primitives as input (IN_PRIM) the halo of plane k+1 and the
-    // own column's plane k+2 are copied asynchronously during plane k;
-    // halo_ready: this thread's halo cell of plane k is in hbuf
-    bool halo_ready = false;
+    auto fetch_halo = [&](int p) {
+      if (!(IN_PRIM && copy_prim_async(B, hbuf + tid, NH, x0 + hx, y0 + hy, p)))
+        load_cell_to<IN_PRIM>(B, ph, hbuf + tid, NH, x0 + hx, y0 + hy, p);
+    };
+    // HS: the limited slopes of the x / y halo cells of plane p (rows -1 and
+    // TY, columns -1 and TX) from hbuf (plane p's halo) and the own centres
+    // of plane p (cslot(p)) of the tile's edge threads, into hsl[p & 1]
+    auto halo_slope = [&](int h, int p) {
+      const double* cc = cen + (p & 1) * 5 * NT;
+      const double *a, *b, *c, *g;
+      int sa, sb, sc, L, ci;
+      if (h < 2 * TX) {  // y slope of row -1 (s = 0) or row TY (s = 1)
+        const int s = h / TX, lx = h % TX, ly = s ? TY : -1;
+        if (y0 + ly > n1 || x0 + lx >= n0) return;
+        g = gyc;
+        L = LY;
+        ci = ly + 2;
+        if (s == 0) {
+          a = hbuf + lx, sa = NH;
+          b = hbuf + TX + lx, sb = NH;
+          c = cc + lx, sc = NT;
+        } else {
+          a = cc + (TY - 1) * TX + lx, sa = NT;
+          b = hbuf + 2 * TX + lx, sb = NH;
+          c = hbuf + 3 * TX + lx, sc = NH;
+        }
+      } else {  // x slope of column -1 (s = 0) or column TX (s = 1)
+        const int j = h - 2 * TX, s = j / TY, ly = j % TY, lx = s ? TX : -1;
+        if (x0 + lx > n0 || y0 + ly >= n1) return;
+        g = gxc;
+        L = LX;
+        ci = lx + 2;
+        const int hb = 4 * TX + 4 * ly;  // hbuf index of the cell (-2, ly)
+        if (s == 0) {
+          a = hbuf + hb, sa = NH;
+          b = hbuf + hb + 1, sb = NH;
+          c = cc + ly * TX, sc = NT;
+        } else {
+          a = cc + ly * TX + TX - 1, sa = NT;
+          b = hbuf + hb + 2, sb = NH;
+          c = hbuf + hb + 3, sc = NH;
+        }
+      }
+      const double dxl = g[G_DXI * L + ci], dxr = g[G_DXI * L + ci + 1];
+      const double sql = g[G_SQ * L + ci], sqr = g[G_SQ * L + ci + 1];
+      const double cden = g[G_CDEN * L + ci], rdxl = g[G_RDXI * L + ci],
+                   rdxr = g[G_RDXI * L + ci + 1], rcden = g[G_RCDEN * L + ci];
+      double* out = hsl + (p & 1) * 5 * NHS + h;
+#pragma unroll
+      for (int q = 0; q < 5; ++q)
+        out[q * NHS] = limited_slope(a[q * sa], b[q * sb], c[q * sc], dxl, dxr, sql, sqr, cden,
+                                     rdxl, rdxr, rcden, ph.theta, ph.use_limiter);
+    };
+    if (tid < NH) fetch_halo(z0);
+    if (IN_PRIM) {
+      cp_async_commit();
+      cp_async_wait_all();
+    }
+    __syncthreads();  // geometry caches, the halo of plane z0, the own centres
+    if (HS) {
+      if (tid < NHS) halo_slope(tid, z0);
+      __syncthreads();  // (hbuf is refilled next)
+    }
 
     for (int k = z0; k < z1; ++k) {
       // (1) plane k into the full buffer: own centre from its slot, the
-      // x / y halo from hbuf or loaded; plane k+2 into the freed slot
+      // x / y halo from hbuf; then plane k+2 of the own column into the freed
+      // slot and the halo of plane k+1 into hbuf
       {
         double* src = cslot(k);
 #pragma unroll
@@ -569,43 +645,54 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       if (!(IN_PRIM && copy_prim_async(B, cslot(k + 2), NT, gx, gy, k + 2)))
         load_cell_col<IN_PRIM, TYt>(B, ph, cslot(k + 2), gx, gy, k + 2);
       if (tid < NH) {
-        if (halo_ready) {
-          const int o = (hy + 2) * PW + (hx + 2);
+        const int o = (hy + 2) * PW + (hx + 2);
 #pragma unroll
-          for (int q = 0; q < 5; ++q) full[q * PS + o] = hbuf[q * NH + tid];
-        } else {
-          load_cell<IN_PRIM, TYt>(B, ph, full, hx, hy, x0 + hx, y0 + hy, k);
-        }
-        halo_ready = IN_PRIM && k + 1 < z1 &&
-                     copy_prim_async(B, hbuf + tid, NH, x0 + hx, y0 + hy, k + 1);
+        for (int q = 0; q < 5; ++q) full[q * PS + o] = hbuf[q * NH + tid];
+        if (k + 1 < z1) fetch_halo(k + 1);
       }
       if (IN_PRIM) cp_async_commit();
       __syncthreads();
 
-      // (2) slopes: x [TY][TX+2], y [TY+2][TX] of plane k
+      // (2) slopes of plane k: x [TY][TX] and y [TY][TX] of the tile's cells
+      // (HS; the halo cells' slopes came with the previous plane), or
+      // x [TY][TX+2] and y [TY+2][TX] including them
       if (!PARAB) {
-        constexpr int NXS = TY * (TX + 2), NYS = (TY + 2) * TX;
-        constexpr int PXS = (NXS + 31) / 32 * 32;
-        for (int i = tid; i < PXS + NYS; i += NT) {
-          const bool isx = i < PXS;
-          if (isx && i >= NXS) continue;
-          int lx, ly;
-          if (isx) {
-            ly = i / (TX + 2);
-            lx = i % (TX + 2) - 1;
-            if (x0 + lx > n0 || y0 + ly >= n1) continue;
-          } else {
-            const int j = i - PXS;
-            ly = j / TX - 1;
-            lx = j % TX;
-            if (y0 + ly > n1 || x0 + lx >= n0) continue;
+        if (HS) {
+          for (int i = tid; i < 2 * NT; i += NT) {
+            const bool isx = i < NT;
+            const int j = isx ? i : i - NT, ly = j / TX, lx = j % TX;
+            if (isx ? (x0 + lx > n0 || y0 + ly >= n1) : (y0 + ly > n1 || x0 + lx >= n0))
+              continue;
+            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, isx ? 1 : PW, isx ? gxc : gyc,
+                        isx ? LX : LY, isx ? lx + 2 : ly + 2, ph, (isx ? sxs : sys) + j, NT);
           }
-          cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, isx ? 1 : PW, isx ? gxc : gyc,
-                      isx ? LX : LY, isx ? lx + 2 : ly + 2, ph,
-                      isx ? sxs + ly * (TX + 2) + lx + 1 : sys + (ly + 1) * TX + lx,
-                      isx ? TY * (TX + 2) : (TY + 2) * TX);
+        } else {
+          constexpr int NXS = TY * (TX + 2), NYS = (TY + 2) * TX;
+          constexpr int PXS = (NXS + 31) / 32 * 32;
+          for (int i = tid; i < PXS + NYS; i += NT) {
+            const bool isx = i < PXS;
+            if (isx && i >= NXS) continue;
+            int lx, ly;
+            if (isx) {
+              ly = i / (TX + 2);
+              lx = i % (TX + 2) - 1;
+              if (x0 + lx > n0 || y0 + ly >= n1) continue;
+            } else {
+              const int j = i - PXS;
+              ly = j / TX - 1;
+              lx = j % TX;
+              if (y0 + ly > n1 || x0 + lx >= n0) continue;
+            }
+            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, isx ? 1 : PW, isx ? gxc : gyc,
+                        isx ? LX : LY, isx ? lx + 2 : ly + 2, ph,
+                        isx ? sxs + ly * (TX + 2) + lx + 1 : sys + (ly + 1) * TX + lx,
+                        isx ? TY * (TX + 2) : (TY + 2) * TX);
+          }
         }
       }
+      // this thread's copies (plane k+2 of its column, the halo of plane
+      // k+1) have landed; the barrier shows them to the CTA
+      if (IN_PRIM) cp_async_wait_all();
       __syncthreads();
 
       // (3) faces: x [TY][TX+1], y [TY+1][TX] of plane k, one code path for
@@ -624,10 +711,29 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
           if (isx ? (cx > n0 || cy >= n1) : (cy > n1 || cx >= n0)) continue;
           const int o = (ly + 2) * PW + (lx + 2);
           const int step = isx ? 1 : PW;
-          // slope of the cell before the face, and its stride to the next cell
-          const double* sl = isx ? sxs + ly * (TX + 2) + lx : sys + ly * TX + lx;
-          const int sstep = isx ? 1 : TX;
-          const int sstride = isx ? TY * (TX + 2) : (TY + 2) * TX;
+          // slopes of the cells before (sm_) and after (sp) the face, with
+          // their strides between primitives
+          const double *sm_, *sp;
+          int ssm, ssp;
+          if (HS) {
+            const double* hc = hsl + (k & 1) * 5 * NHS;  // halo slopes of plane k
+            const int e = isx ? ly * TX + lx : ly * TX + lx;
+            if (isx) {
+              sm_ = (lx == 0) ? hc + 2 * TX + ly : sxs + e - 1;
+              sp = (lx == TX) ? hc + 2 * TX + TY + ly : sxs + e;
+              ssm = (lx == 0) ? NHS : NT;
+              ssp = (lx == TX) ? NHS : NT;
+            } else {
+              sm_ = (ly == 0) ? hc + lx : sys + e - TX;
+              sp = (ly == TY) ? hc + TX + lx : sys + e;
+              ssm = (ly == 0) ? NHS : NT;
+              ssp = (ly == TY) ? NHS : NT;
+            }
+          } else {
+            sm_ = isx ? sxs + ly * (TX + 2) + lx : sys + ly * TX + lx;
+            sp = sm_ + (isx ? 1 : TX);
+            ssm = ssp = isx ? TY * (TX + 2) : (TY + 2) * TX;
+          }
           const double wr = isx ? gxc[G_WR * LX + lx + 1] : gyc[G_WR * LY + ly + 1];
           const double wl = isx ? gxc[G_WL * LX + lx + 2] : gyc[G_WL * LY + ly + 2];
           double l[5], r[5];
@@ -643,8 +749,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
               r[q] = parabolic_cell(v[0], v[step], v[2 * step], g, L, tm + 1).vI;
             }
           } else {
-            face_prims(full + o - step, sl, PS, full + o, sl + sstep, PS, sstride, sstride, wr,
-                       wl, l, r);
+            face_prims(full + o - step, sm_, PS, full + o, sp, PS, ssm, ssp, wr, wl, l, r);
           }
           FaceState L, R;
           face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
@@ -674,11 +779,16 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
                                             factor);
           }
         }
+        // HS: the halo slopes of plane k+1, on the threads without a face in
+        // the last round of the loop above
+        if (HS && k + 1 < z1) {
+          constexpr int TAIL = (PXF + NYF) % NT;
+          static_assert(TAIL + NHS <= NT, "halo slopes fit beside the last faces");
+          if (tid >= TAIL && tid < TAIL + NHS) halo_slope(tid - TAIL, k + 1);
+        }
       }
 
-      // (4) z slope at k+1 and z face k+1 of the own column (after this
-      // thread's copies of plane k+2 and of the halo of plane k+1 landed)
-      if (IN_PRIM) cp_async_wait_all();
+      // (4) z slope at k+1 and z face k+1 of the own column
       double zsn[5], zfn[NF];
       if (PARAB) {
         // zsn: the outer values of plane k+1; the face takes the outer
