@@ -189,6 +189,7 @@ struct gfx_fluid {
   unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
   double* partials = nullptr;                  // per-block sums of gfx_fluid_totals
   double* wn = nullptr;  // [5][nP]: the primitives of the state the last stage 2 wrote
+  const double* wn_of = nullptr;  // that state (null when unknown or since rewritten)
   // pipelined gfx_fluid_step_host: copy streams, per-slab events and counters
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[kMaxSlabs] = {}, ev_out[kMaxSlabs] = {}, ev_end = nullptr;
@@ -714,6 +715,7 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   h->prims_pending = false;
   h->features = FEAT_PENDING;
   h->features_src = U;
+  h->wn_of = nullptr;  // the staging copy is overwritten by the next call
   return GFX_OK;
 }
 
@@ -899,6 +901,7 @@ int gfx_fluid_from_primitive(gfx_fluid* h, const double* prim, double* U, void* 
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
   h->prims_pending = true;
+  h->wn_of = nullptr;
   return GFX_OK;
 }
 
@@ -909,6 +912,7 @@ int gfx_fluid_to_primitive(gfx_fluid* h, double* U, double* prim, double* aux, v
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
   h->prims_pending = false;
+  h->wn_of = nullptr;
   return GFX_OK;
 }
 
@@ -976,6 +980,7 @@ int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* st
   h->prims_pending = false;
   h->features = FEAT_PENDING;
   h->features_src = U;
+  h->wn_of = U;
   return GFX_OK;
 }
 
@@ -995,6 +1000,7 @@ int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence
   int rc = gfx_fluid_step(h, h->U_stage, dt, fl, s);
   if (rc) return rc;
   h->features_src = h->U_stage;
+  h->wn_of = nullptr;  // the staging copy is overwritten by the next call
   CUDA_TRY(cudaMemcpyAsync(U_host, h->U_stage, bytes, cudaMemcpyDeviceToHost, s));
   if (fluence_host)
     CUDA_TRY(cudaMemcpyAsync(fluence_host, fl, 36 * h->face_size * sizeof(double),
@@ -1063,6 +1069,7 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
     h->prims_pending = false;
     h->features = FEAT_PENDING;
     h->features_src = U;
+    h->wn_of = U;
     // remaining cycles: one graph per cycle, replayed
     if (h->graph && (h->graph_U != U)) {
       cudaGraphExecDestroy(h->graph);
@@ -1121,11 +1128,15 @@ int gfx_fluid_step_timed(gfx_fluid* h, double* U, double dt, double* fluence, do
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
   const bool detect = (h->features == FEAT_PENDING);
-  int rc = enqueue_step(h, U, h->dt_slot, nullptr, fluence, detect, s, ev);
+  // the kernels of an evolve cycle when U is the state this handle's last
+  // stage 2 produced: features and stage 1 from the primitives it stored
+  const bool from_wn = (U == h->wn_of) && !h->prims_pending;
+  int rc = enqueue_step(h, U, h->dt_slot, nullptr, fluence, detect, s, ev, from_wn);
   if (rc == GFX_OK) {
     h->prims_pending = false;
     h->features = FEAT_PENDING;
     h->features_src = U;
+    h->wn_of = U;
     cudaError_t e = cudaEventSynchronize(ev[4]);
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
       float ms = 0.f;
@@ -1335,6 +1346,7 @@ int gfx_fluid_batch_evolve(gfx_fluid_batch* B, double finish_time, int n_cycles,
   for (gfx_fluid* h : B->h) {
     h->prims_pending = false;
     h->features = FEAT_PENDING;
+    h->wn_of = nullptr;
   }
   for (int b = 0; b < B->n; ++b) B->h[b]->features_src = B->U[b];
   if (n_cycles > 1) {
@@ -1410,6 +1422,7 @@ int gfx_fluid_resume(gfx_fluid* h, double* U) {
   h->prims_pending = false;
   h->features = FEAT_PENDING;
   h->features_src = U;
+  h->wn_of = nullptr;
   return GFX_OK;
 }
 

@@ -155,7 +155,11 @@ int gfx_fluid_evolve(gfx_fluid *h, double *U_dev, double time, int i_cycle,
 /* gfx_fluid_step with a CUDA event recorded around each launch (the
  * reference's per-phase timers, StorageDivergence_Form.f90:45-74): ms_out[4]
  * receives the device milliseconds of features, stage 1, stage 2 and the
- * ghost refresh.  Synchronises the stream. */
+ * ghost refresh.  Synchronises the stream.  It times the kernels of an
+ * evolve cycle: when U_dev is the state that the last step, timed step or
+ * evolve on this handle produced, features and stage 1 start from the
+ * primitives that step's stage 2 stored, so U_dev must not have been changed
+ * since by other means. */
 int gfx_fluid_step_timed(gfx_fluid *h, double *U_dev, double dt, double *fluence_dev,
                          double *ms_out, void *stream);
 
