@@ -207,21 +207,67 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Starts the asynchronous copy of the stored primitives of cell (gx, gy, gz)
-// (possibly ghosts) into 5 shared slots at stride `stride`, unless the
-// boundary map reverses a velocity there: then it starts nothing and returns
-// false, and the caller loads the cell with load_cell / load_cell_col.
-__device__ __forceinline__ bool copy_prim_async(const BrickDesc& B, double* dst, int stride,
-                                                int gx, int gy, int gz) {
+// Starts the asynchronous copy of the input values of cell (gx, gy, gz)
+// (possibly ghosts) into 5 shared slots at stride `stride`: the stored
+// primitives N, V1, V2, V3, E (IN_PRIM, compact layout) or the conserved D,
+// S1, S2, S3, G (ghost layout).  cell_flips: the velocity components the
+// boundary map reverses there (bit d: V_d+1), which finish_cell applies once
+// the copy has landed.
+__device__ __forceinline__ int cell_flips(const BrickDesc& B, int gx, int gy, int gz) {
+  bool nx, ny, nz;
+  bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
+  bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
+  bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
+  return (int)nx | ((int)ny << 1) | ((int)nz << 2);
+}
+
+template <bool IN_PRIM>
+__device__ __forceinline__ void copy_cell_async(const BrickDesc& B, double* dst, int stride,
+                                               int gx, int gy, int gz) {
   bool nx, ny, nz;
   const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
   const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
   const int sz = bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
-  if (nx || ny || nz) return false;
-  const double* p = B.P_in + (sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz));
+  (void)nx, (void)ny, (void)nz;
+  const double* p;
+  long long fs;
+  if (IN_PRIM) {
+    p = B.P_in + (sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz));
+    fs = B.nP;
+  } else {
+    p = B.U_in + ((sx + 2) + (long long)B.m[0] * ((sy + 2) + (long long)B.m[1] * (sz + 2)));
+    fs = B.nV;
+  }
 #pragma unroll
-  for (int q = 0; q < 5; ++q) cp_async8(dst + q * stride, p + q * B.nP);
-  return true;
+  for (int q = 0; q < 5; ++q) cp_async8(dst + q * stride, p + q * fs);
+}
+
+// After this thread's copy_cell_async into the slots has landed: the
+// primitives of the cell there (recovered from the conserved values for a
+// conserved input), with the reversed velocities negated -- the values
+// load_cell_to gives.
+template <bool IN_PRIM>
+__device__ __forceinline__ void finish_cell(const Phys& ph, double* dst, int stride, int flips) {
+  if (IN_PRIM && !flips) return;
+  Prim w;
+  if (IN_PRIM) {
+    w.N = dst[0];
+    w.V1 = dst[stride];
+    w.V2 = dst[2 * stride];
+    w.V3 = dst[3 * stride];
+    w.E = dst[4 * stride];
+  } else {
+    Cons c{dst[0], dst[stride], dst[2 * stride], dst[3 * stride], dst[4 * stride]};
+    cons_to_prim(c, w, ph.nmin);
+  }
+  if (flips & 1) w.V1 = -w.V1;
+  if (flips & 2) w.V2 = -w.V2;
+  if (flips & 4) w.V3 = -w.V3;
+  dst[0] = w.N;
+  dst[stride] = w.V1;
+  dst[2 * stride] = w.V2;
+  dst[3 * stride] = w.V3;
+  dst[4 * stride] = w.E;
 }
 
 // Reconstructed face states of the face between cells (im) and (ip) along one
@@ -569,10 +615,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       hy = j / 4;
       hx = (s < 2) ? s - 2 : TX + s - 2;
     }
-    auto fetch_halo = [&](int p) {
-      if (!(IN_PRIM && copy_prim_async(B, hbuf + tid, NH, x0 + hx, y0 + hy, p)))
-        load_cell_to<IN_PRIM>(B, ph, hbuf + tid, NH, x0 + hx, y0 + hy, p);
-    };
+
     // HS: the limited slopes of the x / y halo cells of plane p (rows -1 and
     // TY, columns -1 and TX) from hbuf (plane p's halo) and the own centres
     // of plane p (cslot(p)) of the tile's edge threads, into hsl[p & 1]
@@ -622,11 +665,11 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         out[q * NHS] = limited_slope(a[q * sa], b[q * sb], c[q * sc], dxl, dxr, sql, sqr, cden,
                                      rdxl, rdxr, rcden, ph.theta, ph.use_limiter);
     };
-    if (tid < NH) fetch_halo(z0);
-    if (IN_PRIM) {
-      cp_async_commit();
-      cp_async_wait_all();
-    }
+    if (tid < NH) copy_cell_async<IN_PRIM>(B, hbuf + tid, NH, x0 + hx, y0 + hy, z0);
+    cp_async_commit();
+    cp_async_wait_all();
+    if (tid < NH)
+      finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips(B, x0 + hx, y0 + hy, z0));
     __syncthreads();  // geometry caches, the halo of plane z0, the own centres
     if (HS) {
       if (tid < NHS) halo_slope(tid, z0);
@@ -642,15 +685,14 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
 #pragma unroll
         for (int q = 0; q < 5; ++q) full[q * PS + c_off] = src[q * NT];
       }
-      if (!(IN_PRIM && copy_prim_async(B, cslot(k + 2), NT, gx, gy, k + 2)))
-        load_cell_col<IN_PRIM, TYt>(B, ph, cslot(k + 2), gx, gy, k + 2);
+      copy_cell_async<IN_PRIM>(B, cslot(k + 2), NT, gx, gy, k + 2);
       if (tid < NH) {
         const int o = (hy + 2) * PW + (hx + 2);
 #pragma unroll
         for (int q = 0; q < 5; ++q) full[q * PS + o] = hbuf[q * NH + tid];
-        if (k + 1 < z1) fetch_halo(k + 1);
+        if (k + 1 < z1) copy_cell_async<IN_PRIM>(B, hbuf + tid, NH, x0 + hx, y0 + hy, k + 1);
       }
-      if (IN_PRIM) cp_async_commit();
+      cp_async_commit();
       __syncthreads();
 
       // (2) slopes of plane k: x [TY][TX] and y [TY][TX] of the tile's cells
@@ -691,8 +733,12 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         }
       }
       // this thread's copies (plane k+2 of its column, the halo of plane
-      // k+1) have landed; the barrier shows them to the CTA
-      if (IN_PRIM) cp_async_wait_all();
+      // k+1) have landed and become primitives; the barrier shows them to
+      // the CTA
+      cp_async_wait_all();
+      finish_cell<IN_PRIM>(ph, cslot(k + 2), NT, cell_flips(B, gx, gy, k + 2));
+      if (tid < NH && k + 1 < z1)
+        finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips(B, x0 + hx, y0 + hy, k + 1));
       __syncthreads();
 
       // (3) faces: x [TY][TX+1], y [TY+1][TX] of plane k, one code path for
