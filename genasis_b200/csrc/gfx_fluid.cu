@@ -145,7 +145,7 @@ int num_sms() {
 }  // namespace
 
 // z slabs of the pipelined gfx_fluid_step_host
-constexpr int kMaxSlabs = 16;
+constexpr int kMaxSlabs = 32;
 
 struct gfx_fluid {
   gfx_fluid_config cfg;
@@ -573,16 +573,35 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   const Box& b = h->box;
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   if (h->prims_pending) return GFX_ERR_UNSUPPORTED;
-  // the slabs' own work list: z chunks of the tuned length, shortened so
-  // that the brick has up to kMaxSlabs of them (at least 2 planes each)
+  // the slabs' own work list, cut along z into chunks of at least 2 planes:
+  // kThin chunks of half length first (the copies back begin once the first
+  // slabs are computed, so these arrive and finish early), then chunks of
+  // the tuned length, shortened so that the brick has up to kMaxSlabs slabs
+  constexpr int kThin = 4;
   const int n2 = b.n[2];
   const WorkItem first = make_items(b.n, 0, h->z_chunk, h->tile_y)[0];
   const int len0 = first.z1 - first.z0;
   const int len = std::min(len0, std::max(2, (n2 + kMaxSlabs - 1) / kMaxSlabs));
-  const int nchunks = (n2 + len - 1) / len;
-  if (nchunks < 2 || n2 - (nchunks - 1) * len < 2) return GFX_ERR_UNSUPPORTED;
-  if (h->host_chunk != len || h->host_tile_y != h->tile_y) {
-    std::vector<WorkItem> items = make_items(b.n, 0, len, h->tile_y);
+  const int thin = std::max(2, len / 2);
+  const int n_thin = (n2 >= kThin * thin + 2 * len) ? kThin : 0;
+  std::vector<int> cz(1, 0);
+  for (int c = 0; c < n_thin; ++c) cz.push_back(cz.back() + thin);
+  {
+    const int rest = n2 - cz.back();
+    int l = len;
+    while (rest % l == 1 && l < rest) ++l;  // no one-plane chunk at the end
+    for (int z = cz.back() + l; z < n2; z += l) cz.push_back(z);
+    cz.push_back(n2);
+  }
+  const int nchunks = (int)cz.size() - 1;
+  if (nchunks < 2 || cz[nchunks] - cz[nchunks - 1] < 2) return GFX_ERR_UNSUPPORTED;
+  const int ty = h->tile_y;
+  const int cx = (b.n[0] + TX - 1) / TX, cy = (b.n[1] + ty - 1) / ty, cols = cx * cy;
+  if (h->host_chunk != len || h->host_tile_y != ty) {
+    std::vector<WorkItem> items;
+    for (int c = 0; c < nchunks; ++c)
+      for (int y = 0; y < cy; ++y)
+        for (int x = 0; x < cx; ++x) items.push_back({0, x * TX, y * ty, cz[c], cz[c + 1]});
     cudaFree(h->host_items);
     h->host_items = nullptr;
     h->host_chunk = 0;
@@ -592,15 +611,18 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
                         cudaMemcpyHostToDevice));
     h->host_n_items = (int)items.size();
     h->host_chunk = len;
-    h->host_tile_y = h->tile_y;
+    h->host_tile_y = ty;
   }
-  const int cols = ((b.n[0] + TX - 1) / TX) * ((b.n[1] + h->tile_y - 1) / h->tile_y);
+  // slabs: the thin chunks one by one, the others in even groups
   const int S = std::min(kMaxSlabs, nchunks);
+  const int S_thin = std::min(n_thin, S - 1);
   int it[kMaxSlabs + 1], zs[kMaxSlabs + 1];
   for (int j = 0; j <= S; ++j) {
-    const int c = (int)((long long)j * nchunks / S);
+    const int c = (j <= S_thin) ? j
+                                : S_thin + (int)((long long)(j - S_thin) * (nchunks - S_thin) /
+                                                 (S - S_thin));
     it[j] = c * cols;
-    zs[j] = (j == S) ? n2 : c * len;
+    zs[j] = cz[c];
   }
   if (!h->copy_in) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
   if (!h->copy_out) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));

@@ -1,7 +1,8 @@
 """gfx_fluid_step_host on host arrays: the pipelined path (z slabs copied in,
 computed and copied back on three streams) gives the device step's result
 bit for bit, state and boundary fluence, over consecutive steps, for every
-kind of z boundary."""
+kind of z boundary, with thin first slabs and with slabs of several chunks
+(tall bricks)."""
 import numpy as np
 import pytest
 
@@ -21,7 +22,13 @@ def _cases():
                       n_ramp_cycles=1,
                       boundary=(("OUTFLOW", "REFLECTING"), ("PERIODIC", "PERIODIC"),
                                 ("OUTFLOW", "OUTFLOW")))
+    tall_p = FluidConfig(n_cells=(12, 8, 300), boundary=(("PERIODIC", "PERIODIC"),) * 3,
+                         riemann_solver="HLLC", courant_factor=0.8, n_ramp_cycles=1)
+    tall_o = FluidConfig(n_cells=(12, 8, 150), riemann_solver="HLLC", courant_factor=0.8,
+                         n_ramp_cycles=1)
     return {
+        "tall_hllc_periodic": (tall_p, problems.random_state(tall_p, seed=14)),
+        "tall_hllc_outflow": (tall_o, problems.random_state(tall_o, seed=15)),
         "random_hllc_periodic": (kh_cfg, problems.random_state(kh_cfg, seed=12)),
         "rt_hllc_gravity_reflecting": (rt_cfg, rt),
         "random_hll_outflow": (mix, problems.random_state(mix, seed=13)),
@@ -32,7 +39,7 @@ CASES = _cases()
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("z_chunk", [4, 0])
+@pytest.mark.parametrize("z_chunk", [4, 16, 0])
 def test_host_step_matches_the_device_step(name, z_chunk):
     import torch
 
