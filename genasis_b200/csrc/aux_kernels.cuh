@@ -367,7 +367,11 @@ __global__ void __launch_bounds__(kDetThreads, 3)
   const int i = i0 + ox, j = j0 + oy, ro = (ox + 1) + RX * (oy + 1);
   const bool out_in = tid < kDetTX * kDetTY && i < b.n[0] && j < b.n[1];
   const bool inner_xy = i >= 1 && j >= 1 && i <= b.n[0] - 2 && j <= b.n[1] - 2;
-  for (int kk = kb - 1; kk <= ke; ++kk) {
+  const int cplane = b.n[0] * b.n[1];
+  int dfo = i + b.n[0] * j + cplane * (kb - 2);  // df offset of (i, j, kk - 1)
+  // the ring slots of planes kk, kk - 1 and kk - 2
+  uint8_t *s_new = sS[0], *s_cur = sS[2], *s_old = sS[1];
+  for (int kk = kb - 1; kk <= ke; ++kk, dfo += cplane) {
     const bool live = ok && kk >= 0 && kk < b.n[2];
     double P = 0.0, V1 = 0.0, V2 = 0.0, V3 = 0.0;
     if (live) {
@@ -401,7 +405,7 @@ __global__ void __launch_bounds__(kDetThreads, 3)
         if (has_ym && shock_between(P, sP[tid - RX], V2 - sV2[tid - RX], thr)) bits |= 2;
         if (kk >= 1 && kk >= kb && shock_between(P, Pz, V3 - Vz, thr)) bits |= 4;
       }
-      sS[(kk + 3) % 3][tid] = bits;
+      s_new[tid] = bits;
     }
     Pz = P;
     Vz = V3;
@@ -410,9 +414,9 @@ __global__ void __launch_bounds__(kDetThreads, 3)
     if (k >= kb && out_in) {
       uint8_t bits = 0;
       if (inner_xy && k >= 1 && k <= b.n[2] - 2) {
-        const uint8_t* m = sS[(k + 2) % 3];  // plane k - 1
-        const uint8_t* c = sS[k % 3];
-        const uint8_t* p = sS[(k + 1) % 3];
+        const uint8_t* m = s_old;  // plane k - 1
+        const uint8_t* c = s_cur;
+        const uint8_t* p = s_new;
         const unsigned s0 = c[ro], sxp = c[ro + 1], sxm = c[ro - 1], syp = c[ro + RX],
                        sym = c[ro - RX], szp = p[ro], szm = m[ro];
         const unsigned sxp_ym = c[ro + 1 - RX], syp_xm = c[ro + RX - 1], sxp_zm = m[ro + 1],
@@ -422,8 +426,12 @@ __global__ void __launch_bounds__(kDetThreads, 3)
         if (((s0 | sxp | sym | sxp_ym) & 1) || ((s0 | szp | sym | szp_ym) & 4)) bits |= 2;
         if (((s0 | sxp | szm | sxp_zm) & 1) || ((s0 | syp | szm | syp_zm) & 2)) bits |= 4;
       }
-      df[i + (long long)b.n[0] * (j + (long long)b.n[1] * k)] = bits;
+      df[dfo] = bits;
     }
+    uint8_t* t = s_old;
+    s_old = s_cur;
+    s_cur = s_new;
+    s_new = t;
   }
 }
 
