@@ -204,7 +204,7 @@ template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED,
           bool PARAB = false, int TYt = kTileY>
 cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
                            int n_items, int* counter, const Phys& ph, cudaStream_t s) {
-  using SM = StageLayout<NF, TYt>;
+  using SM = StageLayout<NF, TYt, PARAB>;
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
   static int per_sm = 1;

@@ -23,19 +23,23 @@ namespace gfx {
 constexpr int TX = 32;          // tile width (x), one warp per row
 constexpr int kTileY = 16;      // default tile rows; 8 is the other height built
 
-// The tile shape TX x TYt and what follows from it: NT threads per CTA, the
-// plane pitch PW and height PH with the 2-cell halo, PS doubles per plane and
-// variable.  Functions that depend on the tile take TYt as a template
-// parameter and open with GFX_TILE(TYt).
-#define GFX_TILE(TYt)                          \
-  constexpr int TY = (TYt);                    \
-  constexpr int NT = TX * TY;                  \
-  constexpr int PW = TX + 4;                   \
-  constexpr int PH = TY + 4;                   \
-  constexpr int PS = PW * PH;                  \
-  (void)TY; (void)NT; (void)PW; (void)PH; (void)PS
+// The tile shape TX x TYt and what follows from it: NT threads per CTA.
+// Functions that depend on the tile take TYt as a template parameter and
+// open with GFX_TILE(TYt).
+#define GFX_TILE(TYt)       \
+  constexpr int TY = (TYt); \
+  constexpr int NT = TX * TY; \
+  (void)TY; (void)NT
 // CTAs per SM the registers allow at 128 registers per thread
 constexpr int tile_min_ctas(int ty) { return (TX * ty >= 512) ? 1 : 2; }
+// Ring of halo cells around the tile in the full plane: two for PARABOLIC
+// (each face reconstructs both its cells) and for 16-row tiles (where the
+// compiler keeps more in registers with that pitch); one for 8-row tiles,
+// whose two CTAs per SM need the smaller plane (faces and slopes read the
+// neighbours only; the halo cells' own slopes come from the halo buffer).
+__host__ __device__ constexpr int full_ring(bool parab, int ty) {
+  return (parab || ty >= 16) ? 2 : 1;
+}
 
 enum { MODE_INCREMENT = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
 enum { BC_OUTFLOW = 0, BC_REFLECTING = 1, BC_PERIODIC = 2 };
@@ -107,10 +111,11 @@ __device__ __forceinline__ int bc_map(int g, int n, int bc_lo, int bc_hi, bool& 
 
 // Loads the primitives of cell (gx, gy) of plane gz (all possibly ghosts) into
 // a ring plane at local (ly, lx).
-template <bool IN_PRIM, int TYt>
+template <bool IN_PRIM, int TYt, int FR>
 __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, double* plane,
                                           int lx, int ly, int gx, int gy, int gz) {
   GFX_TILE(TYt);
+  constexpr int FW = TX + 2 * FR, FS = FW * (TY + 2 * FR);
   bool nx, ny, nz;
   const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
   const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
@@ -139,12 +144,12 @@ __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, do
   if (nx) w.V1 = -w.V1;
   if (ny) w.V2 = -w.V2;
   if (nz) w.V3 = -w.V3;
-  const int o = (ly + 2) * PW + (lx + 2);
+  const int o = (ly + FR) * FW + (lx + FR);
   plane[o] = w.N;
-  plane[PS + o] = w.V1;
-  plane[2 * PS + o] = w.V2;
-  plane[3 * PS + o] = w.V3;
-  plane[4 * PS + o] = w.E;
+  plane[FS + o] = w.V1;
+  plane[2 * FS + o] = w.V2;
+  plane[3 * FS + o] = w.V3;
+  plane[4 * FS + o] = w.E;
 }
 
 // Loads the primitives of one cell into 5 shared slots at stride `stride`.
@@ -384,18 +389,19 @@ __device__ __forceinline__ void fill_geo(const AxisGeo& G, int m, int t0, int L,
   }
 }
 
-template <int NF, int TYt>
+template <int NF, int TYt, bool PARAB = false>
 struct StageLayout {
-  static constexpr int TY = TYt, NT = TX * TYt, PW = TX + 4, PH = TYt + 4, PS = PW * PH;
-  static constexpr int kFull = 5 * PS;            // plane k with its x / y halo
+  static constexpr int TY = TYt, NT = TX * TYt;
+  static constexpr int FR = full_ring(PARAB, TYt), FW = TX + 2 * FR, FS = FW * (TY + 2 * FR);
+  static constexpr int kFull = 5 * FS;            // plane k with its x / y halo ring
   static constexpr int kCen = 2 * 5 * NT;         // centres of planes k+1, k+2
   static constexpr int kZs = 5 * NT;              // z slope of plane k (own column)
   static constexpr int kZf = NF * NT;             // z flux of face k (own column)
-  // HS: the slopes of the x / y halo cells of plane k+1 are formed during
-  // plane k (from the halo copied ahead) into a double-buffered array, so
-  // that the slope phase holds the tile's own cells only; 16-row tiles (with
-  // 8-row tiles two CTAs share an SM and the extra space does not fit)
-  static constexpr bool HS = TYt >= 16;
+  // HS (all but PARABOLIC, which has no slope phase): the slopes of the x / y
+  // halo cells of plane k+1 are formed during plane k (from the halo copied
+  // ahead) into a double-buffered array, so that the slope phase holds the
+  // tile's own cells only
+  static constexpr bool HS = !PARAB;
   static constexpr int kNHS = 2 * TX + 2 * TYt;  // halo slopes of a plane
   static constexpr int kSx = HS ? 5 * NT : 5 * TY * (TX + 2);
   static constexpr int kSy = HS ? 5 * NT : 5 * (TY + 2) * TX;
@@ -498,21 +504,22 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
                                             int tx, int ty, int gx, int gy, int z0, bool own,
                                             double dt) {
   GFX_TILE(TYt);
+  constexpr int FR = full_ring(PARAB, TYt), FW = TX + 2 * FR, FS = FW * (TY + 2 * FR);
   auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
-  double* fc = full + (ty + 2) * PW + (tx + 2);
-  load_cell<IN_PRIM, TYt>(B, ph, full, tx, ty, gx, gy, z0 - 2);
+  double* fc = full + (ty + FR) * FW + (tx + FR);
+  load_cell<IN_PRIM, TYt, FR>(B, ph, full, tx, ty, gx, gy, z0 - 2);
   load_cell_col<IN_PRIM, TYt>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
   load_cell_col<IN_PRIM, TYt>(B, ph, cslot(z0), gx, gy, z0);
   double s_m[5], s_0[5], vI0[5];
   if (PARAB)
-    z_parabolic(B, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, vI0, s_m);
+    z_parabolic(B, z0 - 1, fc, FS, cslot(z0 - 1), NT, cslot(z0), NT, vI0, s_m);
   else
-    z_slope(B.geo[2], ph, z0 - 1, fc, PS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
-  load_cell<IN_PRIM, TYt>(B, ph, full, tx, ty, gx, gy, z0 + 1);
+    z_slope(B.geo[2], ph, z0 - 1, fc, FS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
+  load_cell<IN_PRIM, TYt, FR>(B, ph, full, tx, ty, gx, gy, z0 + 1);
   if (PARAB)
-    z_parabolic(B, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, vI0, s_0);
+    z_parabolic(B, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, FS, vI0, s_0);
   else
-    z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, PS, s_0);
+    z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, FS, s_0);
   double F[NF];
   if (PARAB)
     z_face_lr<HLLC, NF>(B, ph, z0, s_m, vI0, gx, gy, own, dt, F);
@@ -526,7 +533,7 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
   // plane z0+1 into its centre slot (the slot of z0-1)
   double* d = cslot(z0 + 1);
 #pragma unroll
-  for (int q = 0; q < 5; ++q) d[q * NT] = fc[q * PS];
+  for (int q = 0; q < 5; ++q) d[q * NT] = fc[q * FS];
 }
 
 // BATCHED: the work items span many bricks; each item's brick descriptor is
@@ -541,7 +548,8 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
                  const WorkItem* __restrict__ items, int n_items, int* __restrict__ counter,
                  const __grid_constant__ Phys ph) {
   GFX_TILE(TYt);
-  using SL = StageLayout<NF, TYt>;
+  using SL = StageLayout<NF, TYt, PARAB>;
+  constexpr int FR = SL::FR, FW = SL::FW, FS = SL::FS;
   extern __shared__ double smem[];
   double* full = smem;
   double* cen = full + SL::kFull;
@@ -556,7 +564,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
   double* hbuf = gyc + SL::kGy;
   double* hsl = hbuf + SL::kHalo;
   constexpr int NH = SL::kNH, NHS = SL::kNHS;
-  constexpr bool HS = SL::HS && !PARAB;
+  constexpr bool HS = SL::HS;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
   __shared__ BrickDesc s_desc;
@@ -564,7 +572,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  const int c_off = (ty + 2) * PW + (tx + 2);  // own cell in the full plane
+  const int c_off = (ty + FR) * FW + (tx + FR);  // own cell in the full plane
   const BrickDesc& B = BATCHED ? s_desc : single;
 
   for (;;) {
@@ -596,7 +604,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
     fill_geo<TYt>(B.geo[1], B.m[1], y0, LY, gyc, tid);
 
     // own column helpers: a "column pointer" addresses 5 values at stride NT
-    // (centre slots) or PS (full plane)
+    // (centre slots) or FS (full plane)
     auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
     // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
     stage_prologue<IN_PRIM, HLLC, NF, PARAB, TYt>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx,
@@ -683,53 +691,30 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       {
         double* src = cslot(k);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) full[q * PS + c_off] = src[q * NT];
+        for (int q = 0; q < 5; ++q) full[q * FS + c_off] = src[q * NT];
       }
       copy_cell_async<IN_PRIM>(B, cslot(k + 2), NT, gx, gy, k + 2);
       if (tid < NH) {
-        const int o = (hy + 2) * PW + (hx + 2);
+        if (hx >= -FR && hx < TX + FR && hy >= -FR && hy < TY + FR) {  // in the ring
+          const int o = (hy + FR) * FW + (hx + FR);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) full[q * PS + o] = hbuf[q * NH + tid];
+          for (int q = 0; q < 5; ++q) full[q * FS + o] = hbuf[q * NH + tid];
+        }
         if (k + 1 < z1) copy_cell_async<IN_PRIM>(B, hbuf + tid, NH, x0 + hx, y0 + hy, k + 1);
       }
       cp_async_commit();
       __syncthreads();
 
       // (2) slopes of plane k: x [TY][TX] and y [TY][TX] of the tile's cells
-      // (HS; the halo cells' slopes came with the previous plane), or
-      // x [TY][TX+2] and y [TY+2][TX] including them
-      if (!PARAB) {
-        if (HS) {
-          for (int i = tid; i < 2 * NT; i += NT) {
-            const bool isx = i < NT;
-            const int j = isx ? i : i - NT, ly = j / TX, lx = j % TX;
-            if (isx ? (x0 + lx > n0 || y0 + ly >= n1) : (y0 + ly > n1 || x0 + lx >= n0))
-              continue;
-            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, isx ? 1 : PW, isx ? gxc : gyc,
-                        isx ? LX : LY, isx ? lx + 2 : ly + 2, ph, (isx ? sxs : sys) + j, NT);
-          }
-        } else {
-          constexpr int NXS = TY * (TX + 2), NYS = (TY + 2) * TX;
-          constexpr int PXS = (NXS + 31) / 32 * 32;
-          for (int i = tid; i < PXS + NYS; i += NT) {
-            const bool isx = i < PXS;
-            if (isx && i >= NXS) continue;
-            int lx, ly;
-            if (isx) {
-              ly = i / (TX + 2);
-              lx = i % (TX + 2) - 1;
-              if (x0 + lx > n0 || y0 + ly >= n1) continue;
-            } else {
-              const int j = i - PXS;
-              ly = j / TX - 1;
-              lx = j % TX;
-              if (y0 + ly > n1 || x0 + lx >= n0) continue;
-            }
-            cell_slopes(full + (ly + 2) * PW + (lx + 2), PS, isx ? 1 : PW, isx ? gxc : gyc,
-                        isx ? LX : LY, isx ? lx + 2 : ly + 2, ph,
-                        isx ? sxs + ly * (TX + 2) + lx + 1 : sys + (ly + 1) * TX + lx,
-                        isx ? TY * (TX + 2) : (TY + 2) * TX);
-          }
+      // (the halo cells' slopes came with the previous plane); PARABOLIC has
+      // no slope phase
+      if (HS) {
+        for (int i = tid; i < 2 * NT; i += NT) {
+          const bool isx = i < NT;
+          const int j = isx ? i : i - NT, ly = j / TX, lx = j % TX;
+          if (isx ? (x0 + lx > n0 || y0 + ly >= n1) : (y0 + ly > n1 || x0 + lx >= n0)) continue;
+          cell_slopes(full + (ly + FR) * FW + (lx + FR), FS, isx ? 1 : FW, isx ? gxc : gyc,
+                      isx ? LX : LY, isx ? lx + 2 : ly + 2, ph, (isx ? sxs : sys) + j, NT);
         }
       }
       // this thread's copies (plane k+2 of its column, the halo of plane
@@ -755,15 +740,16 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
           const int lx = isx ? j % (TX + 1) : j % TX;
           const int cx = x0 + lx, cy = y0 + ly;
           if (isx ? (cx > n0 || cy >= n1) : (cy > n1 || cx >= n0)) continue;
-          const int o = (ly + 2) * PW + (lx + 2);
-          const int step = isx ? 1 : PW;
+          const int o = (ly + FR) * FW + (lx + FR);
+          const int step = isx ? 1 : FW;
           // slopes of the cells before (sm_) and after (sp) the face, with
-          // their strides between primitives
+          // their strides between primitives: the tile's own slopes, or the
+          // halo slopes of plane k at the tile's edges (HS)
           const double *sm_, *sp;
           int ssm, ssp;
           if (HS) {
-            const double* hc = hsl + (k & 1) * 5 * NHS;  // halo slopes of plane k
-            const int e = isx ? ly * TX + lx : ly * TX + lx;
+            const double* hc = hsl + (k & 1) * 5 * NHS;
+            const int e = ly * TX + lx;
             if (isx) {
               sm_ = (lx == 0) ? hc + 2 * TX + ly : sxs + e - 1;
               sp = (lx == TX) ? hc + 2 * TX + TY + ly : sxs + e;
@@ -775,10 +761,6 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
               ssm = (ly == 0) ? NHS : NT;
               ssp = (ly == TY) ? NHS : NT;
             }
-          } else {
-            sm_ = isx ? sxs + ly * (TX + 2) + lx : sys + ly * TX + lx;
-            sp = sm_ + (isx ? 1 : TX);
-            ssm = ssp = isx ? TY * (TX + 2) : (TY + 2) * TX;
           }
           const double wr = isx ? gxc[G_WR * LX + lx + 1] : gyc[G_WR * LY + ly + 1];
           const double wl = isx ? gxc[G_WL * LX + lx + 2] : gyc[G_WL * LY + ly + 2];
@@ -790,12 +772,12 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             const int tm = (isx ? cx : cy) + 1;  // ghost-layout index of the cell before
 #pragma unroll 1
             for (int q = 0; q < 5; ++q) {
-              const double* v = full + q * PS + o - step;
+              const double* v = full + q * FS + o - step;
               l[q] = parabolic_cell(v[-step], v[0], v[step], g, L, tm).vO;
               r[q] = parabolic_cell(v[0], v[step], v[2 * step], g, L, tm + 1).vI;
             }
           } else {
-            face_prims(full + o - step, sm_, PS, full + o, sp, PS, ssm, ssp, wr, wl, l, r);
+            face_prims(full + o - step, sm_, FS, full + o, sp, FS, ssm, ssp, wr, wl, l, r);
           }
           FaceState L, R;
           face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
@@ -840,13 +822,13 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         // zsn: the outer values of plane k+1; the face takes the outer
         // values of plane k (zss) and the inner ones of plane k+1
         double zI[5], zl[5];
-        z_parabolic(B, k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zI, zsn);
+        z_parabolic(B, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zI, zsn);
 #pragma unroll
         for (int q = 0; q < 5; ++q) zl[q] = zss[q * NT + tid];
         z_face_lr<HLLC, NF>(B, ph, k + 1, zl, zI, gx, gy, own, dt, zfn);
       } else {
-        z_slope(GZ, ph, k + 1, full + c_off, PS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
-        z_face<HLLC, NF>(B, ph, k + 1, full + c_off, PS, zss + tid, NT, cslot(k + 1), NT, zsn,
+        z_slope(GZ, ph, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
+        z_face<HLLC, NF>(B, ph, k + 1, full + c_off, FS, zss + tid, NT, cslot(k + 1), NT, zsn,
                          1, gx, gy, own, dt, zfn);
       }
       __syncthreads();
@@ -897,8 +879,8 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
           }
         }
         if (MODE != MODE_INCREMENT) {
-          const double N = full[c_off], V1 = full[PS + c_off], V2 = full[2 * PS + c_off],
-                       V3 = full[3 * PS + c_off], E = full[4 * PS + c_off];
+          const double N = full[c_off], V1 = full[FS + c_off], V2 = full[2 * FS + c_off],
+                       V3 = full[3 * FS + c_off], E = full[4 * FS + c_off];
           if (GRAV) {
             // ApplyGravity_F (ApplyGravity_F__Command.f90:124-264) with the
             // uniform gradient (0, 0, a); the x and y momentum terms subtract
