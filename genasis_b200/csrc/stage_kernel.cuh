@@ -1,13 +1,17 @@
 // stage_kernel.cuh -- fused finite-volume stage for sm_100a.
 //
 // One CTA owns a TX x TY column of cells of one brick and marches it along z
-// over [z0, z1).  Per z plane it
-//   1. brings the next plane's primitives into a 3-plane ring in shared memory
-//      (cons->prim on load for a conserved input) and the x / y halo of the
-//      current plane, with the boundary conditions applied as index maps,
-//   2. computes the limited slopes of x / y (current plane) and z (next plane),
-//   3. computes the Riemann fluxes of every x, y face of the plane and of the
-//      next z face (each face once),
+// over [z0, z1).  Per z plane k it
+//   1. moves plane k into the plane buffer (the own cells from a ring of own
+//      column values, the x / y halo from a halo buffer) and starts
+//      asynchronous copies (cp.async) of the halo of plane k+1 and of the own
+//      column's plane k+2, with the boundary conditions applied as index maps,
+//   2. computes the limited x / y slopes of the tile's cells (those of the
+//      halo cells were formed during plane k-1), then finishes the copies in
+//      place (cons->prim for a conserved input, reversed velocities),
+//   3. computes the Riemann fluxes of every x, y face of the plane (each face
+//      once), the halo cells' slopes of plane k+1, and the z slope and z face
+//      k+1 of every own column,
 //   4. forms the divergence increment of every cell in the reference's order
 //      (x, then y, then z contributions) and applies the RK stage epilogue.
 // This replaces the ~40 full-array sweeps per direction of
@@ -403,8 +407,8 @@ struct StageLayout {
   // tile's own cells only
   static constexpr bool HS = !PARAB;
   static constexpr int kNHS = 2 * TX + 2 * TYt;  // halo slopes of a plane
-  static constexpr int kSx = HS ? 5 * NT : 5 * TY * (TX + 2);
-  static constexpr int kSy = HS ? 5 * NT : 5 * (TY + 2) * TX;
+  static constexpr int kSx = HS ? 5 * NT : 0;  // x slopes of the tile's cells
+  static constexpr int kSy = HS ? 5 * NT : 0;  // y slopes
   static constexpr int kFx = NF * TY * (TX + 1);
   static constexpr int kFy = NF * (TY + 1) * TX;
   static constexpr int kGx = G_NTAB * (TX + 4);
