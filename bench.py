@@ -241,7 +241,7 @@ def pipe_use(kernel):
     ncu capture: what bounds it instead of HBM."""
     p = _stage_profile(kernel)
     return {"fp64_pipe_active": p.get("fp64_pipe_active"), "issue_active": p.get("issue_active"),
-            "source": "profiles/stage_kernel_sine160.md (ncu, 160^3)"}
+            "source": "profiles/stage_traffic.json (ncu, 160^3)"}
 
 
 def run_ours(args):

@@ -16,7 +16,7 @@
 //      (x, then y, then z contributions) and applies the RK stage epilogue.
 // This replaces the ~40 full-array sweeps per direction of
 // IncrementDivergence_FV % Compute (IncrementDivergence_FV__Form.f90:344-412)
-// and the Copy / MultiplyAdd / ComputeFromConserved sweeps of the RK driver
+// and the Copy / MultiplyAdd / ComputeFromConserved sweeps of the RK stepper
 // (Step_RK_C_ASC__Template.f90:761-1281) with one pass per stage.
 #pragma once
 

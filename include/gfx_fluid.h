@@ -7,7 +7,7 @@
  * Every entry point returns an int status (GFX_OK = 0, negative on error) and
  * never aborts; gfx_fluid_last_error() gives the message of the last failure
  * on the calling thread.  The Fortran side reaches these through
- * ISO_C_BINDING interfaces.
+ * ISO_C_BINDING interfaces (include/gfx_fluid_f.f90).
  *
  * Data layout (the reference's StorageForm % Value(nValues, nVariables),
  * Storage_Form.f90:30): one contiguous FP64 array per variable, x fastest,
@@ -35,7 +35,7 @@ enum gfx_status {
   GFX_OK = 0,
   GFX_ERR_ARGUMENT = -1,    /* bad pointer, size or configuration value */
   GFX_ERR_CUDA = -2,        /* a CUDA runtime call or kernel launch failed */
-  GFX_ERR_UNSUPPORTED = -3, /* option the reference has but this build does not */
+  GFX_ERR_UNSUPPORTED = -3, /* option the reference has but this library does not */
   GFX_ERR_STATE = -4,       /* non-finite or non-positive state detected */
   GFX_ERR_TIMEOUT = -5,     /* a bounded device-side wait expired */
   GFX_ERR_NO_MEMORY = -6    /* device or host allocation failed */

@@ -4,7 +4,7 @@ import numpy as np
 
 from oracle.oracle import Oracle
 
-# The parity bar of the north star: per step, per conserved field,
+# The parity bar: per step, per conserved field,
 # max |U_gpu - U_oracle| / max |U_oracle| <= 1e-12 over proper cells.
 PARITY_RTOL = 1e-12
 
