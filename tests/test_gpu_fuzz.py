@@ -53,3 +53,29 @@ def test_random_configuration_matches_oracle(i):
         box.step(dt)
         assert_parity(to_np(box.U), o.conserved(), cfg, "case %d step %d" % (i, n))
     box.close()
+
+
+@pytest.mark.parametrize("i", range(0, N_CASES, 2))
+def test_random_configuration_evolve_and_host_step_equal_the_steps(i):
+    """The evolve graph (stored primitives, fused CFL) and the pipelined host
+    step give the device steps' states bit for bit."""
+    import torch
+
+    from genasis_b200.fluid import FluidBox
+
+    cfg, prim = _case(i)
+    dev, evo, hst = FluidBox(cfg), FluidBox(cfg), FluidBox(cfg)
+    for box in (dev, evo, hst):
+        box.compute_from_primitive(prim)
+    host = dev.U.detach().cpu().pin_memory()
+    for n in range(4):
+        dt = dev.compute_time_step(n)
+        dev.step(dt)
+        hst.step_host(host, dt)
+    t, c = evo.evolve(1e300, 0.0, 0, max_cycles=4)
+    torch.cuda.synchronize()
+    assert c == 4
+    assert np.array_equal(to_np(evo.U), to_np(dev.U))
+    assert np.array_equal(host.numpy(), to_np(dev.U))
+    for box in (dev, evo, hst):
+        box.close()
