@@ -5,6 +5,8 @@ limiter parameters, states with and without jumps.  Each case takes three
 steps from identical inputs with the per-step parity bar, starting with the
 primitives kept at initialisation and continuing from the conserved state,
 as the reference's integrator does."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -79,3 +81,40 @@ def test_random_configuration_evolve_and_host_step_equal_the_steps(i):
     assert np.array_equal(host.numpy(), to_np(dev.U))
     for box in (dev, evo, hst):
         box.close()
+
+
+@pytest.mark.parametrize("b", range(4))
+def test_random_batches_equal_single_bricks(b):
+    """Batches of random LINEAR bricks of one Riemann solver, without
+    gravity and with common physical parameters (what a batch holds), evolve
+    bit for bit as the single bricks."""
+    import torch
+
+    from genasis_b200.batch import FluidBatch
+    from genasis_b200.fluid import FluidBox
+
+    cases = [_case(i) for i in range(N_CASES)]
+    solver = "HLLC" if b % 2 == 0 else "HLL"
+    picked = [(c, p) for c, p in cases
+              if c.riemann_solver == solver and c.reconstruction == "LINEAR"
+              and c.uniform_acceleration == 0.0][b // 2::2][:5]
+    assert len(picked) >= 3
+    # a batch shares its physical parameters
+    picked = [(dataclasses.replace(c, limiter_parameter=1.4, courant_factor=0.8), p)
+              for c, p in picked]
+    cfgs = [c for c, _ in picked]
+    prims = [p for _, p in picked]
+    batch = FluidBatch(cfgs)
+    batch.set_primitives(prims)
+    batch.evolve(n_cycles=4)
+    times, cycles = batch.clocks()
+    for k, (cfg, prim) in enumerate(picked):
+        box = FluidBox(cfg)
+        box.compute_from_primitive(prim)
+        t, c = box.evolve(1e300, 0.0, 0, max_cycles=4)
+        torch.cuda.synchronize()
+        assert c == cycles[k] == 4 and t == times[k]
+        p = (slice(None),) + cfg.proper
+        assert np.array_equal(to_np(batch.boxes[k].U)[p], to_np(box.U)[p]), k
+        box.close()
+    batch.close()
