@@ -279,24 +279,6 @@ __device__ __forceinline__ void finish_cell(const Phys& ph, double* dst, int str
   dst[4 * stride] = w.E;
 }
 
-// Reconstructed face states of the face between cells (im) and (ip) along one
-// axis, IncrementDivergence_FV__Kernel.f90:70-90: V_IL = V(i-1) + dXR(i-1) dVdX(i-1),
-// V_IR = V(i) - dXL(i) dVdX(i).
-template <int NF>
-__device__ __forceinline__ void face_states(const double* vm, const double* sm_, int stride_m,
-                                            const double* vp, const double* sp, int stride_p,
-                                            int sstride_m, int sstride_p, double wr, double wl,
-                                            const Phys& ph, FaceState& L, FaceState& R) {
-  double l[5], r[5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) {
-    l[v] = vm[v * stride_m] + wr * sm_[v * sstride_m];
-    r[v] = vp[v * stride_p] - wl * sp[v * sstride_p];
-  }
-  face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
-  face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
-}
-
 __device__ __forceinline__ bool df_bit(const BrickDesc& B, int d, int gx, int gy, int gz) {
   if (B.df == nullptr) return false;
   if (gx < 0 || gy < 0 || gz < 0 || gx >= B.n[0] || gy >= B.n[1] || gz >= B.n[2]) return false;
