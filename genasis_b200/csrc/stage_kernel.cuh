@@ -596,9 +596,9 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
     stage_prologue<IN_PRIM, HLLC, NF, PARAB, TYt>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx,
                                                   gy, z0, own, dt);
     // the halo cell of this thread (threads below NH): two rows below and
-    // above the tile, two columns left and right; hbuf holds it for the next
-    // plane (copied asynchronously from stored primitives where no boundary
-    // map reverses a velocity, loaded otherwise), starting with plane z0
+    // above the tile, two columns left and right; hbuf holds its primitives
+    // for the next plane (copied asynchronously, then finished in place),
+    // starting with plane z0
     int hx = 0, hy = 0;
     if (tid < 4 * TX) {
       const int s = tid / TX;
