@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="sine",
-                    choices=["sine", "bricks", "adjoint", "adjoint_step", "rt", "sod"],
+                    choices=["sine", "bricks", "adjoint", "adjoint_step", "rt", "sod", "chart"],
                     help="sine: the 256^3 headline; bricks: 512 uneven bricks, batched "
                          "launch against a loop of per-brick launches; adjoint: 128^3 "
                          "Kelvin-Helmholtz, adjoint against forward and finite differences")
@@ -56,8 +56,13 @@ def parse():
                     help="adjoint workload: finite-difference directions")
     ap.add_argument("--adjoint-steps", type=int, default=10,
                     help="rt workload: steps of the adjoint run at the end")
-    ap.add_argument("--full-crossing", action="store_true",
-                    help="sine workload: also run to t = 1 (one crossing) for the L1 error")
+    ap.add_argument("--no-full-crossing", action="store_true",
+                    help="sine workload: skip the run to t = 1 (one crossing) for the L1 error")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="sine workload: only the headline (no fast build, no per-step "
+                         "parity at full size, no C1 / C3 / C4 / C5 sub-objects)")
+    ap.add_argument("--variant", default="exact", choices=["exact", "fast"],
+                    help="library build of the headline (sine workload) or of the workload")
     ap.add_argument("--tile-rows", type=int, default=0,
                     help="sine workload: tile rows (8 or 16) instead of the autotuner's choice")
     ap.add_argument("--z-chunk", type=int, default=0,
@@ -244,32 +249,15 @@ def pipe_use(kernel):
             "source": "profiles/stage_traffic.json (ncu, 160^3)"}
 
 
-def run_ours(args):
+def _timed_evolve(box, steps, warmup, local, world):
+    """Warm-up cycles (they also capture the cycle graph), then `steps` cycles
+    of gfx_fluid_evolve timed with CUDA events on the launching stream between
+    barriers, with the clocks sampled meanwhile."""
     import torch
 
-    world, rank, local = dist_init()
-    from genasis_b200 import problems
-
-    cfg, prim = problems.sine_wave(args.n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
-    cells = cfg.n_proper
-    # tile and pencil from the autotuner's table (tuned here if absent), or
-    # as given on the command line
-    from genasis_b200 import autotune
-
-    if args.tile_rows or args.z_chunk:
-        from genasis_b200.fluid import FluidBox
-
-        box = FluidBox(cfg)
-        box.set_tuning(args.z_chunk, 0, args.tile_rows)
-    else:
-        box = autotune.tuned_box(cfg, adjoint=False)
-    box.compute_from_primitive(prim)
-    del prim
     stream = torch.cuda.current_stream()
-    # warm-up cycles (also captures the cycle graph)
-    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(args.warmup, 3))
+    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
     torch.cuda.synchronize()
-
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = box.kernel_launches()
@@ -278,38 +266,118 @@ def run_ours(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=args.steps)
+    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=steps)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop()
-    launches = box.kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms, world)
-    steps_done = cyc2 - cyc
-    value = replica_rate(cells, steps_done, ms, world)
+    return {"ms": ev0.elapsed_time(ev1), "steps": cyc2 - cyc, "t_sim": t_sim, "cycle": cyc2,
+            "launches": box.kernel_launches() - launches0, "clocks": clocks}
 
-    # L1 density error against the exact translated profile at the end of the timed
-    # region (before the extra steps below move the state on)
+
+def _sine_box(args, cfg, prim, variant):
+    """The 256^3 sine-wave brick of a library build, with the autotuner's tile
+    and pencil (or the command line's), initialised from prim."""
+    from genasis_b200 import autotune
+    from genasis_b200.fluid import FluidBox
+
+    if args.tile_rows or args.z_chunk:
+        box = FluidBox(cfg, variant=variant)
+        box.set_tuning(args.z_chunk, 0, args.tile_rows)
+    else:
+        box = autotune.tuned_box(cfg, adjoint=False, variant=variant)
+    box.compute_from_primitive(prim)
+    return box
+
+
+def _sine_l1(box, cfg, t):
+    from genasis_b200 import problems
+
     prim_t, _ = box.compute_from_conserved(primitive=True)
-    exact = problems.sine_density(cfg, t_sim)
-    l1 = problems.l1_error(prim_t[0].cpu().numpy(), exact, cfg)
+    l1 = problems.l1_error(prim_t[0].cpu().numpy(), problems.sine_density(cfg, t), cfg)
     del prim_t
-    crossing = None
-    if args.full_crossing:
-        # on to t = 1 (one box crossing), the last step cut to land on it
-        t_end, c_end = box.evolve(1.0, t_sim, cyc2)
-        torch.cuda.synchronize()
-        prim_t, _ = box.compute_from_conserved(primitive=True)
-        crossing = {"time": t_end, "cycles": c_end,
-                    "l1_density_error": problems.l1_error(
-                        prim_t[0].cpu().numpy(), problems.sine_density(cfg, t_end), cfg)}
-        del prim_t
+    return l1
 
-    # per-kernel device times of the fused stages (CUDA events per launch)
-    dt = box.compute_time_step(cyc2)
+
+def _oracle_sine(n, steps, warmup=1):
+    """The CPU oracle on the n^3 sine wave: `warmup` untimed steps, then
+    `steps` timed ones, all host threads; returns the rate, the seconds, the
+    threads, and the last timed step as (state before it, cycle, dt, state
+    after it) for the per-step parity of the GPU builds."""
+    from genasis_b200 import problems
+    from oracle.oracle import Oracle
+
+    cfg, prim = problems.sine_wave(n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    i = 0
+    for _ in range(warmup):
+        o.step(o.timestep(i))
+        i += 1
+    el = 0.0
+    before = None
+    for k in range(steps):
+        dt = o.timestep(i)
+        if k == steps - 1:
+            before = (o.conserved(), i, dt)
+        t0 = time.perf_counter()
+        o.step(dt)
+        el += time.perf_counter() - t0
+        i += 1
+    return n ** 3 * steps / el, el, Oracle.n_threads(), before + (o.conserved(),)
+
+
+def _field_errors(a, b, idx):
+    """max |a - b| per field over idx, relative to the field's max |b|."""
+    import numpy as np
+
+    return [float(np.abs(a[f][idx] - b[f][idx]).max()) /
+            max(float(np.abs(b[f][idx]).max()), 1e-300) for f in range(a.shape[0])]
+
+
+def _quantity_errors(a, b, idx):
+    """As _field_errors, with each momentum component relative to the largest
+    momentum component's max (the momentum vector's scale)."""
+    import numpy as np
+
+    scale = [max(float(np.abs(b[f][idx]).max()), 1e-300) for f in range(b.shape[0])]
+    scale[1:4] = [max(scale[1:4])] * 3
+    return [float(np.abs(a[f][idx] - b[f][idx]).max()) / scale[f] for f in range(a.shape[0])]
+
+
+def _step_parity(box, cfg, before):
+    """One GPU step from the oracle's state before its last timed step (the
+    same dt, features detected from that state) against the oracle's result:
+    errors per field (relative to the field's max) and per quantity
+    (momentum components relative to the momentum vector's max), and the
+    CFL time step of the state against the oracle's."""
+    import numpy as np
+    import torch
+
+    U_prev, cycle, dt, U_next = before
+    box.set_conserved(torch.as_tensor(U_prev, device="cuda"))
+    box.detect_features()
+    dt_g = box.compute_time_step(cycle)
+    box.step(dt)
+    g = box.U.cpu().numpy()
+    p = cfg.proper
+    fe = _field_errors(g, U_next, p)
+    qe = _quantity_errors(g, U_next, p)
+    bitwise = [bool(np.array_equal(g[f][p], U_next[f][p])) for f in range(6)]
+    del g
+    return {"max_rel_err_per_field": fe, "max_rel_err_per_quantity": qe,
+            "max_rel_err": max(fe), "within_1e-12": max(fe) <= 1e-12,
+            "bitwise_equal_fields": bitwise, "dt_rel_diff": abs(dt_g - dt) / dt,
+            "dt_equal": dt_g == dt}
+
+
+def _stage_timing(box, cfg, cyc, steps):
+    """Per-kernel device times of an evolve cycle's kernels (CUDA events per
+    launch, gfx_fluid_step_timed) and the roofline of the dominant stage."""
+    cells = cfg.n_proper
+    dt = box.compute_time_step(cyc)
     per = {"features": [], "stage1": [], "stage2": [], "ghosts": []}
-    for _ in range(min(args.steps, 10)):
+    for _ in range(min(steps, 10)):
         f, s1, s2, gh = box.step_timed(dt)
         per["features"].append(f)
         per["stage1"].append(s1)
@@ -319,16 +387,34 @@ def run_ours(args):
     dom = max(("stage1", "stage2"), key=lambda k: avg[k])
     peak, peak_kind = peaks()
     achieved = STAGE_BYTES[dom] * cells / (avg[dom] / 1000.0) / 1e9
-    traffic = traffic_per_launch(dom, cells)
-    roofline = {"bound": "hbm", "kernel": "stage_kernel (%s)" % dom, "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                "peak_source": peak_kind,
-                "algorithmic_bytes_per_cell": STAGE_BYTES[dom],
-                "avg_launch_ms": avg[dom],
-                "kernel_ms": avg,
-                "step_hbm_frac": STEP_BYTES * value / world / 1e9 / peak,
-                "ncu_pipes": pipe_use(dom)}
+    return dt, avg, dom, {
+        "bound": "hbm", "kernel": "stage_kernel (%s)" % dom, "achieved": achieved,
+        "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": traffic_per_launch(dom, cells), "peak_source": peak_kind,
+        "algorithmic_bytes_per_cell": STAGE_BYTES[dom], "avg_launch_ms": avg[dom],
+        "kernel_ms": avg}
 
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_init()
+    from genasis_b200 import problems
+
+    cfg, prim = problems.sine_wave(args.n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
+    cells = cfg.n_proper
+    box = _sine_box(args, cfg, prim, args.variant)
+    t = _timed_evolve(box, args.steps, args.warmup, local, world)
+    ms, steps_done, t_sim, cyc2 = t["ms"], t["steps"], t["t_sim"], t["cycle"]
+    ms_max = max_over_ranks(ms, world)
+    value = replica_rate(cells, steps_done, ms, world)
+    # L1 density error against the exact translated profile at the end of the
+    # timed region (before the extra steps below move the state on)
+    l1 = _sine_l1(box, cfg, t_sim)
+
+    dt, avg, dom, roofline = _stage_timing(box, cfg, cyc2, args.steps)
+    roofline["step_hbm_frac"] = STEP_BYTES * value / world / 1e9 / roofline["peak"]
+    roofline["ncu_pipes"] = pipe_use(dom)
 
     # end to end: H2D of the state from pinned host memory, the step, D2H
     e2e = None
@@ -349,13 +435,73 @@ def run_ours(args):
         e2e = {"value": world * cells * n_e / el, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": nbytes, "steps": n_e,
                "how": "gfx_fluid_step_host on a pinned host state, pipelined over z slabs"}
+        del host
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, el, cores = cpu_step_rate(args.n, 2, warmup=1)
+    single = rank == 0 and world == 1
+    extras = single and not args.no_extras
+    crossing = None
+    if extras and not args.no_full_crossing:
+        # on to t = 1 (one box crossing), the last step cut to land on it
+        box.compute_from_primitive(prim)
+        t_end, c_end = box.evolve(1.0, 0.0, 0)
+        torch.cuda.synchronize()
+        crossing = {"time": t_end, "cycles": c_end, "l1_density_error": _sine_l1(box, cfg, t_end),
+                    "norm": "sum |rho - rho_exact| / sum |rho_exact| over proper cells"}
+
+    cpu = parity = None
+    if single and not args.no_cpu_baseline:
+        rate, el, cores, before = _oracle_sine(args.n, 2, warmup=1)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "2 RK2 steps (after 1 warm-up) of the %d^3 sine-wave workload on the "
-                         "CPU oracle, %.1f s" % (args.n, el)}
+                         "CPU oracle (the C restatement, -O3 -ffp-contract=off; not GenASiS's "
+                         "Fortran), %.1f s" % (args.n, el)}
+        parity = {"workload": "sine_wave_%d" % args.n,
+                  "how": "one GPU step from the oracle's state before its last timed step, "
+                         "same dt, against the oracle's result, proper cells",
+                  args.variant: _step_parity(box, cfg, before)}
+    box.close()
+    del box
+    torch.cuda.empty_cache()
+
+    fast = None
+    if extras:
+        other = "fast" if args.variant == "exact" else "exact"
+        fb = _sine_box(args, cfg, prim, other)
+        tf = _timed_evolve(fb, args.steps, args.warmup, local, world)
+        vf = cells * tf["steps"] / (tf["ms"] / 1000.0)
+        l1_f = _sine_l1(fb, cfg, tf["t_sim"])  # before the timed steps below move it on
+        _, avg_f, dom_f, roof_f = _stage_timing(fb, cfg, tf["cycle"], args.steps)
+        fast = {"variant": other, "library": "genasis_b200/" + (
+                    "libgfx_fluid_fast.so" if other == "fast" else "libgfx_fluid.so"),
+                "value": vf, "unit": UNIT, "ms_per_step": tf["ms"] / tf["steps"],
+                "steps": tf["steps"], "roofline": roof_f,
+                "step_hbm_frac": STEP_BYTES * vf / 1e9 / roof_f["peak"],
+                "clocks": tf["clocks"], "gpu_launches": tf["launches"],
+                "l1_density_error": l1_f}
+        if parity is not None:
+            parity[other] = _step_parity(fb, cfg, before)
+        fb.close()
+        del fb
+        torch.cuda.empty_cache()
+    del prim
+
+    configs = None
+    if extras:
+        configs = {}
+        v = args.variant
+        for key, fn in (("c1_sod", lambda: sod_result(128, 100, v)),
+                        ("c3_bricks", lambda: bricks_result(50, 3, 512, v)),
+                        ("c4_adjoint", lambda: adjoint_result(128, 64, 3, True, v)),
+                        ("c5_rt", lambda: rt_result(200, 3, 10, v)),
+                        ("chart_2x2x2", lambda: chart_result(args.n, (2, 2, 2), args.steps,
+                                                             args.warmup, v))):
+            t0 = time.perf_counter()
+            try:
+                configs[key] = fn()
+            except Exception as e:  # noqa: BLE001 -- reported, the headline stands
+                configs[key] = {"error": "%s: %s" % (type(e).__name__, e)}
+            configs[key]["wall_s"] = time.perf_counter() - t0
+            torch.cuda.empty_cache()
 
     if rank == 0:
         line = {
@@ -367,42 +513,55 @@ def run_ours(args):
             "config": {"workload": "sine_wave_%d" % args.n, "cells": cells, "riemann": "HLLC",
                        "reconstruction": "PLM theta 1.4", "boundary": "periodic",
                        "cfl": 0.8, "rk": 2, "parallelism": "replicas" if world > 1 else "single",
+                       "library": args.variant,
                        "l2": "inputs larger than L2 (state %.0f MB)" % (
-                           6 * box.n_values * 8 / 1e6),
+                           6 * (args.n + 4) ** 3 * 8 / 1e6),
                        "l1_density_error": l1, "sim_time": t_sim,
                        "full_crossing": crossing,
-                       "tuning": {"z_chunk": box.tuning[0], "tile": "32x%d" % box.tuning[2]}},
+                       "tuning": _tuning_of(args, cfg)},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": launches,
-            "clocks": clocks,
+            "gpu_launches": t["launches"],
+            "clocks": t["clocks"],
+            "parity": parity,
+            "fast_build": fast,
+            "configs": configs,
         }
         print(json.dumps(line), flush=True)
-    box.close()
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
 
 
-def run_bricks(args):
+def _tuning_of(args, cfg):
+    from genasis_b200 import autotune
+
+    if args.tile_rows or args.z_chunk:
+        return {"z_chunk": args.z_chunk, "tile": "32x%d" % (args.tile_rows or 16)}
+    e = autotune.load_cache().get(autotune.brick_key(cfg, args.variant), {})
+    return {"z_chunk": e.get("z_chunk"), "tile": "32x%s" % e.get("tile_rows")}
+
+
+def bricks_result(steps=50, warmup=3, n_bricks=512, variant="exact"):
     """512 independent bricks, edges U{16..96} per axis (seeded), seeded
     two-state Riemann problems, outflow, PLM + HLL, RK2, CFL 0.8: K cycles of
     the batched path (one persistent launch per stage, one graph per cycle)
-    against K cycles of each brick's own single-brick path, brick after brick."""
+    against K cycles of each brick's own single-brick path, brick after brick,
+    each timed with CUDA events."""
     import torch
 
     from genasis_b200 import problems
     from genasis_b200.batch import FluidBatch
 
     torch.cuda.set_device(0)
-    bricks = problems.random_bricks(count=args.bricks, seed=20261203, riemann_solver="HLL")
+    bricks = problems.random_bricks(count=n_bricks, seed=20261203, riemann_solver="HLL")
     cfgs = [c for c, _ in bricks]
     prims = [p for _, p in bricks]
     cells = sum(c.n_proper for c in cfgs)
-    batch = FluidBatch(cfgs)
-    K = args.steps
+    batch = FluidBatch(cfgs, variant=variant)
+    K = steps
     # the pencil length of the batch's work items: autotuned (cached per GPU
     # and brick set), outside the timed region
     from genasis_b200 import autotune
@@ -412,16 +571,18 @@ def run_bricks(args):
     t_tune = time.perf_counter() - t_tune
     # warm-up (graph capture) on a copy of the initial states, then reset
     batch.set_primitives(prims)
-    batch.evolve(n_cycles=max(args.warmup, 3))
+    batch.evolve(n_cycles=max(warmup, 3))
     torch.cuda.synchronize()
     batch.set_primitives(prims)
     batch.set_clocks(0.0, 0)
     torch.cuda.synchronize()
     l0 = batch.kernel_launches()
-    t0 = time.perf_counter()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
     batch.evolve(n_cycles=K)
+    e[1].record()
     torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
+    t_batch = e[0].elapsed_time(e[1]) / 1000.0
     launches_batch = batch.kernel_launches() - l0
     U_batch = [b.U.clone() for b in batch.boxes]
     # the same bricks through the single-brick path, one after another
@@ -432,20 +593,24 @@ def run_bricks(args):
         b.compute_from_primitive(p)
     torch.cuda.synchronize()
     l1 = sum(b.kernel_launches() for b in batch.boxes)
-    t0 = time.perf_counter()
+    e[2].record()
     for b in batch.boxes:
         b.evolve(1e300, 0.0, 0, max_cycles=K)
+    e[3].record()
     torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
+    t_plain = e[2].elapsed_time(e[3]) / 1000.0
     launches_plain = sum(b.kernel_launches() for b in batch.boxes) - l1
     same = all(torch.equal(a, b.U) for a, b in zip(U_batch, batch.boxes))
     line = {
         "metric": "FP64 cell-updates/s (batched bricks)", "value": cells * K / t_batch,
-        "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(args.warmup, 3),
+        "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(warmup, 3),
         "ms_per_step": 1000.0 * t_batch / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "bricks_%d" % args.bricks, "cells": cells, "riemann": "HLL",
-                   "boundary": "outflow", "cfl": 0.8, "edges": "U{16..96}", "seed": 20261203},
+        "config": {"workload": "bricks_%d" % n_bricks, "cells": cells, "riemann": "HLL",
+                   "boundary": "outflow", "cfl": 0.8, "edges": "U{16..96}", "seed": 20261203,
+                   "library": variant,
+                   "plain_loop": "each brick's own gfx_fluid_evolve (a graph per cycle), "
+                                 "brick after brick"},
         "plain_loop": {"value": cells * K / t_plain, "ms_per_step": 1000.0 * t_plain / K,
                        "gpu_launches": launches_plain},
         "speedup_vs_plain_loop": t_plain / t_batch,
@@ -455,8 +620,8 @@ def run_bricks(args):
         "bitwise_equal_to_plain": same,
         "gpu_launches": launches_batch,
     }
-    print(json.dumps(line), flush=True)
     batch.close()
+    return line
 
 
 def stage_roofline(box, cells, dt, n):
@@ -519,13 +684,12 @@ def run_adjoint_step(args):
     box.close()
 
 
-def run_sod(args):
-    """The plain method at its small configuration: the 3-D Sod tube on 128^3
+def sod_result(n=128, steps=100, variant="exact"):
+    """The plain method at its small configuration: the 3-D Sod tube on n^3
     cells (left rho = 1, p = 1; right rho = 0.125, p = 0.1; diaphragm x = 0.5),
-    PLM + HLL, RK2, CFL 0.8, outflow, --steps steps (100) on the GPU and on
+    PLM + HLL, RK2, CFL 0.8, outflow, `steps` steps (100) on the GPU and on
     the oracle side by side: per-step parity from identical inputs on the
-    first steps, the final states of the two free runs, the totals against
-    the boundary fluence, and both rates."""
+    first steps, the final states of the two free runs, and both rates."""
     import numpy as np
     import torch
 
@@ -535,13 +699,12 @@ def run_sod(args):
     from oracle.oracle import Oracle
 
     torch.cuda.set_device(0)
-    n = args.n if args.n != 256 else 128
     cfg = FluidConfig(n_cells=(n, n, n), riemann_solver="HLL", courant_factor=0.8,
                       n_ramp_cycles=1)
     prim = problems.riemann(cfg, 1.0, 1.0, (0, 0, 0), 0.125, 0.1, (0, 0, 0), (0.5, 0, 0),
                             (1.0, 0, 0))
     p = cfg.proper
-    box = FluidBox(cfg)
+    box = FluidBox(cfg, variant=variant)
     box.compute_from_primitive(prim)
     o = Oracle(cfg)
     o.set_primitive(prim)
@@ -554,7 +717,7 @@ def run_sod(args):
     gpu_ms = 0.0
     cpu_s = 0.0
     dts = []
-    for i in range(args.steps):
+    for i in range(steps):
         dt = o.timestep(i)
         dts.append(dt)
         if i < 3:  # per-step parity: the GPU step from the oracle's state
@@ -575,24 +738,27 @@ def run_sod(args):
     Ug = box.U.cpu().numpy()
     Uo = o.conserved()
     line = {
-        "workload": "sod_%d_hll_%d_steps" % (n, args.steps), "cells": cfg.n_proper,
+        "workload": "sod_%d_hll_%d_steps" % (n, steps), "cells": cfg.n_proper,
+        "library": variant,
         "per_step_max_rel_diff_first_3_steps": per_step,
         "final_max_rel_diff_free_runs": rel(Ug, Uo),
         "final_bitwise_equal_fields": [bool(np.array_equal(Ug[f][p], Uo[f][p])) for f in range(6)],
-        "gpu_cell_updates_per_s": cfg.n_proper * args.steps / (gpu_ms / 1000.0),
-        "cpu_oracle_cell_updates_per_s": cfg.n_proper * args.steps / cpu_s,
+        "gpu_cell_updates_per_s": cfg.n_proper * steps / (gpu_ms / 1000.0),
+        "gpu_timing": "CUDA events around each gfx_fluid_step (a host synchronisation per "
+                      "step for the oracle's dt)",
+        "cpu_oracle_cell_updates_per_s": cfg.n_proper * steps / cpu_s,
         "cpu_threads": Oracle.n_threads(), "sim_time": float(sum(dts)),
     }
-    print(json.dumps(line), flush=True)
     box.close()
+    return line
 
 
-def run_rt(args):
+def rt_result(steps=200, warmup=3, adjoint_steps=10, variant="exact"):
     """3-D Rayleigh-Taylor on 384 x 384 x 768 cells ([0,0.5]^2 x [0,1]),
     gravity 0.1 along -z as a source in the RK stages, periodic x / y,
-    reflecting z, PLM + HLLC, RK2, CFL 0.8: throughput over --steps cycles
+    reflecting z, PLM + HLLC, RK2, CFL 0.8: throughput over `steps` cycles
     with the HBM roofline of the stage kernel and the mass balance, then the
-    adjoint of the last --adjoint-steps steps (per-step checkpoints, stage
+    adjoint of the last `adjoint_steps` steps (per-step checkpoints, stage
     recomputation) against the forward time of the same steps."""
     import torch
 
@@ -603,34 +769,34 @@ def run_rt(args):
     cfg, prim = problems.rayleigh_taylor()
     cells = cfg.n_proper
 
-    box = autotune.tuned_box(cfg, adjoint=False)
+    box = autotune.tuned_box(cfg, adjoint=False, variant=variant)
     box.compute_from_primitive(prim)
     del prim
     dv = cell_volumes(box)
     p = cfg.proper
     mass0 = float((box.U[0][p] * dv[p]).sum())
-    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(args.warmup, 3))
+    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
     torch.cuda.synchronize()
     sampler = ClockSampler(0)
     sampler.start()
     l0 = box.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=args.steps)
+    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=steps)
     e1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = box.kernel_launches() - l0
     ms = e0.elapsed_time(e1)
-    steps = cyc2 - cyc
+    n_done = cyc2 - cyc
     mass1 = float((box.U[0][p] * dv[p]).sum())
     dt = box.compute_time_step(cyc2)
     roof = stage_roofline(box, cells, dt, 5)
     adj = None
-    if args.adjoint_steps > 0:
+    if adjoint_steps > 0:
         U0 = box.U.clone()
         dts = []
-        for i in range(args.adjoint_steps):
+        for i in range(adjoint_steps):
             dts.append(box.compute_time_step(cyc2 + i))
             box.step(dts[-1])
         # an untimed forward first: its checkpoints take their memory from the
@@ -652,21 +818,66 @@ def run_rt(args):
                "adjoint_over_forward": e[1].elapsed_time(e[2]) / e[0].elapsed_time(e[1]),
                "objective": "sum rho^2 dV", "gradient_finite": bool(torch.isfinite(grad).all())}
         del cps, grad, final, lam, U0
-    value = cells * steps / (ms / 1000.0)
+    value = cells * n_done / (ms / 1000.0)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": ms / steps, "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": n_done,
+        "warmup": max(warmup, 3), "ms_per_step": ms / n_done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "rayleigh_taylor_384x384x768", "cells": cells,
                    "riemann": "HLLC", "gravity": 0.1, "boundary": "periodic x/y, reflecting z",
-                   "cfl": 0.8, "sim_time": t_sim,
+                   "cfl": 0.8, "sim_time": t_sim, "library": variant,
                    "l2": "inputs larger than L2 (state %.1f GB)" % (6 * box.n_values * 8 / 1e9),
                    "mass_rel_change": (mass1 - mass0) / mass0},
         "roofline": roof, "step_hbm_frac": STEP_BYTES * value / 1e9 / roof["peak"],
         "adjoint": adj, "gpu_launches": launches, "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
     box.close()
+    return line
+
+
+def chart_result(n=256, n_bricks=(2, 2, 2), steps=20, warmup=3, variant="exact"):
+    """The sine-wave workload on n^3 cells as a chart of n_bricks bricks
+    (Chart_SLD's decomposition, all bricks on this device): cycles of the
+    chart's evolve timed with CUDA events, and the final state against the
+    single n^3 brick after the same cycles (bit for bit)."""
+    import numpy as np
+    import torch
+
+    from genasis_b200 import problems
+    from genasis_b200.chart import FluidChart
+    from genasis_b200.fluid import FluidBox
+
+    torch.cuda.set_device(0)
+    cfg, prim = problems.sine_wave(n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
+    chart = FluidChart(cfg, n_bricks, variant=variant)
+    chart.from_primitive(prim)
+    t_sim, cyc = chart.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
+    l0 = chart.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    t_sim, cyc2 = chart.evolve(1e30, t_sim, cyc, max_cycles=steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = chart.kernel_launches() - l0
+    got = chart.gather()
+    chart.close()
+    del chart
+    torch.cuda.empty_cache()
+    box = FluidBox(cfg, variant=variant)
+    box.compute_from_primitive(prim)
+    t_b, c_b = box.evolve(1e30, 0.0, 0, max_cycles=cyc2)
+    ref = box.U.cpu().numpy()
+    box.close()
+    p = cfg.proper
+    same = [bool(np.array_equal(got[f][p], ref[f][p])) for f in range(6)]
+    return {"workload": "sine_wave_%d_chart_%dx%dx%d" % ((n,) + tuple(n_bricks)),
+            "bricks": int(np.prod(n_bricks)), "brick_cells": [n // b for b in n_bricks],
+            "library": variant, "value": cfg.n_proper * (cyc2 - cyc) / (ms / 1000.0),
+            "unit": UNIT, "steps": cyc2 - cyc, "ms_per_step": ms / (cyc2 - cyc),
+            "gpu_launches": launches, "cycles_compared": cyc2,
+            "bitwise_equal_to_single_brick": same, "time_equal": t_b == t_sim}
 
 
 def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=None):
@@ -698,7 +909,7 @@ def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=No
     return errs
 
 
-def run_adjoint_workload(args):
+def adjoint_result(n=128, directions=64, warmup=3, oracle_fd=True, variant="exact"):
     """128^3 periodic Kelvin-Helmholtz (density 2 / 1, shear +-0.5, vy =
     0.01 sin(4 pi x) + 1e-3 seeded noise, p = 2.5), PLM + HLLC, RK2, CFL 0.8,
     20 steps; J = sum rho^2 dV at the final time.  Times the forward run with
@@ -714,13 +925,13 @@ def run_adjoint_workload(args):
     from genasis_b200.fluid import FluidBox
 
     torch.cuda.set_device(0)
-    n, n_steps = args.n if args.n != 256 else 128, 20
+    n_steps = 20
     out = {}
-    for variant in ("spec", "noisy"):
+    for state in ("spec", "noisy"):
         cfg, prim = problems.kelvin_helmholtz(n)
-        if variant == "noisy":
+        if state == "noisy":
             prim = problems.noisy(prim, amp=2e-2, seed=20261205)
-        box = autotune.tuned_box(cfg)
+        box = autotune.tuned_box(cfg, variant=variant)
         box.compute_from_primitive(prim)
         box.compute_from_conserved()
         U0 = box.U.clone()
@@ -731,7 +942,7 @@ def run_adjoint_workload(args):
         dv = cell_volumes(box)
         launches0 = box.kernel_launches()
         fwd, adj, fwd_plain = [], [], []
-        for rep in range(max(args.warmup, 3) + 3):
+        for rep in range(max(warmup, 3) + 3):
             e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             torch.cuda.synchronize()
             e[0].record()
@@ -744,13 +955,13 @@ def run_adjoint_workload(args):
             run_forward(box, U0, dts, False, keep=False)
             e[3].record()
             torch.cuda.synchronize()
-            if rep >= max(args.warmup, 3):
+            if rep >= max(warmup, 3):
                 fwd.append(e[0].elapsed_time(e[1]))
                 adj.append(e[1].elapsed_time(e[2]))
                 fwd_plain.append(e[2].elapsed_time(e[3]))
             del cps
         launches = box.kernel_launches() - launches0
-        errs = _fd_check(box, cfg, U0, dts, grad, dv, args.directions, seed=20261205)
+        errs = _fd_check(box, cfg, U0, dts, grad, dv, directions, seed=20261205)
         errs_np = np.array(errs)
         entry = {
             "forward_ms": statistics.median(fwd), "adjoint_ms": statistics.median(adj),
@@ -760,7 +971,7 @@ def run_adjoint_workload(args):
             "fd_median_rel_err": float(np.median(errs_np)),
             "fd_max_rel_err": float(errs_np.max()),
         }
-        if variant == "noisy":
+        if state == "noisy":
             # the same check at larger eps: at eps = 1e-6 a unit direction over
             # all 6 x n^3 values moves each value by ~1e-10, close to the
             # rounding floor of the differenced states
@@ -771,14 +982,14 @@ def run_adjoint_workload(args):
                                      "median_rel_err": float(np.median(e_s)),
                                      "max_rel_err": float(e_s.max())}
             entry["fd_eps_sweep"] = sweep
-        if variant == "noisy" and not args.no_cpu_baseline:
+        if state == "noisy" and oracle_fd:
             # the reference-FD gradient: the oracle's step, on a 32^3 brick of
             # the same noisy state, 4 directions
             from oracle.oracle import Oracle
 
             cfg_s, prim_s = problems.kelvin_helmholtz(32)
             prim_s = problems.noisy(prim_s, amp=2e-2, seed=20261205)
-            bs = FluidBox(cfg_s)
+            bs = FluidBox(cfg_s, variant=variant)
             bs.compute_from_primitive(prim_s)
             bs.compute_from_conserved()
             U0s = bs.U.clone()
@@ -805,41 +1016,49 @@ def run_adjoint_workload(args):
                               rho_fn=rho_oracle)
             entry["oracle_fd_32cubed"] = {"directions": 4, "max_rel_err": max(e_ref)}
             bs.close()
-        out[variant] = entry
+        out[state] = entry
         box.close()
     spec = out["spec"]
     line = {
         "metric": "adjoint/forward cost", "value": spec["adjoint_over_forward"],
         "unit": "x (adjoint ms / forward ms)", "n_gpus": 1, "steps": n_steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": spec["adjoint_ms"] / n_steps,
+        "warmup": max(warmup, 3), "ms_per_step": spec["adjoint_ms"] / n_steps,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": "kelvin_helmholtz_%d_adjoint" % n, "riemann": "HLLC",
                    "boundary": "periodic", "cfl": 0.8, "steps": n_steps,
                    "objective": "sum rho^2 dV", "checkpointing": "per step",
-                   "fd_eps": 1e-6, "fd_seed": 20261205},
+                   "fd_eps": 1e-6, "fd_seed": 20261205, "library": variant},
         "spec_state": spec, "noisy_state": out["noisy"],
         "gpu_launches": launches,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "bricks":
-        run_bricks(args)
+        return
+    if args.workload == "sine":
+        run_ours(args)
+        return
+    n = args.n if args.n != 256 else 128
+    if args.workload == "bricks":
+        line = bricks_result(args.steps, args.warmup, args.bricks, args.variant)
     elif args.workload == "adjoint":
-        run_adjoint_workload(args)
+        line = adjoint_result(n, args.directions, args.warmup, not args.no_cpu_baseline,
+                              args.variant)
     elif args.workload == "adjoint_step":
         run_adjoint_step(args)
+        return
     elif args.workload == "sod":
-        run_sod(args)
-    elif args.workload == "rt":
-        run_rt(args)
+        line = sod_result(n, args.steps, args.variant)
+    elif args.workload == "chart":
+        line = chart_result(args.n, (2, 2, 2), args.steps, args.warmup, args.variant)
     else:
-        run_ours(args)
+        line = rt_result(args.steps, args.warmup, args.adjoint_steps, args.variant)
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

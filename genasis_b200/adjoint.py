@@ -25,7 +25,7 @@ def step_adjoint(box: FluidBox, U_n, dt, lam_np1, lam_n=None, U_np1=None,
     torch = _torch()
     if lam_n is None:
         lam_n = torch.empty_like(lam_np1)
-    lib.call("gfx_fluid_step_adjoint", box.h, _ptr(U_n.contiguous()), float(dt),
+    box.call("gfx_fluid_step_adjoint", box.h, _ptr(U_n.contiguous()), float(dt),
              _ptr(lam_np1.contiguous()), _ptr(lam_n), _ptr(U_np1), int(bool(detect_features)),
              _stream())
     return lam_n
@@ -36,7 +36,7 @@ def prepare_state(box: FluidBox, U0, detect_first):
     features of U0 (detect_first) or zero features (the first step after
     initialisation from primitives)."""
     box.U.copy_(U0)
-    lib.call("gfx_fluid_to_primitive", box.h, _ptr(box.U), None, None, _stream())
+    box.call("gfx_fluid_to_primitive", box.h, _ptr(box.U), None, None, _stream())
     if detect_first:
         box.detect_features()
     else:

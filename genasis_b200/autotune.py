@@ -62,16 +62,23 @@ def save_cache(cache):
     os.replace(tmp, path)
 
 
-def brick_key(cfg):
+def _variant_suffix(variant):
+    # the exact library's entries carry no suffix; the fast build is timed
+    # on its own (its kernels need fewer instructions and registers)
+    return "" if (variant or "exact") == "exact" else ":" + variant
+
+
+def brick_key(cfg, variant=None):
     edges = "x".join(str(16 * ((int(n) + 15) // 16)) for n in cfg.n_cells)
     grav = "g" if cfg.uniform_acceleration != 0.0 else "0"
-    return "brick:%s:%s:%s" % (edges, cfg.riemann_solver, grav)
+    return "brick:%s:%s:%s%s" % (edges, cfg.riemann_solver, grav, _variant_suffix(variant))
 
 
-def batch_key(cfgs):
+def batch_key(cfgs, variant=None):
     sizes = ",".join("x".join(str(int(n)) for n in c.n_cells) for c in cfgs)
     digest = hashlib.sha1(sizes.encode()).hexdigest()[:12]
-    return "batch:%d:%s:%s" % (len(cfgs), cfgs[0].riemann_solver, digest)
+    return "batch:%d:%s:%s%s" % (len(cfgs), cfgs[0].riemann_solver, digest,
+                                 _variant_suffix(variant))
 
 
 def _time(fn, reps):
@@ -87,14 +94,14 @@ def _time(fn, reps):
     return start.elapsed_time(end) / reps
 
 
-def tune_brick(cfg, reps=3, adjoint=True, seed=1):
+def tune_brick(cfg, reps=3, adjoint=True, seed=1, variant=None):
     """Times the step for every pencil length and (if adjoint) the adjoint
     step for every segment on a seeded state of cfg's size; returns
     {"z_chunk", "adjoint_segment", "ms": {...}}."""
     torch = _torch()
     from .adjoint import step_adjoint
 
-    box = FluidBox(cfg)
+    box = FluidBox(cfg, variant=variant)
     box.compute_from_primitive(problems.random_state(cfg, seed=seed, shocks=False))
     box.compute_from_conserved()
     U0 = box.U.clone()
@@ -129,14 +136,15 @@ def tune_brick(cfg, reps=3, adjoint=True, seed=1):
                    "adjoint": {str(k): v for k, v in ms_s.items()}}}
 
 
-def tuned_box(cfg, retune=False, adjoint=True):
-    """A FluidBox with the cached (or freshly tuned) knobs of cfg's bucket."""
+def tuned_box(cfg, retune=False, adjoint=True, variant=None):
+    """A FluidBox of the library variant with the cached (or freshly tuned)
+    knobs of cfg's bucket."""
     cache = load_cache()
-    key = brick_key(cfg)
+    key = brick_key(cfg, variant)
     if retune or "tile_rows" not in cache.get(key, {}):
-        cache[key] = tune_brick(cfg, adjoint=adjoint)
+        cache[key] = tune_brick(cfg, adjoint=adjoint, variant=variant)
         save_cache(cache)
-    box = FluidBox(cfg)
+    box = FluidBox(cfg, variant=variant)
     e = cache[key]
     box.set_tuning(e["z_chunk"], e["adjoint_segment"], e["tile_rows"])
     return box
@@ -149,7 +157,7 @@ def tune_batch(batch, prims, cycles=3, retune=False):
     caches them.  The bricks' states are reset from prims afterwards.
     Returns ((tile_rows, z_chunk), ms per cycle by candidate, from_cache)."""
     cache = load_cache()
-    key = batch_key([b.config for b in batch.boxes])
+    key = batch_key([b.config for b in batch.boxes], batch.variant)
     e = cache.get(key, {})
     if not retune and "tile_rows" in e:
         batch.set_pencil_length(e["z_chunk"], e["tile_rows"])

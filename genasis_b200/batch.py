@@ -14,9 +14,13 @@ from .fluid import FluidBox, _stream
 
 
 class FluidBatch:
-    def __init__(self, configs, device=None):
-        self.boxes = [FluidBox(c, device=device) for c in configs]
+    def __init__(self, configs, device=None, variant=None):
+        self.variant = variant or lib.default_variant()
+        self.boxes = [FluidBox(c, device=device, variant=self.variant) for c in configs]
         self.h = None
+
+    def _call(self, name, *args):
+        return lib.call(name, *args, variant=self.variant)
 
     def set_pencil_length(self, z_chunk, tile_rows=None):
         """The z length of the cell pencils of every brick's work items (0 =
@@ -26,7 +30,7 @@ class FluidBatch:
             _, seg, rows = getattr(b, "tuning", (0, 0, 0))
             b.set_tuning(z_chunk, seg, rows if tile_rows is None else tile_rows)
         if self.h is not None:
-            lib.load().gfx_fluid_batch_destroy(self.h)
+            lib.load(self.variant).gfx_fluid_batch_destroy(self.h)
             self.h = None
 
     def set_primitives(self, prims):
@@ -40,37 +44,37 @@ class FluidBatch:
         hs = (ctypes.c_void_p * n)(*[b.h.value for b in self.boxes])
         us = (ctypes.c_void_p * n)(*[b.U.data_ptr() for b in self.boxes])
         h = ctypes.c_void_p()
-        lib.call("gfx_fluid_batch_create", n, hs, us, ctypes.byref(h))
+        self._call("gfx_fluid_batch_create", n, hs, us, ctypes.byref(h))
         self.h = h
 
     def set_clocks(self, time=0.0, i_cycle=0):
         self._ensure()
-        lib.call("gfx_fluid_batch_set_clocks", self.h, float(time), int(i_cycle))
+        self._call("gfx_fluid_batch_set_clocks", self.h, float(time), int(i_cycle))
 
     def evolve(self, finish_time=1e300, n_cycles=1):
         """Advances every brick by its own CFL steps until finish_time or
         n_cycles more cycles (asynchronous on the current stream)."""
         self._ensure()
-        lib.call("gfx_fluid_batch_evolve", self.h, float(finish_time), int(n_cycles), _stream())
+        self._call("gfx_fluid_batch_evolve", self.h, float(finish_time), int(n_cycles), _stream())
 
     def clocks(self):
         self._ensure()
         n = len(self.boxes)
         t = np.zeros(n)
         c = np.zeros(n, dtype=np.int32)
-        lib.call("gfx_fluid_batch_clocks", self.h, t.ctypes.data_as(ctypes.c_void_p),
+        self._call("gfx_fluid_batch_clocks", self.h, t.ctypes.data_as(ctypes.c_void_p),
                  c.ctypes.data_as(ctypes.c_void_p), _stream())
         return t, c
 
     def kernel_launches(self):
         self._ensure()
         n = ctypes.c_longlong()
-        lib.call("gfx_fluid_batch_kernel_launches", self.h, ctypes.byref(n))
+        self._call("gfx_fluid_batch_kernel_launches", self.h, ctypes.byref(n))
         return int(n.value)
 
     def close(self):
         if self.h is not None:
-            lib.load().gfx_fluid_batch_destroy(self.h)
+            lib.load(self.variant).gfx_fluid_batch_destroy(self.h)
             self.h = None
         for b in self.boxes:
             b.close()

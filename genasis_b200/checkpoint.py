@@ -34,5 +34,5 @@ def load(path, device=None):
     box = FluidBox(cfg, device=device)
     torch = _torch()
     box.U.copy_(torch.as_tensor(z["U"], dtype=torch.float64))
-    lib.call("gfx_fluid_resume", box.h, _ptr(box.U))
+    box.call("gfx_fluid_resume", box.h, _ptr(box.U))
     return box, float(z["time"]), int(z["i_cycle"])

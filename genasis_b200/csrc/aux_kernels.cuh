@@ -237,7 +237,7 @@ __device__ __forceinline__ void cell_p_v(const Box& b, const Phys& ph, const dou
   } else {
     const long long o = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
     Cons u{U[o], U[b.nV + o], U[2 * b.nV + o], U[3 * b.nV + o], U[4 * b.nV + o]};
-    cons_to_prim(u, w, ph.nmin);
+    cons_to_prim_exact(u, w, ph.nmin);
   }
   P = ph.gm1 * w.E;
   v[0] = w.V1;
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kDetThreads, 3)
       } else {
         Cons u{raw[0], raw[1], raw[2], raw[3], raw[4]};
         Prim w;
-        cons_to_prim(u, w, ph.nmin);
+        cons_to_prim_exact(u, w, ph.nmin);
         P = ph.gm1 * w.E;
         V1 = w.V1;
         V2 = w.V2;

@@ -1,0 +1,275 @@
+// chart_kernels.cuh -- the kernels of a chart of several bricks on one GPU
+// besides the fused stages: the initial state with the exchanged ghost
+// primitives, shock features across brick faces with ClearBoundary on the
+// chart's own boundary only, and the ghost values at the end of a step.
+//
+// The reference splits a chart into equal bricks, one per MPI rank
+// (Chart_SLD, Chart_Template.f90:440-460), and exchanges the ghost layers of
+// the faces and edges between them (Chart_SLD__Form.f90:131-201, 324-1097).
+// Here every brick of the chart lives in the same device memory, so no ghost
+// is copied: a value outside a brick is read where it lives, in the proper
+// cells of the brick across the face.  A brick's faces are either linked (to
+// the neighbouring brick inside the chart, or across a periodic boundary of
+// the chart to the brick at the other end) or carry the chart's boundary
+// condition (OUTFLOW, REFLECTING).
+#pragma once
+
+#include "aux_kernels.cuh"
+
+namespace gfx {
+
+struct ChartBrick {
+  Box box;              // bc: BC_NEIGHBOR on faces inside the chart
+  int nb[3][2];         // the linked brick across each face (-1: none)
+  double* U;            // conserved state, ghost layout
+  const double* prim;   // initial primitives, ghost layout (chart_from_primitive)
+  double* Pst;          // the kept primitives of the proper cells, compact
+  const double* wn;     // primitives the last stage 2 stored, compact
+  uint8_t* sb;          // shock bits, compact
+  uint8_t* df;          // DIFFUSIVE_FLUX_I bits, compact
+  long long v_off;      // prefix sum of nV over the bricks
+  long long c_off;      // prefix sum of nP
+};
+
+__device__ __forceinline__ int chart_find(const ChartBrick* cb, int n, long long x, bool cells) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long off = cells ? cb[mid].c_off : cb[mid].v_off;
+    if (off <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The brick holding proper coordinates c of brick b (possibly outside it),
+// crossing linked faces one axis after the other (an edge lands in the
+// diagonal brick); c is moved into that brick's frame.  Axes whose face is
+// not linked are left outside.
+__device__ __forceinline__ int chart_owner(const ChartBrick* cb, int b, int* c) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int side = c[a] < 0 ? 0 : (c[a] >= cb[b].box.n[a] ? 1 : -1);
+    if (side >= 0 && cb[b].nb[a][side] >= 0) {
+      const int o = cb[b].nb[a][side];
+      c[a] += side ? -cb[b].box.n[a] : cb[o].box.n[a];
+      b = o;
+    }
+  }
+  return b;
+}
+
+__device__ __forceinline__ bool chart_inside(const Box& bx, const int* c) {
+  return c[0] >= 0 && c[1] >= 0 && c[2] >= 0 && c[0] < bx.n[0] && c[1] < bx.n[1] &&
+         c[2] < bx.n[2];
+}
+
+// A ghost value is written by the exchange when every axis on which it is a
+// ghost is linked and it is not a corner (the faces and edges of
+// Chart_SLD__Form.f90:131-201); on one brick with periodic axes this is the
+// rule of the single-brick ghost refresh.
+__device__ __forceinline__ bool chart_reachable(const ChartBrick& B, const int* p) {
+  int nghost = 0;
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const bool lo = p[d] < 0, hi = p[d] >= B.box.n[d];
+    nghost += lo || hi;
+    if ((lo && B.nb[d][0] < 0) || (hi && B.nb[d][1] < 0)) ok = false;
+  }
+  return ok && nghost > 0 && nghost < 3;
+}
+
+__device__ __forceinline__ long long ghost_index(const Box& bx, const int* p) {
+  return (p[0] + 2) + (long long)bx.m[0] * ((p[1] + 2) + (long long)bx.m[1] * (p[2] + 2));
+}
+
+// ComputeFromPrimitive on every value of every brick after the exchange of
+// the primitives (Integrator_C_PS__Form.f90:194-203): an exchange-reachable
+// ghost takes the primitives of the cell it images; the primitives of the
+// proper cells are kept as the first step's state.
+__global__ void chart_from_primitive_kernel(const ChartBrick* __restrict__ cb, int n,
+                                            long long total, Phys ph) {
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = chart_find(cb, n, x, false);
+    const ChartBrick& B = cb[b];
+    const long long v = x - B.v_off, nV = B.box.nV;
+    int t[3];
+    decode3(v, B.box.m[0], B.box.m[1], t[0], t[1], t[2]);
+    int p[3] = {t[0] - 2, t[1] - 2, t[2] - 2};
+    const double* src = B.prim;
+    long long sv = v, snV = nV;
+    if (chart_reachable(B, p)) {
+      int c[3] = {p[0], p[1], p[2]};
+      const ChartBrick& S = cb[chart_owner(cb, b, c)];
+      src = S.prim;
+      sv = ghost_index(S.box, c);
+      snV = S.box.nV;
+    }
+    FaceState s;
+    face_state<6>(src[sv], src[snV + sv], src[2 * snV + sv], src[3 * snV + sv],
+                  src[4 * snV + sv], ph, s);
+    B.U[v] = s.D;
+    B.U[nV + v] = s.S1;
+    B.U[2 * nV + v] = s.S2;
+    B.U[3 * nV + v] = s.S3;
+    B.U[4 * nV + v] = s.G;
+    B.U[5 * nV + v] = s.DS;
+    if (chart_inside(B.box, p)) {
+      const long long c = p[0] + (long long)B.box.n[0] * (p[1] + (long long)B.box.n[1] * p[2]);
+      const long long nP = B.box.nP;
+      B.Pst[c] = s.N;
+      B.Pst[nP + c] = s.V1;
+      B.Pst[2 * nP + c] = s.V2;
+      B.Pst[3 * nP + c] = s.V3;
+      B.Pst[4 * nP + c] = s.E;
+    }
+  }
+}
+
+// Pressure and velocities of proper cell c of a brick (exact recovery from
+// the conserved state, or the stored primitives with PST).
+template <bool PST>
+__device__ __forceinline__ void chart_p_v(const ChartBrick& B, const Phys& ph, const int* c,
+                                          double& P, double* v) {
+  Prim w;
+  if (PST) {
+    const long long i = c[0] + (long long)B.box.n[0] * (c[1] + (long long)B.box.n[1] * c[2]);
+    const long long nP = B.box.nP;
+    w.E = B.wn[4 * nP + i];
+    w.V1 = B.wn[nP + i];
+    w.V2 = B.wn[2 * nP + i];
+    w.V3 = B.wn[3 * nP + i];
+  } else {
+    const long long o = ghost_index(B.box, c), nV = B.box.nV;
+    Cons u{B.U[o], B.U[nV + o], B.U[2 * nV + o], B.U[3 * nV + o], B.U[4 * nV + o]};
+    cons_to_prim_exact(u, w, ph.nmin);
+  }
+  P = ph.gm1 * w.E;
+  v[0] = w.V1;
+  v[1] = w.V2;
+  v[2] = w.V3;
+}
+
+// DetectShocks_CSL_Kernel (FluidFeatures_P__Kernel.f90:12-186) on the proper
+// cells of every brick: bit e of sb = shock along e between the cell and the
+// one below it, across a face inside the chart into the neighbouring brick
+// (the reference's ghost layer holds that cell); 0 on the chart's own
+// boundary, as on a single brick (no cell that keeps flags reads it).
+template <bool PST>
+__global__ void chart_detect_shock_kernel(const ChartBrick* __restrict__ cb, int n,
+                                          long long total, Phys ph, const int* skip) {
+  if (skip && *skip) return;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = chart_find(cb, n, x, true);
+    const ChartBrick& B = cb[b];
+    const long long c = x - B.c_off;
+    int t[3];
+    decode3(c, B.box.n[0], B.box.n[1], t[0], t[1], t[2]);
+    double P0, v0[3];
+    chart_p_v<PST>(B, ph, t, P0, v0);
+    uint8_t bits = 0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      int q[3] = {t[0], t[1], t[2]};
+      q[e] -= 1;
+      if (q[e] < 0 && B.box.bc[e][0] != BC_NEIGHBOR) continue;
+      const ChartBrick& S = cb[chart_owner(cb, b, q)];
+      double P1, v1[3];
+      chart_p_v<PST>(S, ph, q, P1, v1);
+      if (shock_between(P0, P1, v0[e] - v1[e], ph.shock_threshold)) bits |= (uint8_t)(1u << e);
+    }
+    B.sb[c] = bits;
+  }
+}
+
+// DIFFUSIVE_FLUX_I flags after ClearBoundary_CSL_Kernel (FluidFeatures_P__
+// Kernel.f90:189-313), which the reference applies on the faces of the
+// chart's boundary only (FluidFeatures_P__Form.f90:313-336: InnerBoundary =
+// iaBrick == 1, OuterBoundary = iaBrick == nBricks): a cell keeps flags
+// unless it is within one cell of a chart face, and flag d is set by a shock
+// along e != d at x, x + e_e, x - e_d or x + e_e - e_d, which may lie in the
+// neighbouring or the diagonal brick.
+__global__ void chart_detect_flags_kernel(const ChartBrick* __restrict__ cb, int n,
+                                          long long total, const int* skip) {
+  if (skip && *skip) return;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = chart_find(cb, n, x, true);
+    const ChartBrick& B = cb[b];
+    const long long c = x - B.c_off;
+    int t[3];
+    decode3(c, B.box.n[0], B.box.n[1], t[0], t[1], t[2]);
+    bool keep = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if ((t[d] < 1 && B.box.bc[d][0] != BC_NEIGHBOR) ||
+          (t[d] > B.box.n[d] - 2 && B.box.bc[d][1] != BC_NEIGHBOR))
+        keep = false;
+    uint8_t bits = 0;
+    if (keep) {
+      auto bit = [&](int e, int dx, int dy, int dz) -> bool {
+        int q[3] = {t[0] + dx, t[1] + dy, t[2] + dz};
+        const ChartBrick& S = cb[chart_owner(cb, b, q)];
+        if (!chart_inside(S.box, q)) return false;
+        return (S.sb[q[0] + (long long)S.box.n[0] * (q[1] + (long long)S.box.n[1] * q[2])] >>
+                e) & 1;
+      };
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          if (e == d) continue;
+          const int ex = e == 0, ey = e == 1, ez = e == 2;
+          const int dx = d == 0, dy = d == 1, dz = d == 2;
+          if (bit(e, 0, 0, 0) || bit(e, ex, ey, ez) || bit(e, -dx, -dy, -dz) ||
+              bit(e, ex - dx, ey - dy, ez - dz))
+            bits |= (uint8_t)(1u << d);
+        }
+      }
+    }
+    B.df[c] = bits;
+  }
+}
+
+// Ghost values at the end of a step: an exchange-reachable ghost takes the
+// value of the cell it images, in whichever brick that lies (the reference's
+// exchanged increments keep it equal to that cell); every other ghost keeps
+// its conserved values through the floors of ComputeFromConserved.
+__global__ void chart_ghost_refresh_kernel(const ChartBrick* __restrict__ cb, int n,
+                                           long long total, Phys ph, const int* skip) {
+  if (skip && *skip) return;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int b = chart_find(cb, n, x, false);
+    const ChartBrick& B = cb[b];
+    const long long v = x - B.v_off, nV = B.box.nV;
+    int t[3];
+    decode3(v, B.box.m[0], B.box.m[1], t[0], t[1], t[2]);
+    int p[3] = {t[0] - 2, t[1] - 2, t[2] - 2};
+    if (chart_inside(B.box, p)) continue;
+    if (chart_reachable(B, p)) {
+      int c[3] = {p[0], p[1], p[2]};
+      const ChartBrick& S = cb[chart_owner(cb, b, c)];
+      const long long s = ghost_index(S.box, c), snV = S.box.nV;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) B.U[f * nV + v] = S.U[f * snV + s];
+    } else {
+      Cons u{B.U[v], B.U[nV + v], B.U[2 * nV + v], B.U[3 * nV + v], B.U[4 * nV + v]};
+      Prim w;
+      cons_to_prim(u, w, ph.nmin);
+      double P, CS, SB;
+      eos_cell(w.N, w.E, ph, P, CS, &SB);
+      B.U[v] = u.D;
+      B.U[nV + v] = u.S1;
+      B.U[2 * nV + v] = u.S2;
+      B.U[3 * nV + v] = u.S3;
+      B.U[4 * nV + v] = u.G;
+      B.U[5 * nV + v] = SB * w.N;
+    }
+  }
+}
+
+}  // namespace gfx

@@ -5,7 +5,20 @@
 // baryon mass M and every metric entry are exactly 1 on the rectangular chart,
 // so the products with them that the reference performs are exact and are
 // left out here.
+//
+// GFX_FAST_MATH = 1 builds the speed variant of the same kernels (compiled
+// with --fmad=true): multiplies and adds may fuse, a division by a value with
+// a known rounded reciprocal r is the product a r (within 1.5 ulp of the
+// quotient, where the exact variant corrects it to the rounded quotient), the
+// limiter takes the smallest of those products, and the entropy per baryon is
+// c_v (log P - gamma log N) instead of c_v log(P (1/N)^gamma).  Each changes a
+// result by a few units in the last place of that operation, far inside the
+// 1e-12 per-step bar.  The shock threshold test stays exact in both variants.
 #pragma once
+
+#ifndef GFX_FAST_MATH
+#define GFX_FAST_MATH 0
+#endif
 
 #include <cfloat>
 #include <cstdint>
@@ -60,6 +73,10 @@ __device__ __forceinline__ double fmin3(double a, double b, double c) {
 __device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
 
 __device__ __forceinline__ double markstein(double a, double b, double r) {
+#if GFX_FAST_MATH
+  (void)b;
+  return a * r;
+#endif
   const double q0 = a * r;
   const double e0 = __fma_rn(-b, q0, a);
   const double q1 = __fma_rn(e0, r, q0);
@@ -74,7 +91,12 @@ __device__ __forceinline__ bool exp_in_range(double x) {
 }
 
 __device__ __forceinline__ bool quotient_in_range(double a, double r) {
+#if GFX_FAST_MATH
+  (void)a, (void)r;
+  return true;  // the product a r needs no exponent window
+#else
   return exp_in_range(a) & exp_in_range(a * r);
+#endif
 }
 
 // The same window for a divisor of the chart geometry (a width, a centre
@@ -84,8 +106,13 @@ __device__ __forceinline__ bool quotient_in_range(double a, double r) {
 // 2^700, or a == 0, puts both a and a r inside the window, and one test on
 // a suffices.
 __device__ __forceinline__ bool geo_quotient_in_range(double a) {
+#if GFX_FAST_MATH
+  (void)a;
+  return true;
+#else
   const double ax = fabs(a);
   return (ax >= 0x1p-600 && ax < 0x1p700) || a == 0.0;
+#endif
 }
 
 __device__ __forceinline__ double div_geo(double a, double b, double r) {
@@ -133,6 +160,11 @@ __device__ __forceinline__ double limited_slope(double vm, double v0, double vp,
   const double s = copysign(0.5, dvl) + copysign(0.5, dvr);
   const double a1 = fabs(theta * dvl), a2 = fabs(theta * dvr), a3 = fabs(num);
   const double t1 = a1 * rdxl, t2 = a2 * rdxr, t3 = a3 * rcden;
+#if GFX_FAST_MATH
+  // the smallest of the products with the reciprocals is the slope's size
+  (void)dxl, (void)dxr, (void)sql, (void)cden;
+  return s * fmin3(t1, t2, t3);
+#endif
   // branch-free argmin of the approximations and the runner-up
   const bool p12 = t1 <= t2;
   double tm = p12 ? t1 : t2, tr = p12 ? t2 : t1;
@@ -242,6 +274,18 @@ __device__ __noinline__ FaceVals parabolic_cell(double vM, double vC, double vP,
   return r;
 }
 
+// Entropy per baryon of Apply_EOS_I_E_Kernel (Fluid_P_I__Kernel.f90:244-267)
+// with N0 = P0 = 1, for N > 0 and P > 0: c_v log(P (N0/N)^gamma) as written,
+// or c_v (log P - gamma log N) in the speed variant (two logarithms instead of
+// a logarithm and a power).
+__device__ __forceinline__ double entropy_per_baryon(double P, double N, const Phys& ph) {
+#if GFX_FAST_MATH
+  return ph.c_v * (log(P) - ph.gamma * log(N));
+#else
+  return ph.c_v * log(P * pow(1.0 / N, ph.gamma));
+#endif
+}
+
 // State at one face after ComputeFromPrimitiveCommon (Fluid_P_I__Form.f90:509-601):
 // Apply_EOS_I_E (Fluid_P_I__Kernel.f90:244-267), Compute_D_S_G
 // (Fluid_D__Kernel.f90:47-101), Compute_G_G (Fluid_P__Kernel.f90:12-52),
@@ -259,7 +303,7 @@ __device__ __forceinline__ void face_state(double N, double V1, double V2, doubl
   double CS = 0.0, SB = -kSqrtHuge;
   if (N > 0.0 && P > 0.0) {
     CS = sqrt(ph.gamma * P / N);
-    if (NF == 6) SB = ph.c_v * log(P * pow(1.0 / N, ph.gamma));
+    if (NF == 6) SB = entropy_per_baryon(P, N, ph);
   }
   if (N < 0.0) N = 0.0;
   s.N = N;
@@ -415,6 +459,45 @@ __device__ __forceinline__ void cons_to_prim(Cons& u, Prim& w, double nmin) {
   }
 }
 
+// The recovery as the shock test needs it: the pressure and velocities of the
+// reference's arithmetic, every operation rounded on its own, in both builds.
+// The test's flags switch the flux discontinuously, so a pressure or a
+// velocity difference one unit in the last place off can flip a flag where
+// the jump sits at the threshold or the velocities are equal.  The exact
+// build's cons_to_prim already rounds so; the speed build spells the
+// operations out as intrinsics, which are never fused.
+__device__ __forceinline__ void cons_to_prim_exact(Cons& u, Prim& w, double nmin) {
+#if GFX_FAST_MATH
+  if (u.D > nmin) {
+    w.N = u.D;
+    w.V1 = __ddiv_rn(u.S1, u.D);
+    w.V2 = __ddiv_rn(u.S2, u.D);
+    w.V3 = __ddiv_rn(u.S3, u.D);
+    const double ke = __dadd_rn(__dadd_rn(__dmul_rn(u.S1, w.V1), __dmul_rn(u.S2, w.V2)),
+                                __dmul_rn(u.S3, w.V3));
+    w.E = __dsub_rn(u.G, __dmul_rn(0.5, ke));
+  } else {
+    w.N = nmin;
+    w.V1 = 0.0;
+    w.V2 = 0.0;
+    w.V3 = 0.0;
+    w.E = 0.0;
+    u.D = nmin;
+    u.S1 = 0.0;
+    u.S2 = 0.0;
+    u.S3 = 0.0;
+    u.G = 0.0;
+  }
+  if (w.E < 0.0) {
+    w.E = 0.0;
+    u.G = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dmul_rn(u.S1, w.V1), __dmul_rn(u.S2, w.V2)),
+                                   __dmul_rn(u.S3, w.V3)));
+  }
+#else
+  cons_to_prim(u, w, nmin);
+#endif
+}
+
 // The floored conserved values that cons_to_prim would have produced, rebuilt
 // from the original conserved values and the primitives without divisions:
 // D' = N; S' = S unless D <= nmin; G' = 0.5 (S'.V) exactly when the recovered
@@ -462,7 +545,7 @@ __device__ __forceinline__ void eos_cell(double N, double E, const Phys& ph, dou
   P = ph.gm1 * E;
   if (N > 0.0 && P > 0.0) {
     CS = sqrt(ph.gamma * P / N);
-    if (SB) *SB = ph.c_v * log(P * pow(1.0 / N, ph.gamma));
+    if (SB) *SB = entropy_per_baryon(P, N, ph);
   } else {
     CS = 0.0;
     if (SB) *SB = -kSqrtHuge;

@@ -18,6 +18,7 @@
 
 #include "adjoint_kernels.cuh"
 #include "aux_kernels.cuh"
+#include "chart_kernels.cuh"
 #include "gfx_fluid.h"
 
 using namespace gfx;
@@ -129,17 +130,28 @@ HostAxis build_axis(int n, double mn, double mx, int g) {
 
 enum FeatureState { FEAT_ZERO = 0, FEAT_VALID = 1, FEAT_PENDING = 2 };
 
-int g_num_sms = 0;
-std::once_flag g_sm_once;
+// Launch attributes and the SM count belong to each device's context, so
+// they are set up and cached per device (the current one at the call).
+constexpr int kMaxDevices = 64;
+
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+  return dev;
+}
+
+int g_num_sms[kMaxDevices] = {};
+std::once_flag g_sm_once[kMaxDevices];
 
 int num_sms() {
-  std::call_once(g_sm_once, [] {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
+  const int dev = current_device();
+  if (dev < 0) return 148;
+  std::call_once(g_sm_once[dev], [dev] {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    g_num_sms[dev] = n > 0 ? n : 148;
   });
-  return g_num_sms;
+  return g_num_sms[dev];
 }
 
 }  // namespace
@@ -149,6 +161,7 @@ constexpr int kMaxSlabs = 32;
 
 struct gfx_fluid {
   gfx_fluid_config cfg;
+  const gfx_fluid_chart* chart = nullptr;  // the chart this brick belongs to, if any
   Phys ph;
   Box box;
   HostAxis axis[3];
@@ -162,6 +175,8 @@ struct gfx_fluid {
   unsigned long long* tsi_bits = nullptr;  // [1]
   int* counters = nullptr;                 // [4]
   Clock* clock = nullptr;                  // evolve clock
+  Clock* clock_host = nullptr;             // [2] pinned copies read between chunks
+  cudaEvent_t chunk_ev[2] = {};            // after each copy
   double* dt_slot = nullptr;               // dt of gfx_fluid_step
   WorkItem* items = nullptr;
   int n_items = 0;
@@ -200,26 +215,30 @@ struct gfx_fluid {
 
 namespace {
 
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED,
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, int BAT,
           bool PARAB = false, int TYt = kTileY>
 cudaError_t launch_stage_t(const BrickDesc& d, const BrickDesc* many, const WorkItem* items,
                            int n_items, int* counter, const Phys& ph, cudaStream_t s) {
   using SM = StageLayout<NF, TYt, PARAB>;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  static int per_sm = 1;
-  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BATCHED, PARAB, TYt>;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)SM::kBytes);
-    if (attr_err == cudaSuccess)
-      attr_err =
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SM::NT, SM::kBytes);
-    if (per_sm < 1) per_sm = 1;
+  // the shared-memory attribute and the occupancy, once per device
+  static std::once_flag once[kMaxDevices];
+  static cudaError_t attr_err[kMaxDevices];
+  static int per_sm[kMaxDevices];
+  auto kern = stage_kernel<MODE, IN_PRIM, HLLC, GRAV, NF, BAT, PARAB, TYt>;
+  const int dev = current_device();
+  if (dev < 0) return cudaErrorInvalidDevice;
+  std::call_once(once[dev], [&] {
+    int n = 1;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SM::kBytes);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, SM::NT, SM::kBytes);
+    attr_err[dev] = e;
+    per_sm[dev] = n < 1 ? 1 : n;
   });
-  if (attr_err != cudaSuccess) return attr_err;
+  if (attr_err[dev] != cudaSuccess) return attr_err[dev];
   // persistent grid: every resident CTA slot pulls work items
-  const int grid = std::max(1, std::min(n_items, num_sms() * per_sm));
+  const int grid = std::max(1, std::min(n_items, num_sms() * per_sm[dev]));
   kern<<<grid, SM::NT, SM::kBytes, s>>>(d, many, items, n_items, counter, ph);
   return cudaGetLastError();
 }
@@ -230,8 +249,8 @@ cudaError_t launch_stage_parabolic(int mode, bool in_prim, bool hllc, bool grav,
                                    int* counter, const Phys& ph, cudaStream_t s) {
 #define GFX_PSTAGE(M, IP, HC, GR, NF)                                                     \
   if (mode == M && in_prim == IP && hllc == HC && grav == GR)                            \
-    return launch_stage_t<M, IP, HC, GR, NF, false, true>(d, nullptr, items, n_items,     \
-                                                          counter, ph, s);
+    return launch_stage_t<M, IP, HC, GR, NF, BAT_SINGLE, true>(d, nullptr, items, n_items, \
+                                                               counter, ph, s);
   GFX_PSTAGE(MODE_INCREMENT, false, false, false, 6)
   GFX_PSTAGE(MODE_INCREMENT, false, true, false, 6)
   GFX_PSTAGE(MODE_INCREMENT, true, false, false, 6)
@@ -252,38 +271,66 @@ cudaError_t launch_stage_parabolic(int mode, bool in_prim, bool hllc, bool grav,
   return cudaErrorInvalidValue;
 }
 
-// The LINEAR variants for tile height TYt.
+// The LINEAR variants for tile height TYt.  bat: BAT_SINGLE (d describes
+// the brick), BAT_BRICKS or BAT_CHART (many holds a descriptor per brick).
 template <int TYt>
-cudaError_t launch_stage_linear(int mode, bool in_prim, bool hllc, bool grav,
+cudaError_t launch_stage_linear(int mode, bool in_prim, bool hllc, bool grav, int bat,
                                 const BrickDesc& d, const BrickDesc* many,
                                 const WorkItem* items, int n_items, int* counter,
                                 const Phys& ph, cudaStream_t s) {
-  const bool bat = many != nullptr;
 #define GFX_STAGE(M, IP, HC, GR, NF, BA)                                                  \
   if (mode == M && in_prim == IP && hllc == HC && grav == GR && bat == BA)              \
     return launch_stage_t<M, IP, HC, GR, NF, BA, false, TYt>(d, many, items, n_items,     \
                                                              counter, ph, s);
-#define GFX_STAGE_B(M, IP, HC, GR, NF) \
-  GFX_STAGE(M, IP, HC, GR, NF, false)  \
-  GFX_STAGE(M, IP, HC, GR, NF, true)
-  GFX_STAGE(MODE_INCREMENT, false, false, false, 6, false)
-  GFX_STAGE(MODE_INCREMENT, false, true, false, 6, false)
-  GFX_STAGE(MODE_INCREMENT, true, false, false, 6, false)
-  GFX_STAGE(MODE_INCREMENT, true, true, false, 6, false)
+#define GFX_STAGE_B(M, IP, HC, GR, NF)  \
+  GFX_STAGE(M, IP, HC, GR, NF, BAT_SINGLE) \
+  GFX_STAGE(M, IP, HC, GR, NF, BAT_BRICKS)
+  GFX_STAGE(MODE_INCREMENT, false, false, false, 6, BAT_SINGLE)
+  GFX_STAGE(MODE_INCREMENT, false, true, false, 6, BAT_SINGLE)
+  GFX_STAGE(MODE_INCREMENT, true, false, false, 6, BAT_SINGLE)
+  GFX_STAGE(MODE_INCREMENT, true, true, false, 6, BAT_SINGLE)
   GFX_STAGE_B(MODE_STAGE1, false, false, false, 5)
   GFX_STAGE_B(MODE_STAGE1, false, true, false, 5)
-  GFX_STAGE(MODE_STAGE1, false, false, true, 5, false)
-  GFX_STAGE(MODE_STAGE1, false, true, true, 5, false)
+  GFX_STAGE(MODE_STAGE1, false, false, true, 5, BAT_SINGLE)
+  GFX_STAGE(MODE_STAGE1, false, true, true, 5, BAT_SINGLE)
   GFX_STAGE_B(MODE_STAGE1, true, false, false, 5)
   GFX_STAGE_B(MODE_STAGE1, true, true, false, 5)
-  GFX_STAGE(MODE_STAGE1, true, false, true, 5, false)
-  GFX_STAGE(MODE_STAGE1, true, true, true, 5, false)
+  GFX_STAGE(MODE_STAGE1, true, false, true, 5, BAT_SINGLE)
+  GFX_STAGE(MODE_STAGE1, true, true, true, 5, BAT_SINGLE)
   GFX_STAGE_B(MODE_STAGE2, true, false, false, 5)
   GFX_STAGE_B(MODE_STAGE2, true, true, false, 5)
-  GFX_STAGE(MODE_STAGE2, true, false, true, 5, false)
-  GFX_STAGE(MODE_STAGE2, true, true, true, 5, false)
+  GFX_STAGE(MODE_STAGE2, true, false, true, 5, BAT_SINGLE)
+  GFX_STAGE(MODE_STAGE2, true, true, true, 5, BAT_SINGLE)
 #undef GFX_STAGE_B
 #undef GFX_STAGE
+  return cudaErrorInvalidValue;
+}
+
+// The chart variants (16-row tiles): stage 1 from conserved values or kept
+// primitives, stage 2, with or without HLLC and gravity.
+cudaError_t launch_stage_chart(int mode, bool in_prim, bool hllc, bool grav,
+                               const BrickDesc* many, const WorkItem* items, int n_items,
+                               int* counter, const Phys& ph, cudaStream_t s) {
+  BrickDesc none;
+  memset(&none, 0, sizeof(none));
+#define GFX_CSTAGE(M, IP, HC, GR)                                                          \
+  if (mode == M && in_prim == IP && hllc == HC && grav == GR)                            \
+    return launch_stage_t<M, IP, HC, GR, 5, BAT_CHART, false, kTileY>(none, many, items,  \
+                                                                      n_items, counter,   \
+                                                                      ph, s);
+  GFX_CSTAGE(MODE_STAGE1, false, false, false)
+  GFX_CSTAGE(MODE_STAGE1, false, true, false)
+  GFX_CSTAGE(MODE_STAGE1, false, false, true)
+  GFX_CSTAGE(MODE_STAGE1, false, true, true)
+  GFX_CSTAGE(MODE_STAGE1, true, false, false)
+  GFX_CSTAGE(MODE_STAGE1, true, true, false)
+  GFX_CSTAGE(MODE_STAGE1, true, false, true)
+  GFX_CSTAGE(MODE_STAGE1, true, true, true)
+  GFX_CSTAGE(MODE_STAGE2, true, false, false)
+  GFX_CSTAGE(MODE_STAGE2, true, true, false)
+  GFX_CSTAGE(MODE_STAGE2, true, false, true)
+  GFX_CSTAGE(MODE_STAGE2, true, true, true)
+#undef GFX_CSTAGE
   return cudaErrorInvalidValue;
 }
 
@@ -299,12 +346,13 @@ cudaError_t launch_stage(int mode, bool in_prim, bool hllc, bool grav, const Bri
     return ty == kTileY ? launch_stage_parabolic(mode, in_prim, hllc, grav, d, items, n_items,
                                                  counter, ph, s)
                         : cudaErrorInvalidValue;
+  const int bat_kind = bat ? BAT_BRICKS : BAT_SINGLE;
   if (ty == 8)
-    return launch_stage_linear<8>(mode, in_prim, hllc, grav, d, many, items, n_items, counter,
-                                  ph, s);
+    return launch_stage_linear<8>(mode, in_prim, hllc, grav, bat_kind, d, many, items, n_items,
+                                  counter, ph, s);
   if (ty == kTileY)
-    return launch_stage_linear<kTileY>(mode, in_prim, hllc, grav, d, many, items, n_items,
-                                       counter, ph, s);
+    return launch_stage_linear<kTileY>(mode, in_prim, hllc, grav, bat_kind, d, many, items,
+                                       n_items, counter, ph, s);
   return cudaErrorInvalidValue;
 }
 
@@ -345,7 +393,23 @@ int validate(const gfx_fluid_config* c) {
   if (c->reconstruction != GFX_RECONSTRUCTION_LINEAR &&
       c->reconstruction != GFX_RECONSTRUCTION_PARABOLIC)
     return fail(GFX_ERR_ARGUMENT, "reconstruction = %d", c->reconstruction);
+#if GFX_FAST_MATH
+  // the parabola's extremum tests switch its face values on quantities that
+  // a unit in the last place moves; only the exact build reproduces them
+  if (c->reconstruction == GFX_RECONSTRUCTION_PARABOLIC)
+    return fail(GFX_ERR_UNSUPPORTED,
+                "PARABOLIC reconstruction: the exact build (libgfx_fluid.so) only");
+#endif
   if (!(c->courant_factor > 0.0)) return fail(GFX_ERR_ARGUMENT, "courant_factor must be > 0");
+  return GFX_OK;
+}
+
+// The step entry points of a single brick apply its boundary conditions on
+// every face; a brick of a chart has faces whose ghosts live in its
+// neighbours, so those calls go through the chart.
+int refuse_chart_brick(const gfx_fluid* h, const char* fn) {
+  if (h && h->chart)
+    return fail(GFX_ERR_ARGUMENT, "%s: a brick of a chart steps through gfx_fluid_chart_*", fn);
   return GFX_OK;
 }
 
@@ -374,6 +438,7 @@ BrickDesc make_desc(gfx_fluid* h, const double* U_in, double* U_out, double* K,
   BrickDesc d;
   memset(&d, 0, sizeof(d));
   for (int a = 0; a < 3; ++a) {
+    d.nb[a][0] = d.nb[a][1] = -1;
     d.n[a] = h->box.n[a];
     d.m[a] = h->box.m[a];
     d.bc[a][0] = h->box.bc[a][0];
@@ -741,6 +806,8 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   return GFX_OK;
 }
 
+int create_handle(const gfx_fluid_config* cfg, const HostAxis* axes, gfx_fluid** out);
+
 }  // namespace
 
 extern "C" {
@@ -773,6 +840,17 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
   *out = nullptr;
   int rc = validate(cfg);
   if (rc) return rc;
+  return create_handle(cfg, nullptr, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The handle of one brick: its own chart geometry (axes == null), or the
+// given per-axis tables (a brick of a chart, whose tables are a slice of the
+// chart's).  cfg has been validated by the caller.
+int create_handle(const gfx_fluid_config* cfg, const HostAxis* axes, gfx_fluid** out) {
   gfx_fluid* h = new (std::nothrow) gfx_fluid();
   if (!h) return fail(GFX_ERR_NO_MEMORY, "host allocation failed");
   h->cfg = *cfg;
@@ -794,7 +872,8 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
     b.m[d] = cfg->n_cells[d] + 4;
     b.bc[d][0] = cfg->boundary[d][0];
     b.bc[d][1] = cfg->boundary[d][1];
-    h->axis[d] = build_axis(b.n[d], cfg->min_coordinate[d], cfg->max_coordinate[d], 2);
+    h->axis[d] = axes ? axes[d]
+                      : build_axis(b.n[d], cfg->min_coordinate[d], cfg->max_coordinate[d], 2);
   }
   b.nV = (long long)b.m[0] * b.m[1] * b.m[2];
   b.nP = (long long)b.n[0] * b.n[1] * b.n[2];
@@ -859,6 +938,10 @@ int gfx_fluid_create(const gfx_fluid_config* cfg, gfx_fluid** out) {
   return GFX_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 int gfx_fluid_destroy(gfx_fluid* h) {
   if (!h) return GFX_OK;
   if (h->graph) cudaGraphExecDestroy(h->graph);
@@ -887,6 +970,9 @@ int gfx_fluid_destroy(gfx_fluid* h) {
     if (h->ev_out[j]) cudaEventDestroy(h->ev_out[j]);
   }
   if (h->ev_end) cudaEventDestroy(h->ev_end);
+  for (int j = 0; j < 2; ++j)
+    if (h->chunk_ev[j]) cudaEventDestroy(h->chunk_ev[j]);
+  if (h->clock_host) cudaFreeHost(h->clock_host);
   if (h->copy_in) cudaStreamDestroy(h->copy_in);
   if (h->copy_out) cudaStreamDestroy(h->copy_out);
   if (h->host_stream) cudaStreamDestroy(h->host_stream);
@@ -916,6 +1002,7 @@ int gfx_fluid_geometry(const gfx_fluid* h, int axis, double* c, double* wl, doub
 }
 
 int gfx_fluid_from_primitive(gfx_fluid* h, const double* prim, double* U, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_from_primitive")) return rc0;
   if (!h || !prim || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
   from_primitive_kernel<<<grid_for(h->box.nV, 256), 256, 0, s>>>(h->box, h->ph, prim, U,
@@ -939,6 +1026,7 @@ int gfx_fluid_to_primitive(gfx_fluid* h, double* U, double* prim, double* aux, v
 }
 
 int gfx_fluid_detect_features(gfx_fluid* h, const double* U, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_detect_features")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   int rc = run_features(h, U, h->prims_pending ? h->Pst : nullptr, (cudaStream_t)stream);
   if (rc) return rc;
@@ -969,6 +1057,7 @@ int gfx_fluid_get_features(gfx_fluid* h, uint8_t* flags, void* stream) {
 
 int gfx_fluid_increment(gfx_fluid* h, const double* U, double* K, double dt, double weight,
                         double* fluence, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_increment")) return rc0;
   if (!h || !U || !K) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
   const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
@@ -990,6 +1079,7 @@ int gfx_fluid_increment(gfx_fluid* h, const double* U, double* K, double dt, dou
 }
 
 int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   cudaStream_t s = (cudaStream_t)stream;
@@ -1007,6 +1097,7 @@ int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* st
 }
 
 int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence_host) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_host")) return rc0;
   if (!h || !U_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   const size_t bytes = 6 * (size_t)h->box.nV * sizeof(double);
   if (!h->host_stream) CUDA_TRY(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
@@ -1033,6 +1124,7 @@ int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence
 
 int gfx_fluid_timestep(gfx_fluid* h, const double* U, int i_cycle, double* dt_host,
                        void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_timestep")) return rc0;
   if (!h || !U || !dt_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
   reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 0);
@@ -1060,6 +1152,7 @@ int gfx_fluid_timestep(gfx_fluid* h, const double* U, int i_cycle, double* dt_ho
 
 int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double finish_time,
                      int n_cycles_max, double* time_out, int* i_cycle_out, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_evolve")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (n_cycles_max < 0) return fail(GFX_ERR_ARGUMENT, "n_cycles_max < 0");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1120,16 +1213,36 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
         return fail(GFX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
       h->graph_U = U;
     }
-    int done_cycles = 1;
+    // chunks of cycles, two in flight: after enqueuing chunk j the host
+    // waits for the clock read after chunk j - 1, so the device runs chunk j
+    // while the host decides (a host thread that is slow to wake leaves no
+    // gap on the device).  A chunk enqueued after the finish runs as no-ops
+    // (the kernels test the clock's done flag).
+    if (!h->clock_host) {
+      if (cudaMallocHost(&h->clock_host, 2 * sizeof(Clock)) != cudaSuccess) {
+        h->clock_host = nullptr;
+        return fail(GFX_ERR_NO_MEMORY, "cudaMallocHost of the evolve clock");
+      }
+      for (int j = 0; j < 2; ++j)
+        CUDA_TRY(cudaEventCreateWithFlags(&h->chunk_ev[j], cudaEventDisableTiming));
+    }
+    int done_cycles = 1, slot = 0;
+    bool pending = false;
     const int chunk = 8;
     while (done_cycles < n_cycles_max) {
       const int nrep = std::min(chunk, n_cycles_max - done_cycles);
       for (int r = 0; r < nrep; ++r) CUDA_TRY(cudaGraphLaunch(h->graph, s));
       h->launches += (long long)nrep * h->graph_kernels;
       done_cycles += nrep;
-      CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
-      CUDA_TRY(cudaStreamSynchronize(s));
-      if (c.done) break;
+      CUDA_TRY(cudaMemcpyAsync(h->clock_host + slot, dc, sizeof(Clock), cudaMemcpyDeviceToHost,
+                               s));
+      CUDA_TRY(cudaEventRecord(h->chunk_ev[slot], s));
+      if (pending) {
+        CUDA_TRY(cudaEventSynchronize(h->chunk_ev[slot ^ 1]));
+        if (h->clock_host[slot ^ 1].done) break;
+      }
+      pending = true;
+      slot ^= 1;
     }
   }
   CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
@@ -1141,6 +1254,7 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
 
 int gfx_fluid_step_timed(gfx_fluid* h, double* U, double dt, double* fluence, double* ms_out,
                          void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_timed")) return rc0;
   if (!h || !U || !ms_out) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
   cudaStream_t s = (cudaStream_t)stream;
@@ -1181,8 +1295,10 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
                            gfx_fluid_batch** out) {
   if (!out || n < 1 || !handles || !U) return fail(GFX_ERR_ARGUMENT, "bad batch arguments");
   *out = nullptr;
-  for (int b = 0; b < n; ++b)
+  for (int b = 0; b < n; ++b) {
     if (!handles[b] || !U[b]) return fail(GFX_ERR_ARGUMENT, "brick %d: NULL handle or state", b);
+    if (int rc0 = refuse_chart_brick(handles[b], "gfx_fluid_batch_create")) return rc0;
+  }
   const gfx_fluid_config& c0 = handles[0]->cfg;
   for (int b = 1; b < n; ++b) {
     const gfx_fluid_config& c = handles[b]->cfg;
@@ -1440,6 +1556,7 @@ int gfx_fluid_check_state(gfx_fluid* h, const double* U, void* stream) {
 }
 
 int gfx_fluid_resume(gfx_fluid* h, double* U) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_resume")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   h->prims_pending = false;
   h->features = FEAT_PENDING;
@@ -1529,29 +1646,24 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = GFX_FLUID_NOALLOC_SCRATCH_BYTES;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
 // The array's device address on the current device.  In host code the array's
 // name is only a host-side stand-in, so the address is asked of the runtime,
-// once per device, with that device current.
+// with that device current.  It is asked on every call rather than cached:
+// after a cudaDeviceReset the module is loaded again, possibly elsewhere, and
+// the lookup costs little next to a step.  The first call on a device is the
+// one that loads the module there.
 int noalloc_scratch(unsigned char** out) {
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
+  if (dev < 0 || dev >= kMaxDevices)
     return fail(GFX_ERR_UNSUPPORTED, "device %d: the no-allocation step serves devices 0..%d",
-                dev, kNoAllocMaxDevices - 1);
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(GFX_ERR_CUDA, "cudaGetSymbolAddress of the no-allocation scratch: %s",
-                  cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = (unsigned char*)p;
-  }
-  *out = g_noalloc_ptr[dev];
+                dev, kMaxDevices - 1);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(GFX_ERR_CUDA, "cudaGetSymbolAddress of the no-allocation scratch: %s",
+                cudaGetErrorString(e));
+  *out = (unsigned char*)p;
   return GFX_OK;
 }
 
@@ -1863,6 +1975,7 @@ extern "C" {
 int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const double* lam_np1,
                            double* lam_n, const double* U_np1, int detect_features,
                            void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_adjoint")) return rc0;
   if (!h || !U_n || !lam_np1 || !lam_n) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (lam_n == lam_np1) return fail(GFX_ERR_ARGUMENT, "lam_n must not alias lam_np1");
   if (h->cfg.reconstruction != GFX_RECONSTRUCTION_LINEAR)
@@ -1937,6 +2050,531 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
                                                        lam_n);
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
+  return GFX_OK;
+}
+
+}  // extern "C"
+
+// ---- A chart of several bricks on one device --------------------------------
+// Chart_SLD (Chart_SLD__Form.f90) splits one domain into equal bricks, one
+// per MPI rank, and exchanges the ghost layers of faces and edges between
+// them every stage (ExchangeGhostData, :131-201, called for the increment
+// from Step_RK_C_ASC__Template.f90:1237-1246).  On one device every brick's
+// cells are in the same memory: the chart's stage launches are batched
+// launches whose work items span all bricks, and a halo cell across a face
+// is read from the neighbouring brick's arrays of the same stage (the
+// descriptors of a stage link each brick to the bricks across its faces).
+// The chart has one clock and one time step (the MIN all-reduce of the
+// time step, Integrator_Template.f90:919, is the one CFL word every brick's
+// stage 2 reduces into).
+struct gfx_fluid_chart {
+  gfx_fluid_config cfg;      // the whole chart
+  int nbk[3] = {1, 1, 1};    // bricks per axis
+  int n = 0;                 // bricks
+  std::vector<gfx_fluid*> h;  // brick b = ix + nbk[0] (iy + nbk[1] iz)
+  std::vector<double*> U;     // the bound states
+  std::vector<int> links;     // [b][3][2] brick across each face, or -1
+  Phys ph;
+  bool hllc = false, grav = false;
+  BrickDesc *d1 = nullptr, *d1p = nullptr, *d1w = nullptr, *d2 = nullptr;  // device, [n]
+  std::vector<BrickDesc> hd1, hd1p, hd1w, hd2;                             // host copies
+  ChartBrick* cb = nullptr;
+  std::vector<ChartBrick> hcb;
+  WorkItem* items = nullptr;
+  int n_items = 0;
+  long long total_v = 0, total_c = 0;
+  unsigned long long* tsi_bits = nullptr;  // [1]
+  Clock* clock = nullptr;                  // [2]: the chart's clock, a scratch clock
+  int* counters = nullptr;                 // [4]
+  Clock* clock_host = nullptr;             // [2] pinned
+  cudaEvent_t chunk_ev[2] = {};
+  int features = FEAT_ZERO;
+  bool prims_pending = false;  // the kept primitives are the state (after from_primitive)
+  bool wn_valid = false;       // the primitives the last stage 2 stored are the state's
+  cudaGraphExec_t graph = nullptr;
+  long long graph_kernels = 0, launches = 0;
+};
+
+namespace {
+
+__global__ void chart_set_clock_kernel(Clock* c, double dt) {
+  c->dt = dt;
+  c->done = 0;
+}
+
+int chart_upload_descs(gfx_fluid_chart* C, cudaStream_t s) {
+  const size_t bytes = C->n * sizeof(BrickDesc);
+  CUDA_TRY(cudaMemcpyAsync(C->d1, C->hd1.data(), bytes, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(C->d1p, C->hd1p.data(), bytes, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(C->d1w, C->hd1w.data(), bytes, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(C->d2, C->hd2.data(), bytes, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(C->cb, C->hcb.data(), C->n * sizeof(ChartBrick),
+                           cudaMemcpyHostToDevice, s));
+  // the host copies may change on the next call: the copies above are staged
+  // from pageable memory, finish them before returning
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return GFX_OK;
+}
+
+// The inverse CFL time of every brick's state into the chart's word, and
+// the time step of clock dc from it.
+int chart_initial_dt(gfx_fluid_chart* C, Clock* dc, int clip, cudaStream_t s) {
+  reset_bits_kernel<<<1, 32, 0, s>>>(C->tsi_bits, 1, C->counters, 0);
+  for (int b = 0; b < C->n; ++b) {
+    gfx_fluid* h = C->h[b];
+    inverse_timestep_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(
+        h->box, h->ph, C->U[b], C->prims_pending ? h->Pst : nullptr, h->dgeo[0], h->dgeo[1],
+        h->dgeo[2], C->tsi_bits);
+  }
+  finalize_dt_kernel<<<1, 1, 0, s>>>(C->ph, C->tsi_bits, dc, 1, clip);
+  CUDA_TRY(cudaGetLastError());
+  C->launches += C->n + 2;
+  return GFX_OK;
+}
+
+// The launches of one RK2 step of every brick (dt and the skip flag in the
+// chart's clock): features (across brick faces), stage 1, stage 2, ghosts.
+int enqueue_chart_step(gfx_fluid_chart* C, bool detect, bool from_wn, cudaStream_t s) {
+  const int blk = 256;
+  const int* skip = &C->clock[0].done;
+  reset_bits_kernel<<<1, 32, 0, s>>>(C->tsi_bits, 1, C->counters, 4);
+  CUDA_TRY(cudaGetLastError());
+  C->launches += 1;
+  if (C->hllc && detect) {
+    if (from_wn)
+      chart_detect_shock_kernel<true><<<grid_for(C->total_c, blk), blk, 0, s>>>(
+          C->cb, C->n, C->total_c, C->ph, skip);
+    else
+      chart_detect_shock_kernel<false><<<grid_for(C->total_c, blk), blk, 0, s>>>(
+          C->cb, C->n, C->total_c, C->ph, skip);
+    chart_detect_flags_kernel<<<grid_for(C->total_c, blk), blk, 0, s>>>(C->cb, C->n,
+                                                                        C->total_c, skip);
+    CUDA_TRY(cudaGetLastError());
+    C->launches += 2;
+  }
+  const bool in_prim = C->prims_pending || from_wn;
+  const BrickDesc* d1 = C->prims_pending ? C->d1p : (from_wn ? C->d1w : C->d1);
+  CUDA_TRY(launch_stage_chart(MODE_STAGE1, in_prim, C->hllc, C->grav, d1, C->items, C->n_items,
+                              C->counters, C->ph, s));
+  CUDA_TRY(launch_stage_chart(MODE_STAGE2, true, C->hllc, C->grav, C->d2, C->items,
+                              C->n_items, C->counters + 1, C->ph, s));
+  chart_ghost_refresh_kernel<<<grid_for(C->total_v, blk), blk, 0, s>>>(C->cb, C->n,
+                                                                       C->total_v, C->ph, skip);
+  CUDA_TRY(cudaGetLastError());
+  C->launches += 3;
+  return GFX_OK;
+}
+
+HostAxis slice_axis(const HostAxis& g, int o, int m) {
+  // entries o .. o + m of the chart's tables: the brick's ghost-inclusive
+  // index t is the chart's o + t
+  HostAxis a;
+  auto cut = [&](const std::vector<double>& v, int len) {
+    std::vector<double> r(len, 0.0);
+    for (int t = 0; t < len; ++t)
+      if (o + t < (int)v.size()) r[t] = v[o + t];
+    return r;
+  };
+  a.X = cut(g.X, m);
+  a.WL = cut(g.WL, m);
+  a.WR = cut(g.WR, m);
+  a.W = cut(g.W, m);
+  a.dXI = cut(g.dXI, m + 1);
+  a.SQ = cut(g.SQ, m + 1);
+  a.CDEN = cut(g.CDEN, m + 1);
+  a.RDXI = cut(g.RDXI, m + 1);
+  a.RCDEN = cut(g.RCDEN, m + 1);
+  a.RW = cut(g.RW, m + 1);
+  const int Lg = (int)(g.PAR.size() / PG_N), L = m + 1;
+  a.PAR.assign((size_t)PG_N * L, 0.0);
+  for (int q = 0; q < PG_N; ++q)
+    for (int t = 0; t < L; ++t)
+      if (o + t < Lg) a.PAR[(size_t)q * L + t] = g.PAR[(size_t)q * Lg + o + t];
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfx_fluid_chart_create(const gfx_fluid_config* cfg, const int n_bricks[3],
+                           gfx_fluid_chart** out) {
+  if (!out || !n_bricks) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  int rc = validate(cfg);
+  if (rc) return rc;
+  if (cfg->reconstruction != GFX_RECONSTRUCTION_LINEAR)
+    return fail(GFX_ERR_UNSUPPORTED, "a chart of bricks: LINEAR reconstruction only");
+  int nb[3];
+  for (int a = 0; a < 3; ++a) {
+    if (n_bricks[a] < 1) return fail(GFX_ERR_ARGUMENT, "n_bricks[%d] = %d", a, n_bricks[a]);
+    if (cfg->n_cells[a] % n_bricks[a] != 0)
+      return fail(GFX_ERR_ARGUMENT, "axis %d: %d cells do not split into %d equal bricks", a,
+                  cfg->n_cells[a], n_bricks[a]);
+    nb[a] = cfg->n_cells[a] / n_bricks[a];
+    if (nb[a] < 4)
+      return fail(GFX_ERR_ARGUMENT, "axis %d: bricks of %d cells; at least 4 per axis", a,
+                  nb[a]);
+  }
+  gfx_fluid_chart* C = new (std::nothrow) gfx_fluid_chart();
+  if (!C) return fail(GFX_ERR_NO_MEMORY, "host allocation failed");
+  auto cleanup = [&](int code) {
+    gfx_fluid_chart_destroy(C);
+    return code;
+  };
+  C->cfg = *cfg;
+  for (int a = 0; a < 3; ++a) C->nbk[a] = n_bricks[a];
+  C->n = n_bricks[0] * n_bricks[1] * n_bricks[2];
+  C->hllc = cfg->riemann_solver == GFX_RIEMANN_HLLC;
+  C->grav = cfg->uniform_acceleration != 0.0;
+  // the chart's geometry, of which every brick takes its slice
+  HostAxis G[3];
+  for (int a = 0; a < 3; ++a)
+    G[a] = build_axis(cfg->n_cells[a], cfg->min_coordinate[a], cfg->max_coordinate[a], 2);
+  C->links.assign((size_t)C->n * 6, -1);
+  std::vector<WorkItem> items;
+  std::vector<long long> work;
+  for (int b = 0; b < C->n; ++b) {
+    const int ib[3] = {b % n_bricks[0], (b / n_bricks[0]) % n_bricks[1],
+                       b / (n_bricks[0] * n_bricks[1])};
+    gfx_fluid_config bc = *cfg;
+    HostAxis A[3];
+    for (int a = 0; a < 3; ++a) {
+      bc.n_cells[a] = nb[a];
+      const int o = ib[a] * nb[a];  // the brick's first proper cell in the chart
+      A[a] = slice_axis(G[a], o, nb[a] + 4);
+      // the brick's extent, for the record (the geometry is the slice)
+      bc.min_coordinate[a] = G[a].X[o + 2] - G[a].WL[o + 2];
+      bc.max_coordinate[a] = G[a].X[o + nb[a] + 1] + G[a].WR[o + nb[a] + 1];
+      const bool first = ib[a] == 0, last = ib[a] == n_bricks[a] - 1;
+      const bool per = cfg->boundary[a][0] == GFX_BC_PERIODIC;
+      bc.boundary[a][0] = first ? cfg->boundary[a][0] : BC_NEIGHBOR;
+      bc.boundary[a][1] = last ? cfg->boundary[a][1] : BC_NEIGHBOR;
+      int lo[3] = {ib[0], ib[1], ib[2]}, hi[3] = {ib[0], ib[1], ib[2]};
+      lo[a] = first ? n_bricks[a] - 1 : ib[a] - 1;
+      hi[a] = last ? 0 : ib[a] + 1;
+      auto idx = [&](const int* q) { return q[0] + n_bricks[0] * (q[1] + n_bricks[1] * q[2]); };
+      C->links[b * 6 + a * 2 + 0] = (!first || per) ? idx(lo) : -1;
+      C->links[b * 6 + a * 2 + 1] = (!last || per) ? idx(hi) : -1;
+    }
+    gfx_fluid* h = nullptr;
+    rc = create_handle(&bc, A, &h);
+    if (rc) return cleanup(rc);
+    h->chart = C;
+    C->h.push_back(h);
+    if (b == 0) C->ph = h->ph;
+    // work items of 32 x 16 columns, z chunks of 32 planes, longest first
+    const int len = std::min(nb[2], 32);
+    for (int z = 0; z < nb[2]; z += len)
+      for (int y = 0; y < nb[1]; y += kTileY)
+        for (int x = 0; x < nb[0]; x += TX) {
+          items.push_back({b, x, y, z, std::min(nb[2], z + len)});
+          work.push_back((long long)std::min(TX, nb[0] - x) * std::min(kTileY, nb[1] - y) *
+                         (std::min(nb[2], z + len) - z));
+        }
+  }
+  std::vector<int> order(items.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  std::vector<WorkItem> sorted(items.size());
+  for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
+  C->n_items = (int)sorted.size();
+  const size_t n = (size_t)C->n;
+  if (cudaMalloc(&C->d1, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&C->d1p, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&C->d1w, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&C->d2, n * sizeof(BrickDesc)) != cudaSuccess ||
+      cudaMalloc(&C->cb, n * sizeof(ChartBrick)) != cudaSuccess ||
+      cudaMalloc(&C->items, sorted.size() * sizeof(WorkItem)) != cudaSuccess ||
+      cudaMalloc(&C->tsi_bits, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&C->clock, 2 * sizeof(Clock)) != cudaSuccess ||
+      cudaMalloc(&C->counters, 4 * sizeof(int)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc chart tables"));
+  if (cudaMemcpy(C->items, sorted.data(), sorted.size() * sizeof(WorkItem),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(C->clock, 0, 2 * sizeof(Clock)) != cudaSuccess)
+    return cleanup(fail(GFX_ERR_CUDA, "copy chart work items"));
+  *out = C;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_destroy(gfx_fluid_chart* C) {
+  if (!C) return GFX_OK;
+  if (C->graph) cudaGraphExecDestroy(C->graph);
+  for (gfx_fluid* h : C->h) gfx_fluid_destroy(h);
+  cudaFree(C->d1);
+  cudaFree(C->d1p);
+  cudaFree(C->d1w);
+  cudaFree(C->d2);
+  cudaFree(C->cb);
+  cudaFree(C->items);
+  cudaFree(C->tsi_bits);
+  cudaFree(C->clock);
+  cudaFree(C->counters);
+  for (int j = 0; j < 2; ++j)
+    if (C->chunk_ev[j]) cudaEventDestroy(C->chunk_ev[j]);
+  if (C->clock_host) cudaFreeHost(C->clock_host);
+  delete C;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_n_bricks(const gfx_fluid_chart* C, int* n) {
+  if (!C || !n) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *n = C->n;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_brick(gfx_fluid_chart* C, int b, gfx_fluid** handle, int* brick_index) {
+  if (!C || b < 0 || b >= C->n) return fail(GFX_ERR_ARGUMENT, "brick %d of a chart", b);
+  if (handle) *handle = C->h[b];
+  if (brick_index) {
+    brick_index[0] = b % C->nbk[0];
+    brick_index[1] = (b / C->nbk[0]) % C->nbk[1];
+    brick_index[2] = b / (C->nbk[0] * C->nbk[1]);
+  }
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_bind(gfx_fluid_chart* C, double* const* U) {
+  if (!C || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  for (int b = 0; b < C->n; ++b)
+    if (!U[b]) return fail(GFX_ERR_ARGUMENT, "brick %d: NULL state", b);
+  C->U.assign(U, U + C->n);
+  C->hd1.assign(C->n, BrickDesc());
+  C->hd1p.assign(C->n, BrickDesc());
+  C->hd1w.assign(C->n, BrickDesc());
+  C->hd2.assign(C->n, BrickDesc());
+  C->hcb.assign(C->n, ChartBrick());
+  C->total_v = C->total_c = 0;
+  const double* dt = &C->clock[0].dt;
+  const int* skip = &C->clock[0].done;
+  for (int b = 0; b < C->n; ++b) {
+    gfx_fluid* h = C->h[b];
+    const uint8_t* df = C->hllc ? h->df : nullptr;
+    BrickDesc* ds[4] = {&C->hd1[b], &C->hd1p[b], &C->hd1w[b], &C->hd2[b]};
+    const BrickDesc* dev[4] = {C->d1, C->d1p, C->d1w, C->d2};
+    *ds[0] = make_desc(h, U[b], nullptr, nullptr, nullptr, df, nullptr, dt, 0.5, skip);
+    *ds[1] = make_desc(h, U[b], nullptr, nullptr, h->Pst, df, nullptr, dt, 0.5, skip);
+    *ds[2] = make_desc(h, U[b], nullptr, nullptr, h->wn, df, nullptr, dt, 0.5, skip);
+    *ds[3] = make_desc(h, U[b], U[b], nullptr, h->Yp, df, nullptr, dt, 0.5, skip);
+    ds[3]->wn = h->wn;
+    for (int k = 0; k < 4; ++k) {
+      ds[k]->tsi_bits = C->tsi_bits;
+      ds[k]->links = dev[k];
+      for (int a = 0; a < 3; ++a)
+        for (int side = 0; side < 2; ++side) ds[k]->nb[a][side] = C->links[b * 6 + a * 2 + side];
+    }
+    ChartBrick& c = C->hcb[b];
+    memset(&c, 0, sizeof(c));
+    c.box = h->box;
+    for (int a = 0; a < 3; ++a)
+      for (int side = 0; side < 2; ++side) c.nb[a][side] = C->links[b * 6 + a * 2 + side];
+    c.U = U[b];
+    c.Pst = h->Pst;
+    c.wn = h->wn;
+    c.sb = h->sb;
+    c.df = h->df;
+    c.v_off = C->total_v;
+    c.c_off = C->total_c;
+    C->total_v += h->box.nV;
+    C->total_c += h->box.nP;
+  }
+  if (C->graph) {
+    cudaGraphExecDestroy(C->graph);
+    C->graph = nullptr;
+  }
+  C->wn_valid = false;
+  return chart_upload_descs(C, nullptr);
+}
+
+int gfx_fluid_chart_from_primitive(gfx_fluid_chart* C, const double* const* prim, void* stream) {
+  if (!C || !prim) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int b = 0; b < C->n; ++b) {
+    if (!prim[b]) return fail(GFX_ERR_ARGUMENT, "brick %d: NULL primitives", b);
+    C->hcb[b].prim = prim[b];
+  }
+  int rc = chart_upload_descs(C, s);
+  if (rc) return rc;
+  chart_from_primitive_kernel<<<grid_for(C->total_v, 256), 256, 0, s>>>(C->cb, C->n,
+                                                                         C->total_v, C->ph);
+  CUDA_TRY(cudaGetLastError());
+  C->launches += 1;
+  for (int b = 0; b < C->n; ++b) C->hcb[b].prim = nullptr;
+  C->prims_pending = true;
+  C->wn_valid = false;
+  C->features = FEAT_ZERO;
+  for (gfx_fluid* h : C->h) CUDA_TRY(cudaMemsetAsync(h->df, 0, (size_t)h->box.nP, s));
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_set_conserved(gfx_fluid_chart* C, void* stream) {
+  if (!C) return fail(GFX_ERR_ARGUMENT, "NULL chart");
+  if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int b = 0; b < C->n; ++b) {
+    gfx_fluid* h = C->h[b];
+    to_primitive_kernel<<<grid_for(h->box.nV, 256), 256, 0, s>>>(h->box, h->ph, C->U[b],
+                                                                  nullptr, nullptr);
+  }
+  CUDA_TRY(cudaGetLastError());
+  C->launches += C->n;
+  C->prims_pending = false;
+  C->wn_valid = false;
+  CUDA_TRY(cudaMemsetAsync(&C->clock[0].done, 0, sizeof(int), s));
+  if (C->hllc) {
+    const int blk = 256;
+    chart_detect_shock_kernel<false><<<grid_for(C->total_c, blk), blk, 0, s>>>(
+        C->cb, C->n, C->total_c, C->ph, nullptr);
+    chart_detect_flags_kernel<<<grid_for(C->total_c, blk), blk, 0, s>>>(C->cb, C->n,
+                                                                        C->total_c, nullptr);
+    CUDA_TRY(cudaGetLastError());
+    C->launches += 2;
+  }
+  C->features = FEAT_VALID;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_timestep(gfx_fluid_chart* C, int i_cycle, double* dt_host, void* stream) {
+  if (!C || !dt_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
+  cudaStream_t s = (cudaStream_t)stream;
+  Clock c;
+  memset(&c, 0, sizeof(c));
+  c.cycle = i_cycle;
+  c.finish = DBL_MAX;
+  c.max_cycle = 0x7fffffff;
+  Clock* dc = C->clock + 1;
+  CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  int rc = chart_initial_dt(C, dc, 0, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  *dt_host = c.dt;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_step(gfx_fluid_chart* C, double dt, double* const* fluence, void* stream) {
+  if (!C) return fail(GFX_ERR_ARGUMENT, "NULL chart");
+  if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (fluence) {
+    for (int b = 0; b < C->n; ++b) {
+      C->hd1[b].fluence = C->hd1p[b].fluence = C->hd1w[b].fluence = C->hd2[b].fluence =
+          fluence[b];
+      if (fluence[b])
+        CUDA_TRY(cudaMemsetAsync(fluence[b], 0, sizeof(double) * 36 * C->h[b]->face_size, s));
+    }
+    int rc = chart_upload_descs(C, s);
+    if (rc) return rc;
+  }
+  chart_set_clock_kernel<<<1, 1, 0, s>>>(C->clock, dt);
+  CUDA_TRY(cudaGetLastError());
+  C->launches += 1;
+  const bool from_wn = C->wn_valid && !C->prims_pending;
+  int rc = enqueue_chart_step(C, C->features == FEAT_PENDING, from_wn, s);
+  if (fluence) {
+    for (int b = 0; b < C->n; ++b)
+      C->hd1[b].fluence = C->hd1p[b].fluence = C->hd1w[b].fluence = C->hd2[b].fluence = nullptr;
+    int rc2 = chart_upload_descs(C, s);
+    if (!rc) rc = rc2;
+  }
+  if (rc) return rc;
+  C->prims_pending = false;
+  C->features = FEAT_PENDING;
+  C->wn_valid = true;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_evolve(gfx_fluid_chart* C, double time, int i_cycle, double finish_time,
+                           int n_cycles_max, double* time_out, int* i_cycle_out, void* stream) {
+  if (!C) return fail(GFX_ERR_ARGUMENT, "NULL chart");
+  if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
+  if (n_cycles_max < 0) return fail(GFX_ERR_ARGUMENT, "n_cycles_max < 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  Clock c;
+  memset(&c, 0, sizeof(c));
+  c.time = time;
+  c.finish = finish_time;
+  c.cycle = i_cycle;
+  c.max_cycle = (int)std::min<long long>(0x7fffffffLL, (long long)i_cycle + n_cycles_max);
+  c.done = !(c.time < c.finish && c.cycle < c.max_cycle);
+  Clock* dc = C->clock;
+  CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+  if (!c.done) {
+    int rc = chart_initial_dt(C, dc, 1, s);
+    if (rc) return rc;
+    // the first cycle eagerly (its features and primitives follow the state)
+    rc = enqueue_chart_step(C, C->features == FEAT_PENDING, C->wn_valid && !C->prims_pending, s);
+    if (rc) return rc;
+    advance_clock_kernel<<<1, 1, 0, s>>>(dc, 1);
+    finalize_dt_kernel<<<1, 1, 0, s>>>(C->ph, C->tsi_bits, dc, 1, 1);
+    CUDA_TRY(cudaGetLastError());
+    C->launches += 2;
+    C->prims_pending = false;
+    C->features = FEAT_PENDING;
+    C->wn_valid = true;
+    if (!C->graph) {
+      cudaStream_t cs;
+      CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      const long long before = C->launches;
+      CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      int rc2 = enqueue_chart_step(C, true, true, cs);
+      advance_clock_kernel<<<1, 1, 0, cs>>>(dc, 1);
+      finalize_dt_kernel<<<1, 1, 0, cs>>>(C->ph, C->tsi_bits, dc, 1, 1);
+      cudaError_t ce = cudaStreamEndCapture(cs, &g);
+      cudaStreamDestroy(cs);
+      C->graph_kernels = C->launches - before + 2;
+      C->launches = before;
+      if (rc2) return rc2;
+      if (ce != cudaSuccess) return fail(GFX_ERR_CUDA, "chart graph capture: %s",
+                                         cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&C->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess)
+        return fail(GFX_ERR_CUDA, "chart graph instantiate: %s", cudaGetErrorString(ce));
+    }
+    if (!C->clock_host) {
+      if (cudaMallocHost(&C->clock_host, 2 * sizeof(Clock)) != cudaSuccess) {
+        C->clock_host = nullptr;
+        return fail(GFX_ERR_NO_MEMORY, "cudaMallocHost of the chart clock");
+      }
+      for (int j = 0; j < 2; ++j)
+        CUDA_TRY(cudaEventCreateWithFlags(&C->chunk_ev[j], cudaEventDisableTiming));
+    }
+    // chunks of cycles, two in flight (as gfx_fluid_evolve)
+    int done_cycles = 1, slot = 0;
+    bool pending = false;
+    const int chunk = 8;
+    while (done_cycles < n_cycles_max) {
+      const int nrep = std::min(chunk, n_cycles_max - done_cycles);
+      for (int r = 0; r < nrep; ++r) CUDA_TRY(cudaGraphLaunch(C->graph, s));
+      C->launches += (long long)nrep * C->graph_kernels;
+      done_cycles += nrep;
+      CUDA_TRY(cudaMemcpyAsync(C->clock_host + slot, dc, sizeof(Clock), cudaMemcpyDeviceToHost,
+                               s));
+      CUDA_TRY(cudaEventRecord(C->chunk_ev[slot], s));
+      if (pending) {
+        CUDA_TRY(cudaEventSynchronize(C->chunk_ev[slot ^ 1]));
+        if (C->clock_host[slot ^ 1].done) break;
+      }
+      pending = true;
+      slot ^= 1;
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (time_out) *time_out = c.time;
+  if (i_cycle_out) *i_cycle_out = c.cycle;
+  return GFX_OK;
+}
+
+int gfx_fluid_chart_kernel_launches(const gfx_fluid_chart* C, long long* count) {
+  if (!C || !count) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  *count = C->launches;
   return GFX_OK;
 }
 

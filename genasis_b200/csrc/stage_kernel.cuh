@@ -46,7 +46,13 @@ __host__ __device__ constexpr int full_ring(bool parab, int ty) {
 }
 
 enum { MODE_INCREMENT = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
-enum { BC_OUTFLOW = 0, BC_REFLECTING = 1, BC_PERIODIC = 2 };
+// BC_NEIGHBOR: a face of a brick inside a chart of several bricks, whose
+// ghost cells are the proper cells of the brick across it (Chart_SLD's ghost
+// exchange, Chart_SLD__Form.f90:131-201); no boundary condition applies there
+enum { BC_OUTFLOW = 0, BC_REFLECTING = 1, BC_PERIODIC = 2, BC_NEIGHBOR = 3 };
+// How a stage launch's work items map to bricks: one brick, a batch of
+// independent bricks, or the bricks of one chart (ghosts across linked faces)
+enum { BAT_SINGLE = 0, BAT_BRICKS = 1, BAT_CHART = 2 };
 
 // Per-axis tables over the ghost-inclusive index t in [0, n + 4) (t = cell + 2).
 struct AxisGeo {
@@ -84,6 +90,12 @@ struct BrickDesc {
   double* wn;            // stage 2: primitives N, V1, V2, V3, E of the new state, compact
                          // (or null)
   int tile_y;            // host side: tile rows of the work list (0 = kTileY)
+  // chart bricks: the brick across each face ([axis][inner, outer]) as an
+  // index into `links`, the descriptors of this stage for every brick of the
+  // chart (-1: no brick, the face's boundary condition applies); the periodic
+  // faces of a chart link its end bricks
+  int nb[3][2];
+  const struct BrickDesc* links;
   int pad_;
   AxisGeo geo[3];
 };
@@ -113,41 +125,92 @@ __device__ __forceinline__ int bc_map(int g, int n, int bc_lo, int bc_hi, bool& 
   return max(0, min(n - 1, s));
 }
 
+// The brick that holds the value at coordinates c (possibly ghosts) of brick
+// B, with c moved into that brick's frame.  Chart bricks (CH) cross the
+// linked faces into the neighbours, one axis after the other, so that an
+// edge ghost lands in the diagonal brick; what stays outside is for the
+// boundary maps.  Every brick of a chart has at least 4 cells per axis and a
+// ghost lies at most 2 cells out, so one crossing per axis suffices.
+template <bool CH>
+__device__ __forceinline__ const BrickDesc& cell_owner(const BrickDesc& B, int* c) {
+  if (!CH) return B;
+  const BrickDesc* S = &B;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int side = c[a] < 0 ? 0 : (c[a] >= S->n[a] ? 1 : -1);
+    if (side >= 0) {
+      const int nbi = S->nb[a][side];
+      if (nbi >= 0) {
+        const BrickDesc* N = B.links + nbi;
+        c[a] += side ? -S->n[a] : N->n[a];
+        S = N;
+      }
+    }
+  }
+  return *S;
+}
+
+// The input value of cell (gx, gy, gz) of brick B: the address of its first
+// field (the stored primitives N, V1, V2, V3, E, compact, for IN_PRIM; else
+// the conserved D, S1, S2, S3, G, ghost layout), the stride between fields
+// and the velocity components the boundary maps reverse (bit d: V_d+1).
+template <bool IN_PRIM, bool CH>
+__device__ __forceinline__ const double* cell_src(const BrickDesc& B, int gx, int gy, int gz,
+                                                  long long& fs, int& flips) {
+  int c[3] = {gx, gy, gz};
+  const BrickDesc& S = cell_owner<CH>(B, c);
+  bool nx, ny, nz;
+  const int sx = bc_map(c[0], S.n[0], S.bc[0][0], S.bc[0][1], nx);
+  const int sy = bc_map(c[1], S.n[1], S.bc[1][0], S.bc[1][1], ny);
+  const int sz = bc_map(c[2], S.n[2], S.bc[2][0], S.bc[2][1], nz);
+  flips = (int)nx | ((int)ny << 1) | ((int)nz << 2);
+  if (IN_PRIM) {
+    fs = S.nP;
+    return S.P_in + (sx + (long long)S.n[0] * (sy + (long long)S.n[1] * sz));
+  }
+  fs = S.nV;
+  return S.U_in + ((sx + 2) + (long long)S.m[0] * ((sy + 2) + (long long)S.m[1] * (sz + 2)));
+}
+
+// The primitives of cell (gx, gy, gz) of brick B (possibly a ghost), after
+// the boundary maps: recovered from the conserved values for a conserved
+// input, with the reversed velocities negated.
+template <bool IN_PRIM, bool CH>
+__device__ __forceinline__ Prim load_prim(const BrickDesc& B, const Phys& ph, int gx, int gy,
+                                          int gz) {
+  long long fs;
+  int flips;
+  const double* p = cell_src<IN_PRIM, CH>(B, gx, gy, gz, fs, flips);
+  Prim w;
+  if (IN_PRIM) {
+    w.N = __ldg(p);
+    w.V1 = __ldg(p + fs);
+    w.V2 = __ldg(p + 2 * fs);
+    w.V3 = __ldg(p + 3 * fs);
+    w.E = __ldg(p + 4 * fs);
+  } else {
+    Cons c;
+    c.D = __ldg(p);
+    c.S1 = __ldg(p + fs);
+    c.S2 = __ldg(p + 2 * fs);
+    c.S3 = __ldg(p + 3 * fs);
+    c.G = __ldg(p + 4 * fs);
+    cons_to_prim(c, w, ph.nmin);
+  }
+  if (flips & 1) w.V1 = -w.V1;
+  if (flips & 2) w.V2 = -w.V2;
+  if (flips & 4) w.V3 = -w.V3;
+  return w;
+}
+
 // Loads the primitives of cell (gx, gy) of plane gz (all possibly ghosts) into
 // a ring plane at local (ly, lx).
-template <bool IN_PRIM, int TYt, int FR>
+template <bool IN_PRIM, int TYt, int FR, bool CH>
 __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, double* plane,
                                           int lx, int ly, int gx, int gy, int gz) {
   GFX_TILE(TYt);
   constexpr int FW = TX + 2 * FR, FS = FW * (TY + 2 * FR);
-  bool nx, ny, nz;
-  const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
-  const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
-  const int sz = bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
-  Prim w;
-  if (IN_PRIM) {
-    const long long o = sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz);
-    const double* p = B.P_in;
-    w.N = __ldg(p + o);
-    w.V1 = __ldg(p + B.nP + o);
-    w.V2 = __ldg(p + 2 * B.nP + o);
-    w.V3 = __ldg(p + 3 * B.nP + o);
-    w.E = __ldg(p + 4 * B.nP + o);
-  } else {
-    const long long o =
-        (sx + 2) + (long long)B.m[0] * ((sy + 2) + (long long)B.m[1] * (sz + 2));
-    const double* u = B.U_in;
-    Cons c;
-    c.D = __ldg(u + o);
-    c.S1 = __ldg(u + B.nV + o);
-    c.S2 = __ldg(u + 2 * B.nV + o);
-    c.S3 = __ldg(u + 3 * B.nV + o);
-    c.G = __ldg(u + 4 * B.nV + o);
-    cons_to_prim(c, w, ph.nmin);
-  }
-  if (nx) w.V1 = -w.V1;
-  if (ny) w.V2 = -w.V2;
-  if (nz) w.V3 = -w.V3;
+  const Prim w = load_prim<IN_PRIM, CH>(B, ph, gx, gy, gz);
   const int o = (ly + FR) * FW + (lx + FR);
   plane[o] = w.N;
   plane[FS + o] = w.V1;
@@ -157,37 +220,10 @@ __device__ __forceinline__ void load_cell(const BrickDesc& B, const Phys& ph, do
 }
 
 // Loads the primitives of one cell into 5 shared slots at stride `stride`.
-template <bool IN_PRIM>
+template <bool IN_PRIM, bool CH>
 __device__ __forceinline__ void load_cell_to(const BrickDesc& B, const Phys& ph, double* dst,
                                              int stride, int gx, int gy, int gz) {
-  bool nx, ny, nz;
-  const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
-  const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
-  const int sz = bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
-  Prim w;
-  if (IN_PRIM) {
-    const long long o = sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz);
-    const double* p = B.P_in;
-    w.N = __ldg(p + o);
-    w.V1 = __ldg(p + B.nP + o);
-    w.V2 = __ldg(p + 2 * B.nP + o);
-    w.V3 = __ldg(p + 3 * B.nP + o);
-    w.E = __ldg(p + 4 * B.nP + o);
-  } else {
-    const long long o =
-        (sx + 2) + (long long)B.m[0] * ((sy + 2) + (long long)B.m[1] * (sz + 2));
-    const double* u = B.U_in;
-    Cons c;
-    c.D = __ldg(u + o);
-    c.S1 = __ldg(u + B.nV + o);
-    c.S2 = __ldg(u + 2 * B.nV + o);
-    c.S3 = __ldg(u + 3 * B.nV + o);
-    c.G = __ldg(u + 4 * B.nV + o);
-    cons_to_prim(c, w, ph.nmin);
-  }
-  if (nx) w.V1 = -w.V1;
-  if (ny) w.V2 = -w.V2;
-  if (nz) w.V3 = -w.V3;
+  const Prim w = load_prim<IN_PRIM, CH>(B, ph, gx, gy, gz);
   dst[0] = w.N;
   dst[stride] = w.V1;
   dst[2 * stride] = w.V2;
@@ -196,11 +232,11 @@ __device__ __forceinline__ void load_cell_to(const BrickDesc& B, const Phys& ph,
 }
 
 // Loads the primitives of one cell into a column slot (5 values at stride NT).
-template <bool IN_PRIM, int TYt>
+template <bool IN_PRIM, int TYt, bool CH>
 __device__ __forceinline__ void load_cell_col(const BrickDesc& B, const Phys& ph, double* dst,
                                               int gx, int gy, int gz) {
   GFX_TILE(TYt);
-  load_cell_to<IN_PRIM>(B, ph, dst, NT, gx, gy, gz);
+  load_cell_to<IN_PRIM, CH>(B, ph, dst, NT, gx, gy, gz);
 }
 
 // Asynchronous 8-byte copies from global to shared memory (cp.async, which
@@ -222,31 +258,24 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // S1, S2, S3, G (ghost layout).  cell_flips: the velocity components the
 // boundary map reverses there (bit d: V_d+1), which finish_cell applies once
 // the copy has landed.
+template <bool CH>
 __device__ __forceinline__ int cell_flips(const BrickDesc& B, int gx, int gy, int gz) {
+  int c[3] = {gx, gy, gz};
+  const BrickDesc& S = cell_owner<CH>(B, c);
   bool nx, ny, nz;
-  bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
-  bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
-  bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
+  bc_map(c[0], S.n[0], S.bc[0][0], S.bc[0][1], nx);
+  bc_map(c[1], S.n[1], S.bc[1][0], S.bc[1][1], ny);
+  bc_map(c[2], S.n[2], S.bc[2][0], S.bc[2][1], nz);
   return (int)nx | ((int)ny << 1) | ((int)nz << 2);
 }
 
-template <bool IN_PRIM>
+template <bool IN_PRIM, bool CH>
 __device__ __forceinline__ void copy_cell_async(const BrickDesc& B, double* dst, int stride,
                                                int gx, int gy, int gz) {
-  bool nx, ny, nz;
-  const int sx = bc_map(gx, B.n[0], B.bc[0][0], B.bc[0][1], nx);
-  const int sy = bc_map(gy, B.n[1], B.bc[1][0], B.bc[1][1], ny);
-  const int sz = bc_map(gz, B.n[2], B.bc[2][0], B.bc[2][1], nz);
-  (void)nx, (void)ny, (void)nz;
-  const double* p;
   long long fs;
-  if (IN_PRIM) {
-    p = B.P_in + (sx + (long long)B.n[0] * (sy + (long long)B.n[1] * sz));
-    fs = B.nP;
-  } else {
-    p = B.U_in + ((sx + 2) + (long long)B.m[0] * ((sy + 2) + (long long)B.m[1] * (sz + 2)));
-    fs = B.nV;
-  }
+  int flips;
+  const double* p = cell_src<IN_PRIM, CH>(B, gx, gy, gz, fs, flips);
+  (void)flips;
 #pragma unroll
   for (int q = 0; q < 5; ++q) cp_async8(dst + q * stride, p + q * fs);
 }
@@ -279,10 +308,29 @@ __device__ __forceinline__ void finish_cell(const Phys& ph, double* dst, int str
   dst[4 * stride] = w.E;
 }
 
+// DIFFUSIVE_FLUX_I bit d of cell (gx, gy, gz).  Outside the brick: the bit
+// of the linked brick's cell (chart bricks), else 0 (the ghost layer of a
+// chart boundary, which ClearBoundary clears).
+template <bool CH>
 __device__ __forceinline__ bool df_bit(const BrickDesc& B, int d, int gx, int gy, int gz) {
   if (B.df == nullptr) return false;
-  if (gx < 0 || gy < 0 || gz < 0 || gx >= B.n[0] || gy >= B.n[1] || gz >= B.n[2]) return false;
+  if (gx < 0 || gy < 0 || gz < 0 || gx >= B.n[0] || gy >= B.n[1] || gz >= B.n[2]) {
+    if (!CH) return false;
+    int c[3] = {gx, gy, gz};
+    const BrickDesc& S = cell_owner<true>(B, c);
+    if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= S.n[0] || c[1] >= S.n[1] ||
+        c[2] >= S.n[2])
+      return false;
+    return (S.df[c[0] + (long long)S.n[0] * (c[1] + (long long)S.n[1] * c[2])] >> d) & 1;
+  }
   return (B.df[gx + (long long)B.n[0] * (gy + (long long)B.n[1] * gz)] >> d) & 1;
+}
+
+// Whether face `side` of axis a records the boundary fluence: every face of
+// a single brick, only the chart's own boundary for a chart brick
+// (RecordBoundaryFluence_CSL, IncrementDivergence_FV__Form.f90:1002-1069).
+__device__ __forceinline__ bool records_fluence(const BrickDesc& B, int a, int side) {
+  return B.bc[a][side] != BC_NEIGHBOR;
 }
 
 template <int NF>
@@ -323,17 +371,17 @@ __device__ __forceinline__ void boundary_fluence(const BrickDesc& B, const Phys&
                                                  const double* l, const double* r,
                                                  bool diffusive, const double* F, int face,
                                                  int a, int na, int b, double factor) {
-  if (NF == 6) {
+  if constexpr (NF == 6) {
     record_fluence<6>(B, face, a, na, b, F, factor);
-    return;
-  }
-  FacePrims p;
+  } else {
+    FacePrims p;
 #pragma unroll
-  for (int v = 0; v < 5; ++v) {
-    p.l[v] = l[v];
-    p.r[v] = r[v];
+    for (int v = 0; v < 5; ++v) {
+      p.l[v] = l[v];
+      p.r[v] = r[v];
+    }
+    boundary_fluence6<D, HLLC>(B, ph, p, diffusive, face, a, na, b, factor);
   }
-  boundary_fluence6<D, HLLC>(B, ph, p, diffusive, face, a, na, b, factor);
 }
 
 // Relabels the velocity and momentum components of a face state so that
@@ -437,21 +485,22 @@ __device__ __forceinline__ void z_slope(const AxisGeo& GZ, const Phys& ph, int p
 
 // Flux through the z face between planes p-1 (values a, slopes sm_) and p
 // (values b, slopes sp) of the own column (gx, gy), with its boundary fluence.
-template <bool HLLC, int NF>
+template <bool HLLC, int NF, bool CH>
 __device__ __forceinline__ void z_face_lr(const BrickDesc& B, const Phys& ph, int p,
                                           const double* l, const double* r, int gx, int gy,
                                           bool own, double dt, double* F) {
   FaceState L, R;
   face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
   face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
-  const bool diff = HLLC && df_bit(B, 2, gx, gy, p);
+  const bool diff = HLLC && df_bit<CH>(B, 2, gx, gy, p);
   riemann_flux<2, HLLC, NF>(L, R, diff, F);
-  if (own && (p == 0 || p == B.n[2]) && B.fluence)
+  if (own && (p == 0 || p == B.n[2]) && B.fluence &&
+      (!CH || records_fluence(B, 2, p == 0 ? 0 : 1)))
     boundary_fluence<2, HLLC, NF>(B, ph, l, r, diff, F, p == 0 ? 4 : 5, gx, B.n[0], gy,
                                   B.weight * dt);
 }
 
-template <bool HLLC, int NF>
+template <bool HLLC, int NF, bool CH>
 __device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p,
                                        const double* a, int sa, const double* sm_, int ssm,
                                        const double* b, int sb, const double* sp, int ssp,
@@ -460,7 +509,7 @@ __device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p
   double l[5], r[5];
   face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2), l,
              r);
-  z_face_lr<HLLC, NF>(B, ph, p, l, r, gx, gy, own, dt, F);
+  z_face_lr<HLLC, NF, CH>(B, ph, p, l, r, gx, gy, own, dt, F);
 }
 
 // PARABOLIC: inner and outer face values of the 5 primitives of the own
@@ -484,7 +533,7 @@ __device__ __forceinline__ void z_parabolic(const BrickDesc& B, int p, const dou
 // cache of the plane loop.
 // PARABOLIC (PARAB): zss keeps the outer face values of plane z0 instead of
 // its slopes.
-template <bool IN_PRIM, bool HLLC, int NF, bool PARAB, int TYt>
+template <bool IN_PRIM, bool HLLC, int NF, bool PARAB, int TYt, bool CH>
 __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, double* full,
                                             double* cen, double* zss, double* zfs, int tid,
                                             int tx, int ty, int gx, int gy, int z0, bool own,
@@ -493,24 +542,24 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
   constexpr int FR = full_ring(PARAB, TYt), FW = TX + 2 * FR, FS = FW * (TY + 2 * FR);
   auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
   double* fc = full + (ty + FR) * FW + (tx + FR);
-  load_cell<IN_PRIM, TYt, FR>(B, ph, full, tx, ty, gx, gy, z0 - 2);
-  load_cell_col<IN_PRIM, TYt>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
-  load_cell_col<IN_PRIM, TYt>(B, ph, cslot(z0), gx, gy, z0);
+  load_cell<IN_PRIM, TYt, FR, CH>(B, ph, full, tx, ty, gx, gy, z0 - 2);
+  load_cell_col<IN_PRIM, TYt, CH>(B, ph, cslot(z0 - 1), gx, gy, z0 - 1);
+  load_cell_col<IN_PRIM, TYt, CH>(B, ph, cslot(z0), gx, gy, z0);
   double s_m[5], s_0[5], vI0[5];
   if (PARAB)
     z_parabolic(B, z0 - 1, fc, FS, cslot(z0 - 1), NT, cslot(z0), NT, vI0, s_m);
   else
     z_slope(B.geo[2], ph, z0 - 1, fc, FS, cslot(z0 - 1), NT, cslot(z0), NT, s_m);
-  load_cell<IN_PRIM, TYt, FR>(B, ph, full, tx, ty, gx, gy, z0 + 1);
+  load_cell<IN_PRIM, TYt, FR, CH>(B, ph, full, tx, ty, gx, gy, z0 + 1);
   if (PARAB)
     z_parabolic(B, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, FS, vI0, s_0);
   else
     z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, FS, s_0);
   double F[NF];
   if (PARAB)
-    z_face_lr<HLLC, NF>(B, ph, z0, s_m, vI0, gx, gy, own, dt, F);
+    z_face_lr<HLLC, NF, CH>(B, ph, z0, s_m, vI0, gx, gy, own, dt, F);
   else
-    z_face<HLLC, NF>(B, ph, z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, gx, gy, own,
+    z_face<HLLC, NF, CH>(B, ph, z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, gx, gy, own,
                      dt, F);
 #pragma unroll
   for (int q = 0; q < 5; ++q) zss[q * NT + tid] = s_0[q];
@@ -527,7 +576,7 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
 // brick (read from the constant bank).
 // PARAB: PARABOLIC reconstruction (single bricks): no slope phase; each face
 // reconstructs its two cells, the own column carries outer face values in z.
-template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, bool BATCHED, bool PARAB = false,
+template <int MODE, bool IN_PRIM, bool HLLC, bool GRAV, int NF, int BAT, bool PARAB = false,
           int TYt = kTileY>
 __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
     stage_kernel(const __grid_constant__ BrickDesc single, const BrickDesc* __restrict__ many,
@@ -559,6 +608,8 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int c_off = (ty + FR) * FW + (tx + FR);  // own cell in the full plane
+  constexpr bool BATCHED = BAT != BAT_SINGLE;
+  constexpr bool CH = BAT == BAT_CHART;
   const BrickDesc& B = BATCHED ? s_desc : single;
 
   for (;;) {
@@ -593,7 +644,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
     // (centre slots) or FS (full plane)
     auto cslot = [&](int p) { return cen + (p & 1) * 5 * NT + tid; };
     // ---- prologue (own column only): slopes at z0-1, z0 and the face z0 ----
-    stage_prologue<IN_PRIM, HLLC, NF, PARAB, TYt>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx,
+    stage_prologue<IN_PRIM, HLLC, NF, PARAB, TYt, CH>(B, ph, full, cen, zss, zfs, tid, tx, ty, gx,
                                                   gy, z0, own, dt);
     // the halo cell of this thread (threads below NH): two rows below and
     // above the tile, two columns left and right; hbuf holds its primitives
@@ -659,11 +710,11 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         out[q * NHS] = limited_slope(a[q * sa], b[q * sb], c[q * sc], dxl, dxr, sql, sqr, cden,
                                      rdxl, rdxr, rcden, ph.theta, ph.use_limiter);
     };
-    if (tid < NH) copy_cell_async<IN_PRIM>(B, hbuf + tid, NH, x0 + hx, y0 + hy, z0);
+    if (tid < NH) copy_cell_async<IN_PRIM, CH>(B, hbuf + tid, NH, x0 + hx, y0 + hy, z0);
     cp_async_commit();
     cp_async_wait_all();
     if (tid < NH)
-      finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips(B, x0 + hx, y0 + hy, z0));
+      finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips<CH>(B, x0 + hx, y0 + hy, z0));
     __syncthreads();  // geometry caches, the halo of plane z0, the own centres
     if (HS) {
       if (tid < NHS) halo_slope(tid, z0);
@@ -679,14 +730,15 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
 #pragma unroll
         for (int q = 0; q < 5; ++q) full[q * FS + c_off] = src[q * NT];
       }
-      copy_cell_async<IN_PRIM>(B, cslot(k + 2), NT, gx, gy, k + 2);
+      copy_cell_async<IN_PRIM, CH>(B, cslot(k + 2), NT, gx, gy, k + 2);
       if (tid < NH) {
         if (hx >= -FR && hx < TX + FR && hy >= -FR && hy < TY + FR) {  // in the ring
           const int o = (hy + FR) * FW + (hx + FR);
 #pragma unroll
           for (int q = 0; q < 5; ++q) full[q * FS + o] = hbuf[q * NH + tid];
         }
-        if (k + 1 < z1) copy_cell_async<IN_PRIM>(B, hbuf + tid, NH, x0 + hx, y0 + hy, k + 1);
+        if (k + 1 < z1)
+          copy_cell_async<IN_PRIM, CH>(B, hbuf + tid, NH, x0 + hx, y0 + hy, k + 1);
       }
       cp_async_commit();
       __syncthreads();
@@ -707,9 +759,9 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       // k+1) have landed and become primitives; the barrier shows them to
       // the CTA
       cp_async_wait_all();
-      finish_cell<IN_PRIM>(ph, cslot(k + 2), NT, cell_flips(B, gx, gy, k + 2));
+      finish_cell<IN_PRIM>(ph, cslot(k + 2), NT, cell_flips<CH>(B, gx, gy, k + 2));
       if (tid < NH && k + 1 < z1)
-        finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips(B, x0 + hx, y0 + hy, k + 1));
+        finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips<CH>(B, x0 + hx, y0 + hy, k + 1));
       __syncthreads();
 
       // (3) faces: x [TY][TX+1], y [TY+1][TX] of plane k, one code path for
@@ -772,7 +824,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             to_normal_frame_y(L);
             to_normal_frame_y(R);
           }
-          const bool diff = HLLC && df_bit(B, isx ? 0 : 1, cx, cy, k);
+          const bool diff = HLLC && df_bit<CH>(B, isx ? 0 : 1, cx, cy, k);
           double F[NF];
           riemann_flux<0, HLLC, NF>(L, R, diff, F);
           if (!isx) {
@@ -784,7 +836,9 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
           const int ostride = isx ? TY * (TX + 1) : (TY + 1) * TX;
 #pragma unroll
           for (int u = 0; u < NF; ++u) out[u * ostride] = F[u];
-          if (B.fluence && (isx ? (cx == 0 || cx == n0) : (cy == 0 || cy == n1))) {
+          if (B.fluence && (isx ? (cx == 0 || cx == n0) : (cy == 0 || cy == n1)) &&
+              (!CH || records_fluence(B, isx ? 0 : 1,
+                                      isx ? (cx == 0 ? 0 : 1) : (cy == 0 ? 0 : 1)))) {
             if (isx)
               boundary_fluence<0, HLLC, NF>(B, ph, l, r, diff, F, cx == 0 ? 0 : 1, cy, n1, k,
                                             factor);
@@ -811,10 +865,10 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         z_parabolic(B, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zI, zsn);
 #pragma unroll
         for (int q = 0; q < 5; ++q) zl[q] = zss[q * NT + tid];
-        z_face_lr<HLLC, NF>(B, ph, k + 1, zl, zI, gx, gy, own, dt, zfn);
+        z_face_lr<HLLC, NF, CH>(B, ph, k + 1, zl, zI, gx, gy, own, dt, zfn);
       } else {
         z_slope(GZ, ph, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
-        z_face<HLLC, NF>(B, ph, k + 1, full + c_off, FS, zss + tid, NT, cslot(k + 1), NT, zsn,
+        z_face<HLLC, NF, CH>(B, ph, k + 1, full + c_off, FS, zss + tid, NT, cslot(k + 1), NT, zsn,
                          1, gx, gy, own, dt, zfn);
       }
       __syncthreads();

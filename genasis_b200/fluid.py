@@ -40,28 +40,34 @@ def _ptr(t):
 class FluidBox:
     """One brick of Fluid_P_I on the current CUDA device."""
 
-    def __init__(self, config: FluidConfig, device=None):
+    def __init__(self, config: FluidConfig, device=None, variant=None):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("FluidBox needs a CUDA device (there is no CPU path)")
         self.config = config
         self.device = torch.device(device) if device is not None else torch.device("cuda")
+        # the library build ("exact" or "fast", genasis_b200.lib) of this brick
+        self.variant = variant or lib.default_variant()
         self._c = config.to_c()
         h = ctypes.c_void_p()
-        lib.call("gfx_fluid_create", ctypes.byref(self._c), ctypes.byref(h))
+        self.call("gfx_fluid_create", ctypes.byref(self._c), ctypes.byref(h))
         self.h = h
         n = ctypes.c_size_t()
-        lib.call("gfx_fluid_n_values", self.h, ctypes.byref(n))
+        self.call("gfx_fluid_n_values", self.h, ctypes.byref(n))
         self.n_values = int(n.value)
         fs = ctypes.c_size_t()
-        lib.call("gfx_fluid_fluence_face_size", self.h, ctypes.byref(fs))
+        self.call("gfx_fluid_fluence_face_size", self.h, ctypes.byref(fs))
         self.face_size = int(fs.value)
         self.U = torch.zeros((6,) + config.shape, dtype=torch.float64, device=self.device)
+
+    def call(self, name, *args):
+        """An entry point of this brick's library."""
+        return lib.call(name, *args, variant=self.variant)
 
     # -- lifetime ------------------------------------------------------------
     def close(self):
         if getattr(self, "h", None):
-            lib.load().gfx_fluid_destroy(self.h)
+            lib.load(self.variant).gfx_fluid_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -74,7 +80,7 @@ class FluidBox:
     def geometry(self, axis):
         m = int(self.config.n_cells[axis]) + 2 * int(self.config.n_ghost_layers)
         c, wl, wr = (np.zeros(m) for _ in range(3))
-        lib.call("gfx_fluid_geometry", self.h, axis, c.ctypes.data_as(ctypes.c_void_p),
+        self.call("gfx_fluid_geometry", self.h, axis, c.ctypes.data_as(ctypes.c_void_p),
                  wl.ctypes.data_as(ctypes.c_void_p), wr.ctypes.data_as(ctypes.c_void_p))
         return c, wl, wr
 
@@ -86,7 +92,7 @@ class FluidBox:
         p = torch.as_tensor(np.ascontiguousarray(prim) if isinstance(prim, np.ndarray) else prim,
                             dtype=torch.float64, device=self.device).contiguous()
         assert tuple(p.shape) == (5,) + self.config.shape
-        lib.call("gfx_fluid_from_primitive", self.h, _ptr(p), _ptr(self.U), _stream())
+        self.call("gfx_fluid_from_primitive", self.h, _ptr(p), _ptr(self.U), _stream())
         return self.U
 
     def set_conserved(self, U):
@@ -94,7 +100,7 @@ class FluidBox:
         (floors, DS), so that the next step starts from these values."""
         torch = _torch()
         self.U.copy_(torch.as_tensor(U, dtype=torch.float64))
-        lib.call("gfx_fluid_to_primitive", self.h, _ptr(self.U), None, None, _stream())
+        self.call("gfx_fluid_to_primitive", self.h, _ptr(self.U), None, None, _stream())
         return self.U
 
     def compute_from_conserved(self, detect_features=False, primitive=False, aux=False):
@@ -105,22 +111,22 @@ class FluidBox:
                            device=self.device) if primitive else None
         ax = torch.empty((3,) + self.config.shape, dtype=torch.float64,
                          device=self.device) if aux else None
-        lib.call("gfx_fluid_to_primitive", self.h, _ptr(self.U), _ptr(prim), _ptr(ax), _stream())
+        self.call("gfx_fluid_to_primitive", self.h, _ptr(self.U), _ptr(prim), _ptr(ax), _stream())
         if detect_features:
             self.detect_features()
         return prim, ax
 
     def detect_features(self):
-        lib.call("gfx_fluid_detect_features", self.h, _ptr(self.U), _stream())
+        self.call("gfx_fluid_detect_features", self.h, _ptr(self.U), _stream())
 
     def clear_features(self):
-        lib.call("gfx_fluid_clear_features", self.h, _stream())
+        self.call("gfx_fluid_clear_features", self.h, _stream())
 
     def features(self):
         """DIFFUSIVE_FLUX_I bits (bit d = direction d) over every value."""
         torch = _torch()
         f = torch.zeros(self.config.shape, dtype=torch.uint8, device=self.device)
-        lib.call("gfx_fluid_get_features", self.h, _ptr(f), _stream())
+        self.call("gfx_fluid_get_features", self.h, _ptr(f), _stream())
         return f
 
     def new_fluence(self):
@@ -129,31 +135,31 @@ class FluidBox:
 
     # -- increment, step, time step --------------------------------------------
     def increment(self, K, time_step, weight_rk=1.0, fluence=None):
-        lib.call("gfx_fluid_increment", self.h, _ptr(self.U), _ptr(K), float(time_step),
+        self.call("gfx_fluid_increment", self.h, _ptr(self.U), _ptr(K), float(time_step),
                  float(weight_rk), _ptr(fluence), _stream())
         return K
 
     def step(self, time_step, fluence=None):
-        lib.call("gfx_fluid_step", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
+        self.call("gfx_fluid_step", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
                  _stream())
 
     def step_host(self, U_host, time_step, fluence_host=None):
         """One step on a host (ideally pinned) tensor: copy in, step, copy out."""
-        lib.call("gfx_fluid_step_host", self.h, _ptr(U_host), float(time_step),
+        self.call("gfx_fluid_step_host", self.h, _ptr(U_host), float(time_step),
                  _ptr(fluence_host))
 
     def step_timed(self, time_step, fluence=None):
         """One step with CUDA events around each launch; returns the device
         milliseconds of (features, stage 1, stage 2, ghost refresh)."""
         ms = (ctypes.c_double * 4)()
-        lib.call("gfx_fluid_step_timed", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
+        self.call("gfx_fluid_step_timed", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
                  ms, _stream())
         return tuple(ms)
 
     def set_tuning(self, z_chunk=0, adjoint_segment=0, tile_rows=0):
         """Speed knobs that leave results unchanged (genasis_b200.autotune):
         pencil length, adjoint sweep segment, tile rows (8 or 16)."""
-        lib.call("gfx_fluid_set_tuning", self.h, int(z_chunk), int(adjoint_segment),
+        self.call("gfx_fluid_set_tuning", self.h, int(z_chunk), int(adjoint_segment),
                  int(tile_rows))
         self.tuning = (int(z_chunk), int(adjoint_segment), int(tile_rows))
 
@@ -161,30 +167,30 @@ class FluidBox:
         """sum U dV over the proper cells for the six conserved fields
         (the conservation tallies), as a numpy array."""
         out = np.zeros(6)
-        lib.call("gfx_fluid_totals", self.h, _ptr(self.U if U is None else U),
+        self.call("gfx_fluid_totals", self.h, _ptr(self.U if U is None else U),
                  out.ctypes.data_as(ctypes.c_void_p), _stream())
         return out
 
     def check_state(self, U=None):
         """Raises GfxError (GFX_ERR_STATE) if a proper cell of U (default: the
         box's state) holds a non-finite value."""
-        lib.call("gfx_fluid_check_state", self.h, _ptr(self.U if U is None else U), _stream())
+        self.call("gfx_fluid_check_state", self.h, _ptr(self.U if U is None else U), _stream())
 
     def kernel_launches(self):
         n = ctypes.c_longlong()
-        lib.call("gfx_fluid_kernel_launches", self.h, ctypes.byref(n))
+        self.call("gfx_fluid_kernel_launches", self.h, ctypes.byref(n))
         return int(n.value)
 
     def compute_time_step(self, i_cycle=0):
         dt = ctypes.c_double()
-        lib.call("gfx_fluid_timestep", self.h, _ptr(self.U), int(i_cycle), ctypes.byref(dt),
+        self.call("gfx_fluid_timestep", self.h, _ptr(self.U), int(i_cycle), ctypes.byref(dt),
                  _stream())
         return dt.value
 
     def evolve(self, finish_time, time=0.0, i_cycle=0, max_cycles=2**31 - 1):
         t = ctypes.c_double()
         c = ctypes.c_int()
-        lib.call("gfx_fluid_evolve", self.h, _ptr(self.U), float(time), int(i_cycle),
+        self.call("gfx_fluid_evolve", self.h, _ptr(self.U), float(time), int(i_cycle),
                  float(finish_time), int(max_cycles), ctypes.byref(t), ctypes.byref(c),
                  _stream())
         return t.value, c.value

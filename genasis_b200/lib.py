@@ -1,14 +1,22 @@
 """ctypes binding of libgfx_fluid.so (the C ABI of include/gfx_fluid.h).
 
 The library is the only compute path: if it is missing or cannot load, every
-entry point raises; there is no CPU fallback."""
+entry point raises; there is no CPU fallback.
+
+Two builds of the same C ABI exist (genasis_b200/build_ext.py): "exact"
+(libgfx_fluid.so, the reference's rounding) and "fast"
+(libgfx_fluid_fast.so, fused multiply-adds and products with reciprocals,
+within 1e-12 per step of the exact one).  Every call names its variant;
+without one it takes GFX_FLUID_VARIANT from the environment, else "exact".
+A handle belongs to the library that created it."""
 import ctypes
 import os
 
 from .config import GfxConfig
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgfx_fluid.so")
+LIB_FILES = {"exact": "libgfx_fluid.so", "fast": "libgfx_fluid_fast.so"}
+LIB_PATH = os.path.join(_HERE, LIB_FILES["exact"])
 
 GFX_OK = 0
 STATUS = {
@@ -56,10 +64,21 @@ SIGNATURES = {
     "gfx_fluid_set_tuning": [P, I, I, I],
     "gfx_fluid_totals": [P, P, P, P],
     "gfx_fluid_resume": [P, P],
+    "gfx_fluid_chart_create": [ctypes.POINTER(GfxConfig), ctypes.POINTER(I), ctypes.POINTER(P)],
+    "gfx_fluid_chart_destroy": [P],
+    "gfx_fluid_chart_n_bricks": [P, ctypes.POINTER(I)],
+    "gfx_fluid_chart_brick": [P, I, ctypes.POINTER(P), ctypes.POINTER(I)],
+    "gfx_fluid_chart_bind": [P, P],
+    "gfx_fluid_chart_from_primitive": [P, P, P],
+    "gfx_fluid_chart_set_conserved": [P, P],
+    "gfx_fluid_chart_timestep": [P, I, ctypes.POINTER(D), P],
+    "gfx_fluid_chart_step": [P, D, P, P],
+    "gfx_fluid_chart_evolve": [P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I), P],
+    "gfx_fluid_chart_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
     "gfx_fluid_last_error": [ctypes.c_char_p, SZ],
 }
 
-_lib = None
+_libs = {}
 
 
 class GfxError(RuntimeError):
@@ -68,35 +87,48 @@ class GfxError(RuntimeError):
         self.status = status
 
 
-def load():
-    """Loads the in-tree library (raises if it is absent)."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
+def default_variant():
+    v = os.environ.get("GFX_FLUID_VARIANT", "exact")
+    if v not in LIB_FILES:
+        raise ValueError("GFX_FLUID_VARIANT=%r: expected one of %s" % (v, sorted(LIB_FILES)))
+    return v
+
+
+def lib_path(variant=None):
+    return os.path.join(_HERE, LIB_FILES[variant or default_variant()])
+
+
+def load(variant=None):
+    """Loads the in-tree library of the variant (raises if it is absent)."""
+    variant = variant or default_variant()
+    if variant in _libs:
+        return _libs[variant]
+    path = lib_path(variant)
+    if not os.path.exists(path):
         raise RuntimeError(
-            "libgfx_fluid.so is not built (run genasis_b200/build_ext.py or "
-            "__graft_entry__.build()); there is no fallback path")
-    lib = ctypes.CDLL(LIB_PATH)
+            "%s is not built (run genasis_b200/build_ext.py or __graft_entry__.build()); "
+            "there is no fallback path" % os.path.basename(path))
+    lib = ctypes.CDLL(path)
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int
         fn.argtypes = args
-    _lib = lib
+    _libs[variant] = lib
     return lib
 
 
-def last_error():
+def last_error(variant=None):
     buf = ctypes.create_string_buffer(1024)
-    load().gfx_fluid_last_error(buf, len(buf))
+    load(variant).gfx_fluid_last_error(buf, len(buf))
     return buf.value.decode(errors="replace")
 
 
-def call(name, *args):
-    """Calls an entry point and raises GfxError on a nonzero status."""
-    rc = getattr(load(), name)(*args)
+def call(name, *args, variant=None):
+    """Calls an entry point of the variant's library and raises GfxError on
+    a nonzero status."""
+    rc = getattr(load(variant), name)(*args)
     if rc != GFX_OK:
-        raise GfxError(rc, name, last_error())
+        raise GfxError(rc, name, last_error(variant))
     return rc
 
 

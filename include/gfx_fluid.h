@@ -187,6 +187,58 @@ int gfx_fluid_batch_clocks(gfx_fluid_batch *b, double *time_host, int *cycle_hos
                            void *stream);
 int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch *b, long long *count);
 
+/* ---- A chart of several bricks --------------------------------------------
+ * Chart_SLD (Chart_SLD__Form.f90, Chart_Template.f90:440-460): one domain
+ * (cfg: the whole chart, n_cells its cells per axis) split into n_bricks[0] x
+ * n_bricks[1] x n_bricks[2] equal bricks of n_cells / n_bricks cells (which
+ * must divide evenly, at least 4 per axis), brick b = ix + nx (iy + ny iz).
+ * The reference runs one brick per MPI rank and exchanges the ghost layers of
+ * faces and edges between them each stage (ExchangeGhostData,
+ * Chart_SLD__Form.f90:131-201, from Step_RK_C_ASC__Template.f90:1237-1246);
+ * here all bricks share one device, and a stage reads a neighbour's cells
+ * where they live.  Each brick's geometry is the slice of the chart's
+ * (SetGeometryWidthCenter, Chart_SLD__Form.f90:273-320); the shock features
+ * see across brick faces and ClearBoundary applies on the chart's boundary
+ * only (FluidFeatures_P__Form.f90:313-336); the boundary fluence is recorded
+ * on the chart's boundary faces only (IncrementDivergence_FV__Form.f90:
+ * 1002-1069); the time step is the minimum over the chart (the MIN all-reduce
+ * of Integrator_Template.f90:919).  The results on every cell are those of
+ * one brick of the whole chart, bit for bit.  LINEAR reconstruction.
+ *
+ * gfx_fluid_chart_brick gives a brick's handle (for gfx_fluid_n_values,
+ * gfx_fluid_geometry, gfx_fluid_fluence_face_size, gfx_fluid_totals,
+ * gfx_fluid_get_features (the flags the chart last detected),
+ * gfx_fluid_check_state; the step entry points of a single brick refuse it)
+ * and its brick coordinates.  gfx_fluid_chart_bind gives the bricks' states
+ * ([6][nV] each, caller-owned device arrays); the other calls act on them. */
+typedef struct gfx_fluid_chart gfx_fluid_chart;
+int gfx_fluid_chart_create(const gfx_fluid_config *cfg, const int n_bricks[3],
+                           gfx_fluid_chart **out);
+int gfx_fluid_chart_destroy(gfx_fluid_chart *c);
+int gfx_fluid_chart_n_bricks(const gfx_fluid_chart *c, int *n);
+int gfx_fluid_chart_brick(gfx_fluid_chart *c, int brick, gfx_fluid **handle,
+                          int brick_index[3]);
+int gfx_fluid_chart_bind(gfx_fluid_chart *c, double *const *U_dev);
+/* ComputeFromPrimitive of every brick from prim_dev[b] ([5][nV] of brick b,
+ * ghosts included); a ghost that the exchange reaches takes the primitives of
+ * the cell it images (Integrator_C_PS__Form.f90:194-203). */
+int gfx_fluid_chart_from_primitive(gfx_fluid_chart *c, const double *const *prim_dev,
+                                   void *stream);
+/* ComputeFromConserved on every value of every brick (floors, DS), then
+ * FluidFeatures_P % Detect over the chart: the state set from conserved
+ * values, as gfx_fluid_to_primitive and gfx_fluid_detect_features leave a
+ * brick. */
+int gfx_fluid_chart_set_conserved(gfx_fluid_chart *c, void *stream);
+int gfx_fluid_chart_timestep(gfx_fluid_chart *c, int i_cycle, double *dt_host, void *stream);
+/* One RK2 step of every brick; fluence_dev (may be NULL) holds one array per
+ * brick ([6][6][face_size of the brick]), cleared and filled on the chart's
+ * boundary faces. */
+int gfx_fluid_chart_step(gfx_fluid_chart *c, double dt, double *const *fluence_dev,
+                         void *stream);
+int gfx_fluid_chart_evolve(gfx_fluid_chart *c, double time, int i_cycle, double finish_time,
+                           int n_cycles_max, double *time_out, int *i_cycle_out, void *stream);
+int gfx_fluid_chart_kernel_launches(const gfx_fluid_chart *c, long long *count);
+
 /* ---- Discrete adjoint of one step -----------------------------------------
  * No counterpart in the reference (which has no adjoint); it is the reverse
  * mode of gfx_fluid_step, with dt held fixed.  Given lam_np1_dev ([6][nV],
@@ -224,9 +276,11 @@ int gfx_fluid_step_adjoint(gfx_fluid *h, const double *U_n_dev, double dt,
  * library, which every GPU that loads the library holds until exit.  That
  * bounds the brick at about 81 bytes per proper cell plus the chart tables
  * (37^3 proper cells fit, 38^3 do not); larger bricks get GFX_ERR_ARGUMENT.
- * The first call on a device looks up the array's device address (and sets
- * up the stage kernels' launch attributes if no step ran before); make that
- * first call before any stream capture.  Every call uses the same array: each
+ * Every call looks up the array's device address on the current device (the
+ * first call on a device also loads the library's kernels there and sets up
+ * the stage kernels' launch attributes for that device, if no step ran on it
+ * before); make that first call before any stream capture.  Each device that
+ * calls it has its own copy of the array.  Every call uses the same array: each
  * call rewrites what it reads and zeroes its CFL word and work counters, so
  * calls in sequence are independent, but calls that overlap on the GPU (on
  * different streams or threads) race on the array and give wrong results. */

@@ -65,7 +65,11 @@ module GFX_Fluid_C
     gfx_fluid_batch_set_clocks, gfx_fluid_batch_evolve, &
     gfx_fluid_batch_clocks, gfx_fluid_batch_kernel_launches, &
     gfx_fluid_step_noalloc, gfx_fluid_check_state, gfx_fluid_totals, &
-    gfx_fluid_resume, gfx_fluid_last_error
+    gfx_fluid_resume, gfx_fluid_chart_create, gfx_fluid_chart_destroy, &
+    gfx_fluid_chart_n_bricks, gfx_fluid_chart_brick, gfx_fluid_chart_bind, &
+    gfx_fluid_chart_from_primitive, gfx_fluid_chart_set_conserved, &
+    gfx_fluid_chart_timestep, gfx_fluid_chart_step, gfx_fluid_chart_evolve, &
+    gfx_fluid_chart_kernel_launches, gfx_fluid_last_error
 
   interface
 
@@ -266,6 +270,92 @@ module GFX_Fluid_C
       type ( c_ptr ), value :: Batch
       integer ( c_long_long ), intent ( out ) :: Count
     end function gfx_fluid_batch_kernel_launches
+
+    !-- A chart of several bricks on one device (Chart_SLD's bricks)
+
+    integer ( c_int ) function gfx_fluid_chart_create ( Config, nBricks, Chart ) &
+      bind ( c, name = 'gfx_fluid_chart_create' )
+      import
+      type ( GFX_FluidConfig ), intent ( in ) :: Config
+      integer ( c_int ), intent ( in ) :: nBricks ( 3 )
+      type ( c_ptr ), intent ( out ) :: Chart
+    end function gfx_fluid_chart_create
+
+    integer ( c_int ) function gfx_fluid_chart_destroy ( Chart ) &
+      bind ( c, name = 'gfx_fluid_chart_destroy' )
+      import
+      type ( c_ptr ), value :: Chart
+    end function gfx_fluid_chart_destroy
+
+    integer ( c_int ) function gfx_fluid_chart_n_bricks ( Chart, nBricks ) &
+      bind ( c, name = 'gfx_fluid_chart_n_bricks' )
+      import
+      type ( c_ptr ), value :: Chart
+      integer ( c_int ), intent ( out ) :: nBricks
+    end function gfx_fluid_chart_n_bricks
+
+    integer ( c_int ) function gfx_fluid_chart_brick ( Chart, iBrick, Handle, iaBrick ) &
+      bind ( c, name = 'gfx_fluid_chart_brick' )
+      import
+      type ( c_ptr ), value :: Chart
+      integer ( c_int ), value :: iBrick
+      type ( c_ptr ), intent ( out ) :: Handle
+      integer ( c_int ), intent ( out ) :: iaBrick ( 3 )
+    end function gfx_fluid_chart_brick
+
+    integer ( c_int ) function gfx_fluid_chart_bind ( Chart, Conserved_dev ) &
+      bind ( c, name = 'gfx_fluid_chart_bind' )
+      import
+      type ( c_ptr ), value :: Chart
+      type ( c_ptr ), intent ( in ) :: Conserved_dev ( * )
+    end function gfx_fluid_chart_bind
+
+    integer ( c_int ) function gfx_fluid_chart_from_primitive ( Chart, Primitive_dev, Stream ) &
+      bind ( c, name = 'gfx_fluid_chart_from_primitive' )
+      import
+      type ( c_ptr ), value :: Chart, Stream
+      type ( c_ptr ), intent ( in ) :: Primitive_dev ( * )
+    end function gfx_fluid_chart_from_primitive
+
+    integer ( c_int ) function gfx_fluid_chart_set_conserved ( Chart, Stream ) &
+      bind ( c, name = 'gfx_fluid_chart_set_conserved' )
+      import
+      type ( c_ptr ), value :: Chart, Stream
+    end function gfx_fluid_chart_set_conserved
+
+    integer ( c_int ) function gfx_fluid_chart_timestep ( Chart, iCycle, TimeStep, Stream ) &
+      bind ( c, name = 'gfx_fluid_chart_timestep' )
+      import
+      type ( c_ptr ), value :: Chart, Stream
+      integer ( c_int ), value :: iCycle
+      real ( c_double ), intent ( out ) :: TimeStep
+    end function gfx_fluid_chart_timestep
+
+    integer ( c_int ) function gfx_fluid_chart_step ( Chart, TimeStep, Fluence_dev, Stream ) &
+      bind ( c, name = 'gfx_fluid_chart_step' )
+      import
+      type ( c_ptr ), value :: Chart, Stream
+      real ( c_double ), value :: TimeStep
+      type ( c_ptr ), intent ( in ) :: Fluence_dev ( * )
+    end function gfx_fluid_chart_step
+
+    integer ( c_int ) function gfx_fluid_chart_evolve &
+      ( Chart, Time, iCycle, FinishTime, nCyclesMax, Time_out, iCycle_out, Stream ) &
+      bind ( c, name = 'gfx_fluid_chart_evolve' )
+      import
+      type ( c_ptr ), value :: Chart, Stream
+      real ( c_double ), value :: Time, FinishTime
+      integer ( c_int ), value :: iCycle, nCyclesMax
+      real ( c_double ), intent ( out ) :: Time_out
+      integer ( c_int ), intent ( out ) :: iCycle_out
+    end function gfx_fluid_chart_evolve
+
+    integer ( c_int ) function gfx_fluid_chart_kernel_launches ( Chart, Count ) &
+      bind ( c, name = 'gfx_fluid_chart_kernel_launches' )
+      import
+      type ( c_ptr ), value :: Chart
+      integer ( c_long_long ), intent ( out ) :: Count
+    end function gfx_fluid_chart_kernel_launches
 
     integer ( c_int ) function gfx_fluid_step_noalloc &
       ( Config, Conserved_dev, TimeStep, DetectFeatures, Fluence_dev, Stream ) &

@@ -23,11 +23,17 @@ def test_library_is_built_for_sm100a():
     path = build_ext.build()
     assert os.path.exists(path)
     assert "arch=compute_100a,code=sm_100a" in " ".join(build_ext.NVCC_FLAGS)
-    assert "--fmad=false" in build_ext.NVCC_FLAGS
+    # the exact build rounds every operation on its own; the speed build fuses
+    assert "--fmad=false" in build_ext.VARIANTS["exact"][1]
+    assert "--fmad=true" in build_ext.VARIANTS["fast"][1]
+    assert "-DGFX_FAST_MATH=1" in build_ext.VARIANTS["fast"][1]
+    for v in ("exact", "fast"):
+        assert os.path.exists(build_ext.lib_path(v)), v
 
 
-def test_every_declared_symbol_is_exported_and_bound():
-    so = ctypes.CDLL(lib.LIB_PATH)
+@pytest.mark.parametrize("variant", ["exact", "fast"])
+def test_every_declared_symbol_is_exported_and_bound(variant):
+    so = ctypes.CDLL(lib.lib_path(variant))
     names = header_functions()
     assert len(names) >= 15
     for n in names:

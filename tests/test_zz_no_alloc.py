@@ -54,8 +54,25 @@ def _cases():
 CASES = _cases()
 
 
+@pytest.mark.parametrize("detect_first", [False, True], ids=["zero_features_first",
+                                                           "features_from_the_first_step"])
 @pytest.mark.parametrize("name,cfg,prim", CASES, ids=[c[0] for c in CASES])
-def test_noalloc_step_matches_the_handle_step_twice(name, cfg, prim):
+def test_noalloc_step_matches_the_handle_step_twice(name, cfg, prim, detect_first):
+    _run_pair(name, cfg, prim, detect_first, device="cuda")
+
+
+def test_noalloc_step_on_a_second_device():
+    """Each device holds its own copy of the array and its own launch set-up:
+    the step on device 1 must agree with the handle's step there."""
+    torch = _torch()
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one CUDA device visible")
+    name, cfg, prim = CASES[0]
+    with torch.cuda.device(1):
+        _run_pair(name + " on device 1", cfg, prim, True, device="cuda:1")
+
+
+def _run_pair(name, cfg, prim, detect_first, device):
     torch = _torch()
     c = cfg.to_c()
     h = ctypes.c_void_p()
@@ -63,8 +80,8 @@ def test_noalloc_step_matches_the_handle_step_twice(name, cfg, prim):
     try:
         fs = ctypes.c_size_t()
         lib.call("gfx_fluid_fluence_face_size", h, ctypes.byref(fs))
-        prim_d = torch.tensor(prim, dtype=torch.float64, device="cuda")
-        U_ref = torch.zeros((6,) + cfg.shape, dtype=torch.float64, device="cuda")
+        prim_d = torch.tensor(prim, dtype=torch.float64, device=device)
+        U_ref = torch.zeros((6,) + cfg.shape, dtype=torch.float64, device=device)
         s = _stream()
         lib.call("gfx_fluid_from_primitive", h, _p(prim_d), _p(U_ref), s)
         # state from conserved values, as the no-allocation step takes it
@@ -76,10 +93,13 @@ def test_noalloc_step_matches_the_handle_step_twice(name, cfg, prim):
             dt = ctypes.c_double()
             lib.call("gfx_fluid_timestep", h, _p(U_ref), call, ctypes.byref(dt), s)
             # the first step after initialisation runs on zero features, every
-            # later one detects them from its input state
+            # later one detects them from its input state; with detect_first
+            # the handle detects them before its first step too
+            if call == 0 and detect_first:
+                lib.call("gfx_fluid_detect_features", h, _p(U_ref), s)
             lib.call("gfx_fluid_step", h, _p(U_ref), dt.value, _p(fl_ref), s)
             lib.call("gfx_fluid_step_noalloc", ctypes.byref(c), _p(U_na), dt.value,
-                     1 if call > 0 else 0, _p(fl_na), s)
+                     1 if (call > 0 or detect_first) else 0, _p(fl_na), s)
             torch.cuda.synchronize()
             a, b = to_np(U_na), to_np(U_ref)
             everything = (slice(None),) * 3
