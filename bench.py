@@ -8,6 +8,14 @@ integrator cycle: CFL time step + RK2 step (two fused stages, features,
 ghost refresh), device-resident, replayed from a CUDA graph.  Synthetic
 seeded inputs with the benchmark's shape; the 845 MB state exceeds L2.
 
+The headline runs the fast build (libgfx_fluid_fast.so, FP64 with fused
+multiply-adds); the exact build (libgfx_fluid.so, the reference's rounding)
+is measured beside it, and both are checked against the oracle per step on
+the 256^3 state in the same run.  After the timed region the line also
+carries the full-crossing L1 error and the other benchmark configurations
+(Sod 128^3, 512 bricks, the Kelvin-Helmholtz adjoint, Rayleigh-Taylor
+384 x 384 x 768, the 256^3 wave as a 2 x 2 x 2 chart); --no-extras skips them.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 runs N independent replicas (the benchmark fixes one GPU per domain;
@@ -61,13 +69,16 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="sine workload: only the headline (no fast build, no per-step "
                          "parity at full size, no C1 / C3 / C4 / C5 sub-objects)")
-    ap.add_argument("--variant", default="exact", choices=["exact", "fast"],
-                    help="library build of the headline (sine workload) or of the workload")
+    ap.add_argument("--variant", default="fast", choices=["exact", "fast"],
+                    help="library build of the headline (sine workload; the other build is "
+                         "measured beside it) or of the workload")
     ap.add_argument("--tile-rows", type=int, default=0,
                     help="sine workload: tile rows (8 or 16) instead of the autotuner's choice")
     ap.add_argument("--z-chunk", type=int, default=0,
                     help="sine workload: pencil length instead of the autotuner's choice")
     ap.add_argument("--bricks", type=int, default=512)
+    ap.add_argument("--riemann", default="HLLC", choices=["HLLC", "HLL"],
+                    help="sine workload: the Riemann solver (the benchmark's is HLLC)")
     return ap.parse_args()
 
 
@@ -225,6 +236,33 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def fp64_peak():
+    """The device's FP64 rate (FLOP/s, a fused multiply-add counting two):
+    genasis_b200/libgfx_probe.so times chains of fused multiply-adds on every
+    SM, best of 10 launches."""
+    import ctypes
+
+    try:
+        probe = ctypes.CDLL(os.path.join(ROOT, "genasis_b200", "libgfx_probe.so"))
+        f, ms = ctypes.c_double(), ctypes.c_double()
+        if probe.gfx_probe_fp64(10, ctypes.byref(f), ctypes.byref(ms)) == 0:
+            return f.value
+    except OSError:
+        pass
+    return None
+
+
+def fp64_counts(variant, riemann, kernel):
+    """FP64 operations per cell of a stage kernel launch, counted by ncu
+    (profiles/stage_fp64.json: dadd + dmul + 2 dfma thread instructions,
+    predicated on, per cell of the captured launch)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "stage_fp64.json")) as f:
+            return json.load(f)[variant][riemann][kernel]
+    except Exception:  # noqa: BLE001
+        return None
+
+
 def _stage_profile(kernel):
     path = os.path.join(ROOT, "profiles", "stage_traffic.json")
     try:
@@ -299,7 +337,7 @@ def _sine_l1(box, cfg, t):
     return l1
 
 
-def _oracle_sine(n, steps, warmup=1):
+def _oracle_sine(n, steps, warmup=1, riemann="HLLC"):
     """The CPU oracle on the n^3 sine wave: `warmup` untimed steps, then
     `steps` timed ones, all host threads; returns the rate, the seconds, the
     threads, and the last timed step as (state before it, cycle, dt, state
@@ -307,7 +345,7 @@ def _oracle_sine(n, steps, warmup=1):
     from genasis_b200 import problems
     from oracle.oracle import Oracle
 
-    cfg, prim = problems.sine_wave(n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
+    cfg, prim = problems.sine_wave(n, riemann_solver=riemann, courant=0.8, n_ramp_cycles=1)
     o = Oracle(cfg)
     o.set_primitive(prim)
     i = 0
@@ -371,9 +409,10 @@ def _step_parity(box, cfg, before):
             "dt_equal": dt_g == dt}
 
 
-def _stage_timing(box, cfg, cyc, steps):
+def _stage_timing(box, cfg, cyc, steps, fp64_rate=None):
     """Per-kernel device times of an evolve cycle's kernels (CUDA events per
-    launch, gfx_fluid_step_timed) and the roofline of the dominant stage."""
+    launch, gfx_fluid_step_timed) and the roofline of the dominant stage,
+    with its FP64 rate against the measured FP64 peak beside the HBM one."""
     cells = cfg.n_proper
     dt = box.compute_time_step(cyc)
     per = {"features": [], "stage1": [], "stage2": [], "ghosts": []}
@@ -387,12 +426,28 @@ def _stage_timing(box, cfg, cyc, steps):
     dom = max(("stage1", "stage2"), key=lambda k: avg[k])
     peak, peak_kind = peaks()
     achieved = STAGE_BYTES[dom] * cells / (avg[dom] / 1000.0) / 1e9
-    return dt, avg, dom, {
+    roof = {
         "bound": "hbm", "kernel": "stage_kernel (%s)" % dom, "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": traffic_per_launch(dom, cells), "peak_source": peak_kind,
         "algorithmic_bytes_per_cell": STAGE_BYTES[dom], "avg_launch_ms": avg[dom],
         "kernel_ms": avg}
+    riemann = cfg.riemann_solver if isinstance(cfg.riemann_solver, str) else "HLLC"
+    counts = fp64_counts(box.variant, riemann, dom)
+    if counts is not None:
+        # the DRAM bytes of this build's launch, per cell, scaled to the cells
+        roof["traffic"] = counts["dram_bytes_per_cell"] * cells
+        roof["traffic_source"] = "profiles/stage_fp64.json (ncu at 160^3, per cell x cells)"
+        per_cell = counts["fp64_ops_per_cell"]
+        rate = per_cell * cells / (avg[dom] / 1000.0)
+        roof["fp64"] = {"ops_per_cell": per_cell, "achieved_tflops": rate / 1e12,
+                        "peak_tflops": fp64_rate / 1e12 if fp64_rate else None,
+                        "frac": rate / fp64_rate if fp64_rate else None,
+                        "peak_source": "measured by genasis_b200/libgfx_probe.so (chains of "
+                                       "fused multiply-adds, best of 10)",
+                        "counts_source": "profiles/stage_fp64.json (ncu thread instructions "
+                                         "dadd + dmul + 2 dfma, %s)" % counts.get("case", "")}
+    return dt, avg, dom, roof
 
 
 def run_ours(args):
@@ -401,7 +456,8 @@ def run_ours(args):
     world, rank, local = dist_init()
     from genasis_b200 import problems
 
-    cfg, prim = problems.sine_wave(args.n, riemann_solver="HLLC", courant=0.8, n_ramp_cycles=1)
+    cfg, prim = problems.sine_wave(args.n, riemann_solver=args.riemann, courant=0.8,
+                                   n_ramp_cycles=1)
     cells = cfg.n_proper
     box = _sine_box(args, cfg, prim, args.variant)
     t = _timed_evolve(box, args.steps, args.warmup, local, world)
@@ -412,7 +468,8 @@ def run_ours(args):
     # timed region (before the extra steps below move the state on)
     l1 = _sine_l1(box, cfg, t_sim)
 
-    dt, avg, dom, roofline = _stage_timing(box, cfg, cyc2, args.steps)
+    rate64 = fp64_peak()
+    dt, avg, dom, roofline = _stage_timing(box, cfg, cyc2, args.steps, rate64)
     roofline["step_hbm_frac"] = STEP_BYTES * value / world / 1e9 / roofline["peak"]
     roofline["ncu_pipes"] = pipe_use(dom)
 
@@ -450,7 +507,7 @@ def run_ours(args):
 
     cpu = parity = None
     if single and not args.no_cpu_baseline:
-        rate, el, cores, before = _oracle_sine(args.n, 2, warmup=1)
+        rate, el, cores, before = _oracle_sine(args.n, 2, warmup=1, riemann=args.riemann)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "2 RK2 steps (after 1 warm-up) of the %d^3 sine-wave workload on the "
                          "CPU oracle (the C restatement, -O3 -ffp-contract=off; not GenASiS's "
@@ -470,7 +527,7 @@ def run_ours(args):
         tf = _timed_evolve(fb, args.steps, args.warmup, local, world)
         vf = cells * tf["steps"] / (tf["ms"] / 1000.0)
         l1_f = _sine_l1(fb, cfg, tf["t_sim"])  # before the timed steps below move it on
-        _, avg_f, dom_f, roof_f = _stage_timing(fb, cfg, tf["cycle"], args.steps)
+        _, avg_f, dom_f, roof_f = _stage_timing(fb, cfg, tf["cycle"], args.steps, rate64)
         fast = {"variant": other, "library": "genasis_b200/" + (
                     "libgfx_fluid_fast.so" if other == "fast" else "libgfx_fluid.so"),
                 "value": vf, "unit": UNIT, "ms_per_step": tf["ms"] / tf["steps"],
@@ -489,7 +546,8 @@ def run_ours(args):
     if extras:
         configs = {}
         v = args.variant
-        for key, fn in (("c1_sod", lambda: sod_result(128, 100, v)),
+        # C1's free run is the bitwise check: it runs on the exact build
+        for key, fn in (("c1_sod", lambda: sod_result(128, 100, "exact")),
                         ("c3_bricks", lambda: bricks_result(50, 3, 512, v)),
                         ("c4_adjoint", lambda: adjoint_result(128, 64, 3, True, v)),
                         ("c5_rt", lambda: rt_result(200, 3, 10, v)),
@@ -510,7 +568,8 @@ def run_ours(args):
             "ms_per_step": ms_max / steps_done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "sine_wave_%d" % args.n, "cells": cells, "riemann": "HLLC",
+            "config": {"workload": "sine_wave_%d" % args.n, "cells": cells,
+                       "riemann": args.riemann,
                        "reconstruction": "PLM theta 1.4", "boundary": "periodic",
                        "cfl": 0.8, "rk": 2, "parallelism": "replicas" if world > 1 else "single",
                        "library": args.variant,
@@ -525,7 +584,7 @@ def run_ours(args):
             "gpu_launches": t["launches"],
             "clocks": t["clocks"],
             "parity": parity,
-            "fast_build": fast,
+            "other_build": fast,
             "configs": configs,
         }
         print(json.dumps(line), flush=True)
@@ -880,33 +939,71 @@ def chart_result(n=256, n_bricks=(2, 2, 2), steps=20, warmup=3, variant="exact")
             "bitwise_equal_to_single_brick": same, "time_equal": t_b == t_sim}
 
 
-def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=None):
+def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=None,
+              flips=False):
     """Central differences (J(U0 + eps d) - J(U0 - eps d)) / (2 eps), J = sum
     rho^2 dV, along seeded unit directions over all six fields of the proper
     cells, formed cell by cell; returns the relative errors of the adjoint's
-    directional derivatives."""
+    directional derivatives and, with flips, for each direction whether the
+    two forwards took different branches somewhere (their branch signatures,
+    gfx_fluid_step_branches) and the kinds of decision whose counts differ."""
     import torch
 
-    from genasis_b200.adjoint import run_forward
+    from genasis_b200.adjoint import BRANCH_KINDS, branch_signature, run_forward
 
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
     p = (slice(None),) + cfg.proper
+    sig = {}
     if rho_fn is None:
         def rho_fn(U):
+            if flips:
+                sig["last"] = branch_signature(box, U, dts, False)
+                return box.U[0].clone()
             return run_forward(box, U, dts, False, keep=False)[0][0]
-    errs = []
+    errs, flipped, kinds = [], [], {}
     for _ in range(directions):
         d = torch.zeros_like(U0)
         d[p] = torch.randn(d[p].shape, generator=gen, device="cuda", dtype=torch.float64)
         d /= torch.linalg.vector_norm(d)
         rp = rho_fn(U0 + eps * d)
+        sp = sig.get("last")
         rm = rho_fn(U0 - eps * d)
+        sm = sig.get("last")
         q = cfg.proper
         fd = float(((rp[q] - rm[q]) * (rp[q] + rm[q]) * dv[q]).sum() / (2.0 * eps))
         ad = float((grad * d).sum())
         errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+        if flips:
+            flipped.append(sp[0] != sm[0])
+            for k, name in enumerate(BRANCH_KINDS):
+                if sp[1][k] != sm[1][k]:
+                    kinds[name] = kinds.get(name, 0) + 1
+    if flips:
+        return errs, flipped, kinds
     return errs
+
+
+def _fd_summary(errs, flipped, kinds):
+    import numpy as np
+
+    e = np.array(errs)
+    f = np.array(flipped, dtype=bool)
+    out = {"directions": int(len(e)), "within_1e-6": int((e <= 1e-6).sum()),
+           "median_rel_err": float(np.median(e)), "max_rel_err": float(e.max()),
+           "flipped_directions": int(f.sum()),
+           "directions_by_kind_of_flip": kinds}
+    if (~f).any():
+        out["flip_free"] = {"directions": int((~f).sum()),
+                            "within_1e-6": int((e[~f] <= 1e-6).sum()),
+                            "median_rel_err": float(np.median(e[~f])),
+                            "max_rel_err": float(e[~f].max())}
+    if f.any():
+        out["flipped"] = {"directions": int(f.sum()),
+                          "within_1e-6": int((e[f] <= 1e-6).sum()),
+                          "median_rel_err": float(np.median(e[f])),
+                          "max_rel_err": float(e[f].max())}
+    return out
 
 
 def adjoint_result(n=128, directions=64, warmup=3, oracle_fd=True, variant="exact"):
@@ -961,7 +1058,8 @@ def adjoint_result(n=128, directions=64, warmup=3, oracle_fd=True, variant="exac
                 fwd_plain.append(e[2].elapsed_time(e[3]))
             del cps
         launches = box.kernel_launches() - launches0
-        errs = _fd_check(box, cfg, U0, dts, grad, dv, directions, seed=20261205)
+        errs, flipped, kinds = _fd_check(box, cfg, U0, dts, grad, dv, directions,
+                                         seed=20261205, flips=True)
         errs_np = np.array(errs)
         entry = {
             "forward_ms": statistics.median(fwd), "adjoint_ms": statistics.median(adj),
@@ -970,17 +1068,17 @@ def adjoint_result(n=128, directions=64, warmup=3, oracle_fd=True, variant="exac
             "fd_directions": len(errs), "fd_within_1e-6": int((errs_np <= 1e-6).sum()),
             "fd_median_rel_err": float(np.median(errs_np)),
             "fd_max_rel_err": float(errs_np.max()),
+            "fd_eps_1e-6": _fd_summary(errs, flipped, kinds),
         }
         if state == "noisy":
             # the same check at larger eps: at eps = 1e-6 a unit direction over
             # all 6 x n^3 values moves each value by ~1e-10, close to the
             # rounding floor of the differenced states
             sweep = {}
-            for eps in (1e-5, 1e-4):
-                e_s = np.array(_fd_check(box, cfg, U0, dts, grad, dv, 16, seed=20261207, eps=eps))
-                sweep["%g" % eps] = {"directions": 16, "within_1e-6": int((e_s <= 1e-6).sum()),
-                                     "median_rel_err": float(np.median(e_s)),
-                                     "max_rel_err": float(e_s.max())}
+            for eps in (1e-7, 1e-5, 1e-4):
+                e_s, f_s, k_s = _fd_check(box, cfg, U0, dts, grad, dv, 16, seed=20261207,
+                                          eps=eps, flips=True)
+                sweep["%g" % eps] = _fd_summary(e_s, f_s, k_s)
             entry["fd_eps_sweep"] = sweep
         if state == "noisy" and oracle_fd:
             # the reference-FD gradient: the oracle's step, on a 32^3 brick of

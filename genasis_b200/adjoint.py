@@ -31,6 +31,40 @@ def step_adjoint(box: FluidBox, U_n, dt, lam_np1, lam_n=None, U_np1=None,
     return lam_n
 
 
+BRANCH_KINDS = ("slope_zero", "slope_left", "slope_right", "slope_centred", "ap_0", "ap_left",
+                "ap_right", "am_0", "am_left", "am_right", "hllc_centre", "ac_nonnegative",
+                "md_positive", "floored", "flags")
+
+
+def step_branches(box: FluidBox, U_n, dt, detect_features=True):
+    """The branch signature of one forward step from U_n
+    (gfx_fluid_step_branches): (hash, decisions, counts per kind)."""
+    import ctypes
+
+    import numpy as np
+
+    out = np.zeros(2 + len(BRANCH_KINDS), dtype=np.uint64)
+    box.call("gfx_fluid_step_branches", box.h, _ptr(U_n.contiguous()), float(dt),
+             int(bool(detect_features)), out.ctypes.data_as(ctypes.c_void_p), _stream())
+    return int(out[0]), int(out[1]), out[2:].astype(np.int64)
+
+
+def branch_signature(box: FluidBox, U0, dts, detect_first=False):
+    """The branches of the run of steps dts from U0 (the forward of
+    run_forward): the hash of every step's decisions (summed modulo 2^64)
+    and the counts per kind, summed over the steps."""
+    import numpy as np
+
+    prepare_state(box, U0, detect_first)
+    h, counts = 0, np.zeros(len(BRANCH_KINDS), dtype=np.int64)
+    for i, dt in enumerate(dts):
+        hi, _, ci = step_branches(box, box.U, dt, detect_first or i > 0)
+        h = (h + hi) % (1 << 64)
+        counts += ci
+        box.step(float(dt))
+    return h, counts
+
+
 def prepare_state(box: FluidBox, U0, detect_first):
     """Loads U0 as the box's state from conserved values, with the shock
     features of U0 (detect_first) or zero features (the first step after

@@ -11,7 +11,8 @@ Two variants of the same sources:
   multiply-adds, the entropy per baryon from two logarithms).  Its results
   stay within the 1e-12 per-step bar of the reference's step, not bit for bit.
 
-Both are compiled at once when either is stale."""
+Both are compiled at once when either is stale, beside libgfx_probe.so
+(csrc/fp64_probe.cu), the FP64 rate probe of the bench's FP64 roofline."""
 import os
 import subprocess
 import sys
@@ -56,13 +57,24 @@ def _stale(path):
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+PROBE = ("libgfx_probe.so", "fp64_probe.cu", "build_probe.log")
+
+
 def build(force=False, verbose=False, variants=("exact", "fast")):
-    """Compiles the variants whose library is older than a source; returns
-    the path of the exact library."""
+    """Compiles the variants whose library is older than a source, and the
+    FP64 probe; returns the path of the exact library."""
     env = dict(os.environ)
     env.pop("CC", None)
     env.pop("CXX", None)
     jobs = []
+    probe_out = os.path.join(HERE, PROBE[0])
+    probe_src = os.path.join(CSRC, PROBE[1])
+    if force or not os.path.exists(probe_out) or \
+            os.path.getmtime(probe_src) > os.path.getmtime(probe_out):
+        cmd = [_nvcc(), *NVCC_FLAGS, "-o", probe_out + ".tmp", probe_src]
+        p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                             env=env)
+        jobs.append(("probe", probe_out, os.path.join(HERE, PROBE[2]), cmd, p))
     for v in variants:
         name, flags, log = VARIANTS[v]
         out = os.path.join(HERE, name)

@@ -296,4 +296,179 @@ __global__ void adj_last_kernel(Box b, Phys ph, double dt, const double* __restr
   }
 }
 
+// ---- Branch signature of a forward stage --------------------------------------
+// The adjoint is the derivative of the branch the forward takes at every
+// limiter argument, wave-speed maximum, HLLC decision and floor.  A central
+// difference (J(U + eps d) - J(U - eps d)) / (2 eps) measures that derivative
+// only if both forwards take the same branches everywhere.  The signature of
+// a stage is an order-independent hash of all its decisions (a sum of mixed
+// position-decision codes, added atomically) and a count per kind of
+// decision, so that two forwards can be compared without storing either.
+enum {
+  BR_SLOPE0 = 0,     // limiter: zero slope (BR_SLOPE0 + branch, 4 kinds)
+  BR_AP0 = 4,        // argmax of AP = max(0, vl + CSl, vr + CSr) (3 kinds)
+  BR_AM0 = 7,        // argmax of AM (3 kinds)
+  BR_HLLC = 10,      // the HLLC centre state taken (not the HLL flux)
+  BR_AC_POS = 11,    // AC >= 0 (left centre state) among those
+  BR_MD_POS = 12,    // MD > 0 in the HLLC centre speed
+  BR_FLOOR = 13,     // a floored value of the stage input (N = N_min or E = 0)
+  BR_FLAG = 14,      // a DIFFUSIVE_FLUX_I bit set
+  BR_KINDS = 15
+};
+
+__device__ __forceinline__ unsigned long long branch_mix(unsigned long long x) {
+  // splitmix64's finaliser (S. Vigna, public domain)
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Cell c of stage `stage` (W: its input primitives, compact): for each
+// direction the limiter branch of each primitive's slope and the decisions of
+// the flux through the cell's inner face (between c - 1 and c); the floors of
+// W at c; the flags of df at c.  out[0]: hash, out[1]: decisions counted,
+// out[2 + k]: count of kind k.
+template <bool HLLC>
+__global__ void branch_signature_kernel(const __grid_constant__ AdjDesc A,
+                                        const __grid_constant__ Phys ph, int stage,
+                                        unsigned long long* __restrict__ out) {
+  __shared__ unsigned long long s_acc[2 + BR_KINDS];
+  for (int i = threadIdx.x; i < 2 + BR_KINDS; i += blockDim.x) s_acc[i] = 0;
+  __syncthreads();
+  unsigned long long hash = 0, n_dec = 0;
+  unsigned long long cnt[BR_KINDS];
+#pragma unroll
+  for (int k = 0; k < BR_KINDS; ++k) cnt[k] = 0;
+  const long long nP = A.nP;
+  auto note = [&](unsigned long long pos, int code, int kind) {
+    hash += branch_mix(pos * 64ull + (unsigned long long)code);
+    ++n_dec;
+    if (kind >= 0) ++cnt[kind];
+  };
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nP;
+       c += (long long)gridDim.x * blockDim.x) {
+    int t[3];
+    {
+      const unsigned cc = (unsigned)c, n0 = (unsigned)A.n[0], n1 = (unsigned)A.n[1];
+      const unsigned r = cc / n0;
+      t[0] = (int)(cc - r * n0);
+      t[2] = (int)(r / n1);
+      t[1] = (int)(r - (unsigned)t[2] * n1);
+    }
+    const unsigned long long base = ((unsigned long long)stage * 8ull) * (unsigned long long)nP;
+    // floors of the stage input
+    {
+      const double N = A.W[c], E = A.W[4 * nP + c];
+      const bool fl = (N == ph.nmin && A.W[nP + c] == 0.0 && A.W[2 * nP + c] == 0.0 &&
+                       A.W[3 * nP + c] == 0.0) || E == 0.0;
+      note((base + 0) * 8 + (unsigned long long)c, fl ? 1 : 0, fl ? BR_FLOOR : -1);
+    }
+    if (A.df) {
+      const int f = A.df[c];
+      note((base + 1) * 8 + (unsigned long long)c, f, -1);
+      cnt[BR_FLAG] += __popc(f);
+    }
+#pragma unroll 1
+    for (int D = 0; D < 3; ++D) {
+      const long long st = D == 0 ? 1 : (D == 1 ? A.n[0] : (long long)A.n[0] * A.n[1]);
+      const long long cbase = c - (long long)t[D] * st;  // cell 0 of this pencil
+      const AxisGeo& G = A.geo[D];
+      // the stencil cells t - 2 .. t + 1 along D (boundary maps)
+      double w[4][5];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        bool neg;
+        const int sj = bc_map(t[D] - 2 + j, A.n[D], A.bc[D][0], A.bc[D][1], neg);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) w[j][q] = A.W[q * nP + cbase + sj * st];
+        if (neg) w[j][1 + D] = -w[j][1 + D];
+      }
+      // slopes of cells t - 1 (stencil 0, 1, 2) and t (1, 2, 3) with branches
+      double sl[2][5];
+      int br[2][5];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int tt = t[D] - 1 + e + 2;
+        const double dxl = __ldg(G.dXI + tt), dxr = __ldg(G.dXI + tt + 1);
+        const double sql = __ldg(G.SQ + tt), sqr = __ldg(G.SQ + tt + 1);
+        const double cden = __ldg(G.CDEN + tt), rdxl = __ldg(G.RDXI + tt);
+        const double rdxr = __ldg(G.RDXI + tt + 1), rcden = __ldg(G.RCDEN + tt);
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+          sl[e][q] = limited_slope_branch(w[e][q], w[e + 1][q], w[e + 2][q], dxl, dxr, sql, sqr,
+                                          cden, rdxl, rdxr, rcden, ph.theta, ph.use_limiter,
+                                          br[e][q]);
+      }
+      // the cell's own slopes (each cell counted once per direction)
+#pragma unroll
+      for (int q = 0; q < 5; ++q)
+        note(((base + 2 + D) * 8 + (unsigned long long)q) * (unsigned long long)nP +
+                 (unsigned long long)c,
+             br[1][q], BR_SLOPE0 + br[1][q]);
+      // the inner face of the cell
+      const int tf = t[D] + 2;
+      const double wr = __ldg(G.WR + tf - 1), wl = __ldg(G.WL + tf);
+      double l[5], r[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        l[q] = w[1][q] + wr * sl[0][q];
+        r[q] = w[2][q] - wl * sl[1][q];
+      }
+      FaceState L, R;
+      face_state<5>(l[0], l[1], l[2], l[3], l[4], ph, L);
+      face_state<5>(r[0], r[1], r[2], r[3], r[4], ph, R);
+      const double vl = D == 0 ? L.V1 : (D == 1 ? L.V2 : L.V3);
+      const double vr = D == 0 ? R.V1 : (D == 1 ? R.V2 : R.V3);
+      int ap = 0, am = 0;
+      double AP = 0.0, AM = 0.0;
+      if (vl + L.CS > AP) {
+        AP = vl + L.CS;
+        ap = 1;
+      }
+      if (vr + R.CS > AP) {
+        AP = vr + R.CS;
+        ap = 2;
+      }
+      if (-(vl - L.CS) > AM) {
+        AM = -(vl - L.CS);
+        am = 1;
+      }
+      if (-(vr - R.CS) > AM) {
+        AM = -(vr - R.CS);
+        am = 2;
+      }
+      int code = ap + 3 * am;
+      cnt[BR_AP0 + ap] += 1;
+      cnt[BR_AM0 + am] += 1;
+      if (HLLC) {
+        const bool diff = A.df != nullptr && ((A.df[c] >> D) & 1);
+        const double ml = D == 0 ? L.S1 : (D == 1 ? L.S2 : L.S3);
+        const double mr = D == 0 ? R.S1 : (D == 1 ? R.S2 : R.S3);
+        const double fdl = L.D * vl, fdr = R.D * vr;
+        const double fsl = ml * vl + L.P, fsr = mr * vr + R.P;
+        const double MD = AP * R.D + AM * L.D - fdr + fdl;
+        const double SN = AP * mr + AM * ml - fsr + fsl;
+        const double AC = SN * (fmax2(MD, 0.0) / fmax2(MD * MD, kTiny));
+        const bool centre = !diff && AP != 0.0 && AM != 0.0;
+        code += 9 * ((int)centre + 2 * (int)(AC >= 0.0) + 4 * (int)(MD > 0.0));
+        if (centre) {
+          cnt[BR_HLLC] += 1;
+          if (AC >= 0.0) cnt[BR_AC_POS] += 1;
+        }
+        if (MD > 0.0) cnt[BR_MD_POS] += 1;
+      }
+      note((base + 5 + D) * 8ull * (unsigned long long)nP + (unsigned long long)c, code, -1);
+    }
+  }
+  atomicAdd(&s_acc[0], hash);
+  atomicAdd(&s_acc[1], n_dec);
+#pragma unroll
+  for (int k = 0; k < BR_KINDS; ++k)
+    if (cnt[k]) atomicAdd(&s_acc[2 + k], cnt[k]);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 2 + BR_KINDS; i += blockDim.x)
+    if (s_acc[i]) atomicAdd(&out[i], s_acc[i]);
+}
+
 }  // namespace gfx

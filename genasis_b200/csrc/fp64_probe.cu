@@ -1,0 +1,70 @@
+// fp64_probe.cu -- the FP64 fused multiply-add rate of the device, measured
+// for the bench's FP64 roofline (the HBM roofline's denominator is measured
+// by the driver; the FP64 pipe's is measured here, the same way: a kernel
+// that does nothing else, timed with CUDA events, best of several runs).
+//
+// Every thread runs 8 independent chains of dependent fused multiply-adds
+// (enough independent work to cover the pipe's latency), and writes their sum
+// so that none of the work can be left out.  The grid fills every SM.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+namespace {
+
+constexpr int kChains = 8;
+
+__global__ void __launch_bounds__(256) dfma_kernel(int iters, double a, double b,
+                                                    double* __restrict__ out) {
+  double x[kChains];
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) x[c] = 1.0 + 1e-3 * (threadIdx.x + c);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) x[c] = __fma_rn(x[c], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) s += x[c];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Best of `reps` launches: FP64 operations per second (a fused multiply-add
+// counts two) into *flops, the launch's milliseconds into *ms.  0 on success,
+// -2 on a CUDA error.
+int gfx_probe_fp64(int reps, double* flops, double* ms) {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -2;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -2;
+  const int block = 256, grid = sms * 8, iters = 4096;
+  double* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double) * grid * block) != cudaSuccess) return -2;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int rc = 0;
+  for (int r = 0; r < reps + 1 && rc == 0; ++r) {  // the first launch warms up
+    cudaEventRecord(e0);
+    dfma_kernel<<<grid, block>>>(iters, 0.999999, 1e-7, out);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc = -2;
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (r > 0 && t < best) best = t;
+  }
+  if (cudaGetLastError() != cudaSuccess) rc = -2;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (rc) return rc;
+  *ms = best;
+  *flops = 2.0 * kChains * (double)iters * grid * block / (best * 1e-3);
+  return 0;
+}
+
+}  // extern "C"

@@ -196,6 +196,7 @@ struct gfx_fluid {
   // recomputed U^n+1 when the caller passes none
   double* adj = nullptr;
   uint8_t* adj_flags = nullptr;
+  unsigned long long* branch_buf = nullptr;  // gfx_fluid_step_branches: [2 + kinds]
   double* adj_U = nullptr;
   // tuning (gfx_fluid_set_tuning; 0 = built-in default)
   int z_chunk = 0;
@@ -959,6 +960,7 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->U_stage);
   cudaFree(h->adj);
   cudaFree(h->adj_flags);
+  cudaFree(h->branch_buf);
   cudaFree(h->adj_U);
   cudaFree(h->state_counts);
   cudaFree(h->partials);
@@ -2050,6 +2052,80 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
                                                        lam_n);
   CUDA_TRY(cudaGetLastError());
   h->launches += 1;
+  return GFX_OK;
+}
+
+static_assert(BR_KINDS == GFX_BRANCH_KINDS, "branch kinds of the header");
+
+int gfx_fluid_step_branches(gfx_fluid* h, const double* U_n, double dt, int detect_features,
+                            unsigned long long* out, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_branches")) return rc0;
+  if (!h || !U_n || !out) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (h->cfg.reconstruction != GFX_RECONSTRUCTION_LINEAR)
+    return fail(GFX_ERR_UNSUPPORTED, "branch signature: LINEAR reconstruction only");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  cudaStream_t s = (cudaStream_t)stream;
+  const Box& b = h->box;
+  if (b.nP >= (1LL << 31))
+    return fail(GFX_ERR_UNSUPPORTED, "branch signature: %lld proper cells", b.nP);
+  const size_t nP = (size_t)b.nP;
+  if (!h->adj) {
+    if (cudaMalloc(&h->adj, 20 * nP * sizeof(double)) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
+    if (cudaMalloc(&h->adj_flags, nP) != cudaSuccess)
+      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
+  }
+  if (!h->branch_buf &&
+      cudaMalloc(&h->branch_buf, (2 + BR_KINDS) * sizeof(unsigned long long)) != cudaSuccess)
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc branch signature");
+  double* W0 = h->adj;
+  uint8_t* df = h->adj_flags;
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  const bool grav = h->cfg.uniform_acceleration != 0.0;
+  const int blk = 256;
+  const uint8_t* feat = nullptr;
+  if (hllc && detect_features) {
+    CUDA_TRY(launch_features(b, h->ph, U_n, nullptr, df, 0, b.n[2], s));
+    h->launches += 1;
+    feat = df;
+  }
+  // the forward of the step from U^n, as the adjoint recomputes it: W0, and
+  // stage 1 for W1 (into Yp)
+  adj_prims_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, U_n, W0);
+  set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
+  reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 3;
+  BrickDesc d1 = make_desc(h, U_n, nullptr, nullptr, nullptr, feat, nullptr, h->dt_slot, 0.5,
+                           nullptr);
+  CUDA_TRY(launch_stage(MODE_STAGE1, false, hllc, grav, d1, nullptr, h->items, h->n_items,
+                        h->counters, h->ph, s));
+  h->launches += 1;
+  CUDA_TRY(cudaMemsetAsync(h->branch_buf, 0, (2 + BR_KINDS) * sizeof(unsigned long long), s));
+  AdjDesc A;
+  memset(&A, 0, sizeof(A));
+  for (int a = 0; a < 3; ++a) {
+    A.n[a] = b.n[a];
+    A.bc[a][0] = b.bc[a][0];
+    A.bc[a][1] = b.bc[a][1];
+    A.geo[a] = h->dgeo[a];
+  }
+  A.nP = b.nP;
+  A.df = feat;
+  for (int stage = 0; stage < 2; ++stage) {
+    A.W = stage == 0 ? W0 : h->Yp;
+    if (hllc)
+      branch_signature_kernel<true><<<grid_for(b.nP, blk), blk, 0, s>>>(A, h->ph, stage,
+                                                                        h->branch_buf);
+    else
+      branch_signature_kernel<false><<<grid_for(b.nP, blk), blk, 0, s>>>(A, h->ph, stage,
+                                                                         h->branch_buf);
+    CUDA_TRY(cudaGetLastError());
+    h->launches += 1;
+  }
+  CUDA_TRY(cudaMemcpyAsync(out, h->branch_buf, (2 + BR_KINDS) * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
   return GFX_OK;
 }
 

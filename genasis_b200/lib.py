@@ -60,6 +60,7 @@ SIGNATURES = {
     "gfx_fluid_batch_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
     "gfx_fluid_step_adjoint": [P, P, D, P, P, P, I, P],
     "gfx_fluid_step_noalloc": [ctypes.POINTER(GfxConfig), P, D, I, P, P],
+    "gfx_fluid_step_branches": [P, P, D, I, P, P],
     "gfx_fluid_check_state": [P, P, P],
     "gfx_fluid_set_tuning": [P, I, I, I],
     "gfx_fluid_totals": [P, P, P, P],

@@ -260,6 +260,24 @@ int gfx_fluid_step_adjoint(gfx_fluid *h, const double *U_n_dev, double dt,
                            const double *lam_np1_dev, double *lam_n_dev,
                            const double *U_np1_dev, int detect_features, void *stream);
 
+/* The branches one step from U_n_dev takes, for finite-difference checks of
+ * the adjoint: no counterpart in the reference.  The adjoint is the
+ * derivative of the branch the forward takes at every limiter argument,
+ * wave-speed maximum, HLLC decision and floor; a central difference measures
+ * it only where the forwards at U + eps d and U - eps d take the same
+ * branches.  Recomputes the step's two stages from U_n_dev (features detected
+ * from it when detect_features is nonzero, as in gfx_fluid_step_adjoint) and
+ * writes out_host[0] = an order-independent hash of every decision of both
+ * stages (limiter branch of each slope, the two wave-speed maxima, the HLLC
+ * path, side and centre-speed sign of each face, floored inputs, shock
+ * flags), out_host[1] = the number of decisions and out_host[2 ..
+ * 2 + GFX_BRANCH_KINDS - 1] = counts per kind: limiter zero / left / right /
+ * centred slope, AP arg 0 / 1 / 2, AM arg 0 / 1 / 2, HLLC centre state, AC >=
+ * 0, MD > 0, floored inputs, flags set.  Synchronises the stream. */
+#define GFX_BRANCH_KINDS 15
+int gfx_fluid_step_branches(gfx_fluid *h, const double *U_n_dev, double dt,
+                            int detect_features, unsigned long long *out_host, void *stream);
+
 /* ---- One step without allocation ------------------------------------------
  * No counterpart in the reference (which allocates its storage once per
  * run); added for callers that cannot call cudaMalloc: a host program whose

@@ -60,7 +60,7 @@ module GFX_Fluid_C
     gfx_fluid_clear_features, gfx_fluid_get_features, gfx_fluid_increment, &
     gfx_fluid_fluence_face_size, gfx_fluid_step, gfx_fluid_step_host, &
     gfx_fluid_timestep, gfx_fluid_evolve, gfx_fluid_step_timed, &
-    gfx_fluid_kernel_launches, gfx_fluid_step_adjoint, &
+    gfx_fluid_kernel_launches, gfx_fluid_step_adjoint, gfx_fluid_step_branches, &
     gfx_fluid_set_tuning, gfx_fluid_batch_create, gfx_fluid_batch_destroy, &
     gfx_fluid_batch_set_clocks, gfx_fluid_batch_evolve, &
     gfx_fluid_batch_clocks, gfx_fluid_batch_kernel_launches, &
@@ -270,6 +270,16 @@ module GFX_Fluid_C
       type ( c_ptr ), value :: Batch
       integer ( c_long_long ), intent ( out ) :: Count
     end function gfx_fluid_batch_kernel_launches
+
+    integer ( c_int ) function gfx_fluid_step_branches &
+      ( Handle, Conserved_dev, TimeStep, DetectFeatures, Signature, Stream ) &
+      bind ( c, name = 'gfx_fluid_step_branches' )
+      import
+      type ( c_ptr ), value :: Handle, Conserved_dev, Stream
+      real ( c_double ), value :: TimeStep
+      integer ( c_int ), value :: DetectFeatures
+      integer ( c_long_long ), intent ( out ) :: Signature ( 17 )
+    end function gfx_fluid_step_branches
 
     !-- A chart of several bricks on one device (Chart_SLD's bricks)
 
