@@ -551,8 +551,14 @@ def run_ours(args):
                         ("c3_bricks", lambda: bricks_result(50, 3, 512, v)),
                         ("c4_adjoint", lambda: adjoint_result(128, 64, 3, True, v)),
                         ("c5_rt", lambda: rt_result(200, 3, 10, v)),
+                        # the chart against the single brick: bit for bit on the exact
+                        # build (the same arithmetic on every cell); the fast build's
+                        # chart kernels may fuse differently from its single-brick ones
                         ("chart_2x2x2", lambda: chart_result(args.n, (2, 2, 2), args.steps,
-                                                             args.warmup, v))):
+                                                             args.warmup, "exact")),
+                        ("chart_2x2x2_fast", lambda: chart_result(args.n, (2, 2, 2),
+                                                                  args.steps, args.warmup,
+                                                                  "fast"))):
             t0 = time.perf_counter()
             try:
                 configs[key] = fn()
@@ -718,7 +724,7 @@ def run_adjoint_step(args):
     torch.cuda.set_device(0)
     n = args.n if args.n != 256 else 128
     cfg, prim = problems.kelvin_helmholtz(n)
-    box = FluidBox(cfg)
+    box = FluidBox(cfg, variant=args.variant)
     box.compute_from_primitive(prim)
     box.compute_from_conserved()
     dts = []
@@ -851,6 +857,29 @@ def rt_result(steps=200, warmup=3, adjoint_steps=10, variant="exact"):
     mass1 = float((box.U[0][p] * dv[p]).sum())
     dt = box.compute_time_step(cyc2)
     roof = stage_roofline(box, cells, dt, 5)
+    def adjoint_cost(bx, U0, dts):
+        # an untimed forward first: its checkpoints take their memory from the
+        # allocator once, so that the timed forward measures the steps
+        final, cps = run_forward(bx, U0, dts, True)
+        del final, cps
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        final, cps = run_forward(bx, U0, dts, True)
+        e[1].record()
+        lam = torch.zeros_like(final)
+        lam[0] = 2.0 * final[0] * dv
+        grad = run_adjoint(bx, cps, dts, lam, True)
+        e[2].record()
+        torch.cuda.synchronize()
+        out = {"library": bx.variant, "steps": len(dts), "forward_ms": e[0].elapsed_time(e[1]),
+               "adjoint_ms": e[1].elapsed_time(e[2]),
+               "adjoint_over_forward": e[1].elapsed_time(e[2]) / e[0].elapsed_time(e[1]),
+               "objective": "sum rho^2 dV",
+               "gradient_finite": bool(torch.isfinite(grad).all())}
+        del cps, grad, final, lam
+        return out
+
     adj = None
     if adjoint_steps > 0:
         U0 = box.U.clone()
@@ -858,25 +887,15 @@ def rt_result(steps=200, warmup=3, adjoint_steps=10, variant="exact"):
         for i in range(adjoint_steps):
             dts.append(box.compute_time_step(cyc2 + i))
             box.step(dts[-1])
-        # an untimed forward first: its checkpoints take their memory from the
-        # allocator once, so that the timed forward measures the steps
-        final, cps = run_forward(box, U0, dts, True)
-        del final, cps
-        torch.cuda.synchronize()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        e[0].record()
-        final, cps = run_forward(box, U0, dts, True)
-        e[1].record()
-        lam = torch.zeros_like(final)
-        lam[0] = 2.0 * final[0] * dv
-        grad = run_adjoint(box, cps, dts, lam, True)
-        e[2].record()
-        torch.cuda.synchronize()
-        adj = {"steps": len(dts), "forward_ms": e[0].elapsed_time(e[1]),
-               "adjoint_ms": e[1].elapsed_time(e[2]),
-               "adjoint_over_forward": e[1].elapsed_time(e[2]) / e[0].elapsed_time(e[1]),
-               "objective": "sum rho^2 dV", "gradient_finite": bool(torch.isfinite(grad).all())}
-        del cps, grad, final, lam, U0
+        adj = adjoint_cost(box, U0, dts)
+        # the same steps' adjoint on the other library build, from the same
+        # state with the same time steps
+        other = "exact" if variant == "fast" else "fast"
+        box.close()
+        torch.cuda.empty_cache()
+        box = autotune.tuned_box(cfg, adjoint=False, variant=other)
+        adj["other_build"] = adjoint_cost(box, U0, dts)
+        del U0
     value = cells * n_done / (ms / 1000.0)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": n_done,
@@ -885,7 +904,8 @@ def rt_result(steps=200, warmup=3, adjoint_steps=10, variant="exact"):
         "config": {"workload": "rayleigh_taylor_384x384x768", "cells": cells,
                    "riemann": "HLLC", "gravity": 0.1, "boundary": "periodic x/y, reflecting z",
                    "cfl": 0.8, "sim_time": t_sim, "library": variant,
-                   "l2": "inputs larger than L2 (state %.1f GB)" % (6 * box.n_values * 8 / 1e9),
+                   "l2": "inputs larger than L2 (state %.1f GB)" % (6 * (384 + 4) ** 2 *
+                                                                       (768 + 4) * 8 / 1e9),
                    "mass_rel_change": (mass1 - mass0) / mass0},
         "roofline": roof, "step_hbm_frac": STEP_BYTES * value / 1e9 / roof["peak"],
         "adjoint": adj, "gpu_launches": launches, "clocks": clocks,
@@ -931,12 +951,54 @@ def chart_result(n=256, n_bricks=(2, 2, 2), steps=20, warmup=3, variant="exact")
     box.close()
     p = cfg.proper
     same = [bool(np.array_equal(got[f][p], ref[f][p])) for f in range(6)]
+    scale = [max(float(np.abs(ref[f][p]).max()), 1e-300) for f in range(6)]
+    diff = [float(np.abs(got[f][p] - ref[f][p]).max()) / scale[f] for f in range(6)]
     return {"workload": "sine_wave_%d_chart_%dx%dx%d" % ((n,) + tuple(n_bricks)),
+            "max_rel_diff_to_single_brick": diff,
             "bricks": int(np.prod(n_bricks)), "brick_cells": [n // b for b in n_bricks],
             "library": variant, "value": cfg.n_proper * (cyc2 - cyc) / (ms / 1000.0),
             "unit": UNIT, "steps": cyc2 - cyc, "ms_per_step": ms / (cyc2 - cyc),
             "gpu_launches": launches, "cycles_compared": cyc2,
             "bitwise_equal_to_single_brick": same, "time_equal": t_b == t_sim}
+
+
+def _adjoint_cost(cfg, prim, n_steps, variant, reps=3):
+    """Forward (with per-step checkpoints) and adjoint milliseconds of
+    n_steps steps from prim, J = sum rho^2 dV, on one library build: the
+    medians of reps timed runs after one untimed run."""
+    import torch
+
+    from genasis_b200 import autotune
+    from genasis_b200.adjoint import cell_volumes, run_adjoint, run_forward
+
+    box = autotune.tuned_box(cfg, adjoint=True, variant=variant)
+    box.compute_from_primitive(prim)
+    box.compute_from_conserved()
+    U0 = box.U.clone()
+    dts = []
+    for i in range(n_steps):
+        dts.append(box.compute_time_step(i))
+        box.step(dts[-1])
+    dv = cell_volumes(box)
+    fwd, adj = [], []
+    for rep in range(reps + 1):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        e[0].record()
+        final, cps = run_forward(box, U0, dts, False)
+        e[1].record()
+        lam = torch.zeros_like(final)
+        lam[0] = 2.0 * final[0] * dv
+        run_adjoint(box, cps, dts, lam, False)
+        e[2].record()
+        torch.cuda.synchronize()
+        if rep > 0:
+            fwd.append(e[0].elapsed_time(e[1]))
+            adj.append(e[1].elapsed_time(e[2]))
+        del cps, final, lam
+    box.close()
+    f, a = statistics.median(fwd), statistics.median(adj)
+    return {"library": variant, "forward_ms": f, "adjoint_ms": a, "adjoint_over_forward": a / f}
 
 
 def _fd_check(box, cfg, U0, dts, grad, dv, directions, seed, eps=1e-6, rho_fn=None,
@@ -1117,6 +1179,8 @@ def adjoint_result(n=128, directions=64, warmup=3, oracle_fd=True, variant="exac
         out[state] = entry
         box.close()
     spec = out["spec"]
+    cfg_c, prim_c = problems.kelvin_helmholtz(n)
+    other = _adjoint_cost(cfg_c, prim_c, n_steps, "exact" if variant == "fast" else "fast")
     line = {
         "metric": "adjoint/forward cost", "value": spec["adjoint_over_forward"],
         "unit": "x (adjoint ms / forward ms)", "n_gpus": 1, "steps": n_steps,
@@ -1128,6 +1192,7 @@ def adjoint_result(n=128, directions=64, warmup=3, oracle_fd=True, variant="exac
                    "objective": "sum rho^2 dV", "checkpointing": "per step",
                    "fd_eps": 1e-6, "fd_seed": 20261205, "library": variant},
         "spec_state": spec, "noisy_state": out["noisy"],
+        "other_build_cost": other,
         "gpu_launches": launches,
     }
     return line

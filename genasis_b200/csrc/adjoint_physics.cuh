@@ -89,7 +89,7 @@ __device__ __forceinline__ void face_state_adjoint(const double* w, const FaceSt
   double lE = a.G + ph.gm1 * a.P;
   if (s.CS > 0.0 && a.CS != 0.0) {
     // CS = sqrt(gamma (gamma - 1) E / N): dCS/dE = CS / (2 E), dCS/dN = -CS / (2 N)
-    const double r = 0.5 * s.CS / (N * w[4]);
+    const double r = 0.5 * s.CS * recip(N * w[4]);
     lE += a.CS * r * N;
     lN += -a.CS * r * w[4];
   }
@@ -175,7 +175,11 @@ __device__ __forceinline__ void flux_adjoint(const double* l, const double* r, b
     const double fsl = sl * vl + L.P, fsr = sr * vr + R.P;
     const double MD = AP * R.D + AM * L.D - fdr + fdl;
     const double SN = AP * sr + AM * sl - fsr + fsl;
+#if GFX_FAST_MATH
+    const double m = fmax2(MD, 0.0) * recip(fmax2(MD * MD, kTiny));  // as the forward
+#else
     const double m = fmax2(MD, 0.0) / fmax2(MD * MD, kTiny);
+#endif
     const double AC = SN * m;
     if (!diffusive && AP != 0.0 && AM != 0.0) {
       done = true;
@@ -187,7 +191,7 @@ __device__ __forceinline__ void flux_adjoint(const double* l, const double* r, b
       const double A_V = left ? AM + vs : AP - vs;
       const double A_AC = left ? AM + AC : AP - AC;
       const double den = fmax2(fabs(A_AC), kSqrtTiny);
-      const double inv = 1.0 / den;
+      const double inv = recip(den);
       const double Dc = S.D * A_V * inv;
       double v[3] = {S.V1, S.V2, S.V3};
       v[D] = AC;
@@ -294,7 +298,7 @@ __device__ __forceinline__ void flux_adjoint(const double* l, const double* r, b
     FR[4] = (R.G + R.P) * vr;
     const double sum = AP + AM;
     const bool live = sum > kTiny;
-    const double rden = 1.0 / (live ? sum : kTiny);
+    const double rden = recip(live ? sum : kTiny);
     double lden = 0.0;
     double lFL[5], lFR[5];
 #pragma unroll

@@ -176,9 +176,13 @@ __global__ void chart_detect_shock_kernel(const ChartBrick* __restrict__ cb, int
       int q[3] = {t[0], t[1], t[2]};
       q[e] -= 1;
       if (q[e] < 0 && B.box.bc[e][0] != BC_NEIGHBOR) continue;
-      const ChartBrick& S = cb[chart_owner(cb, b, q)];
       double P1, v1[3];
-      chart_p_v<PST>(S, ph, q, P1, v1);
+      if (q[e] >= 0) {
+        chart_p_v<PST>(B, ph, q, P1, v1);
+      } else {
+        const ChartBrick& S = cb[chart_owner(cb, b, q)];
+        chart_p_v<PST>(S, ph, q, P1, v1);
+      }
       if (shock_between(P0, P1, v0[e] - v1[e], ph.shock_threshold)) bits |= (uint8_t)(1u << e);
     }
     B.sb[c] = bits;
@@ -210,7 +214,13 @@ __global__ void chart_detect_flags_kernel(const ChartBrick* __restrict__ cb, int
         keep = false;
     uint8_t bits = 0;
     if (keep) {
+      // reads reach one cell either way: inside the brick (all but its outer
+      // layer) they index its own bits, else they cross into the neighbours
+      const bool inside = t[0] >= 1 && t[1] >= 1 && t[2] >= 1 && t[0] <= B.box.n[0] - 2 &&
+                          t[1] <= B.box.n[1] - 2 && t[2] <= B.box.n[2] - 2;
+      const long long sy = B.box.n[0], sz = (long long)B.box.n[0] * B.box.n[1];
       auto bit = [&](int e, int dx, int dy, int dz) -> bool {
+        if (inside) return (B.sb[c + dx + dy * sy + dz * sz] >> e) & 1;
         int q[3] = {t[0] + dx, t[1] + dy, t[2] + dz};
         const ChartBrick& S = cb[chart_owner(cb, b, q)];
         if (!chart_inside(S.box, q)) return false;
@@ -238,18 +248,50 @@ __global__ void chart_detect_flags_kernel(const ChartBrick* __restrict__ cb, int
 // value of the cell it images, in whichever brick that lies (the reference's
 // exchanged increments keep it equal to that cell); every other ghost keeps
 // its conserved values through the floors of ComputeFromConserved.
+// The ghost values of every brick, one thread per value of the bricks' ghost
+// shells (s_off: prefix sums of nV - nP over the bricks; the shell of a brick
+// is its two z ghost planes at each end, the y ghost rows and the x ghost
+// columns of its proper planes).
+__device__ __forceinline__ int chart_find_shell(const ChartBrick* cb, int n, long long x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cb[mid].v_off - cb[mid].c_off <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 __global__ void chart_ghost_refresh_kernel(const ChartBrick* __restrict__ cb, int n,
                                            long long total, Phys ph, const int* skip) {
   if (skip && *skip) return;
   for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
        x += (long long)gridDim.x * blockDim.x) {
-    const int b = chart_find(cb, n, x, false);
+    const int b = chart_find_shell(cb, n, x);
     const ChartBrick& B = cb[b];
-    const long long v = x - B.v_off, nV = B.box.nV;
-    int t[3];
-    decode3(v, B.box.m[0], B.box.m[1], t[0], t[1], t[2]);
-    int p[3] = {t[0] - 2, t[1] - 2, t[2] - 2};
-    if (chart_inside(B.box, p)) continue;
+    const long long u = x - (B.v_off - B.c_off), nV = B.box.nV;
+    const long long m0 = B.box.m[0], m1 = B.box.m[1], m2 = B.box.m[2];
+    const long long n1 = B.box.n[1], n2 = B.box.n[2];
+    const long long gz = 4 * m0 * m1, gy = 4 * m0 * n2;
+    long long i, j, k;
+    if (u < gz) {  // planes k = 0, 1, m2 - 2, m2 - 1
+      const long long s = u / (m0 * m1), r = u - s * m0 * m1;
+      k = (s < 2) ? s : m2 - 4 + s;
+      j = r / m0;
+      i = r - j * m0;
+    } else if (u < gz + gy) {  // rows j = 0, 1, m1 - 2, m1 - 1 of the proper planes
+      const long long w = u - gz, s = w / (m0 * n2), r = w - s * m0 * n2;
+      j = (s < 2) ? s : m1 - 4 + s;
+      k = 2 + r / m0;
+      i = r - (k - 2) * m0;
+    } else {  // columns i = 0, 1, m0 - 2, m0 - 1 of the proper rows
+      const long long w = u - gz - gy, s = w / (n1 * n2), r = w - s * n1 * n2;
+      i = (s < 2) ? s : m0 - 4 + s;
+      k = 2 + r / n1;
+      j = 2 + (r - (k - 2) * n1);
+    }
+    const long long v = i + m0 * (j + m1 * k);
+    int p[3] = {(int)i - 2, (int)j - 2, (int)k - 2};
     if (chart_reachable(B, p)) {
       int c[3] = {p[0], p[1], p[2]};
       const ChartBrick& S = cb[chart_owner(cb, b, c)];

@@ -84,6 +84,36 @@ __device__ __forceinline__ double markstein(double a, double b, double r) {
   return __fma_rn(e1, r, q1);
 }
 
+// 1 / b for a normal b: correctly rounded in the exact build; in the speed
+// build the hardware's approximate reciprocal (PTX rcp.approx.ftz.f64)
+// refined by two Newton-Raphson steps y <- y + y (1 - b y), each a pair of
+// fused multiply-adds, which leaves it within about an ulp.
+__device__ __forceinline__ double recip(double b) {
+#if GFX_FAST_MATH
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  return __fma_rn(y, e, y);
+#else
+  return 1.0 / b;
+#endif
+}
+
+// The sound speed sqrt(gamma P / N) for N > 0 and P > 0 (Apply_EOS_I_E_Kernel,
+// Fluid_P_I__Kernel.f90:244-267): as written in the exact build; in the speed
+// build a rsqrt(a N) with a = gamma P, one reciprocal square root (CUDA's
+// rsqrt, within an ulp) instead of a division and a square root.
+__device__ __forceinline__ double sound_speed(double P, double N, const Phys& ph) {
+#if GFX_FAST_MATH
+  const double a = ph.gamma * P;
+  return a * rsqrt(a * N);
+#else
+  return sqrt(ph.gamma * P / N);
+#endif
+}
+
 // |x| == 0 or 2^-900 <= |x| < 2^1001 (NaN and infinities fail).
 __device__ __forceinline__ bool exp_in_range(double x) {
   const double ax = fabs(x);
@@ -302,7 +332,7 @@ __device__ __forceinline__ void face_state(double N, double V1, double V2, doubl
   const double P = ph.gm1 * E;
   double CS = 0.0, SB = -kSqrtHuge;
   if (N > 0.0 && P > 0.0) {
-    CS = sqrt(ph.gamma * P / N);
+    CS = sound_speed(P, N, ph);
     if (NF == 6) SB = entropy_per_baryon(P, N, ph);
   }
   if (N < 0.0) N = 0.0;
@@ -347,7 +377,11 @@ __device__ __forceinline__ void riemann_flux(const FaceState& L, const FaceState
     const double fsl = mom<D>(L) * vl + L.P, fsr = mom<D>(R) * vr + R.P;
     const double MD = AP * R.D + AM * L.D - fdr + fdl;
     const double SN = AP * mom<D>(R) + AM * mom<D>(L) - fsr + fsl;
+#if GFX_FAST_MATH
+    const double MDinv = fmax2(MD, 0.0) * recip(fmax2(MD * MD, kTiny));
+#else
     const double MDinv = fmax2(MD, 0.0) / fmax2(MD * MD, kTiny);
+#endif
     const double AC = SN * MDinv;
     if (!diffusive && AP != 0.0 && AM != 0.0) {
       const FaceState& S = (AC >= 0.0) ? L : R;
@@ -360,7 +394,7 @@ __device__ __forceinline__ void riemann_flux(const FaceState& L, const FaceState
         A_V = AP - vs;
         A_AC = AP - AC;
       }
-      const double inv = 1.0 / fmax2(fabs(A_AC), kSqrtTiny);
+      const double inv = recip(fmax2(fabs(A_AC), kSqrtTiny));
       const double Dc = S.D * A_V * inv;
       const double v1 = (D == 0) ? AC : S.V1;
       const double v2 = (D == 1) ? AC : S.V2;
@@ -402,7 +436,7 @@ __device__ __forceinline__ void riemann_flux(const FaceState& L, const FaceState
   const double UL[6] = {L.D, L.S1, L.S2, L.S3, L.G, L.DS};
   const double UR[6] = {R.D, R.S1, R.S2, R.S3, R.G, R.DS};
   const double den = fmax2(AP + AM, kTiny);
-  const double rden = 1.0 / den;
+  const double rden = recip(den);
   const double apam = AP * AM;
   double num[NF];
   bool ok = true;
@@ -544,7 +578,7 @@ __device__ __forceinline__ void eos_cell(double N, double E, const Phys& ph, dou
                                          double& CS, double* SB) {
   P = ph.gm1 * E;
   if (N > 0.0 && P > 0.0) {
-    CS = sqrt(ph.gamma * P / N);
+    CS = sound_speed(P, N, ph);
     if (SB) *SB = entropy_per_baryon(P, N, ph);
   } else {
     CS = 0.0;

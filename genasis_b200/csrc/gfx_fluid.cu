@@ -2234,8 +2234,9 @@ int enqueue_chart_step(gfx_fluid_chart* C, bool detect, bool from_wn, cudaStream
                               C->counters, C->ph, s));
   CUDA_TRY(launch_stage_chart(MODE_STAGE2, true, C->hllc, C->grav, C->d2, C->items,
                               C->n_items, C->counters + 1, C->ph, s));
-  chart_ghost_refresh_kernel<<<grid_for(C->total_v, blk), blk, 0, s>>>(C->cb, C->n,
-                                                                       C->total_v, C->ph, skip);
+  const long long shell = C->total_v - C->total_c;
+  chart_ghost_refresh_kernel<<<grid_for(shell, blk), blk, 0, s>>>(C->cb, C->n, shell, C->ph,
+                                                                  skip);
   CUDA_TRY(cudaGetLastError());
   C->launches += 3;
   return GFX_OK;

@@ -134,6 +134,9 @@ __device__ __forceinline__ int bc_map(int g, int n, int bc_lo, int bc_hi, bool& 
 template <bool CH>
 __device__ __forceinline__ const BrickDesc& cell_owner(const BrickDesc& B, int* c) {
   if (!CH) return B;
+  if ((unsigned)c[0] < (unsigned)B.n[0] && (unsigned)c[1] < (unsigned)B.n[1] &&
+      (unsigned)c[2] < (unsigned)B.n[2])
+    return B;  // the common case: inside the brick
   const BrickDesc* S = &B;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -878,7 +881,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         const double w0 = gxc[G_W * LX + tx + 2], w1 = gyc[G_W * LY + ty + 2],
                      w2 = __ldg(GZ.W + k + 2);
         const double vol = w0 * w1 * w2;
-        const double rvol = 1.0 / vol;
+        const double rvol = recip(vol);
         const double ax = w1 * w2, ay = w2 * w0, az = w0 * w1;
         const long long gidx =
             (gx + 2) + (long long)B.m[0] * ((gy + 2) + (long long)B.m[1] * (k + 2));
