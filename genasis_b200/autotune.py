@@ -28,9 +28,9 @@ import os
 from . import problems
 from .fluid import FluidBox, _torch
 
-Z_CANDIDATES = (0, 8, 16, 32, 64)
+Z_CANDIDATES = (0, 8, 16, 24, 32, 48, 64, 96)
 ROW_CANDIDATES = (8, 16)
-SEGMENT_CANDIDATES = (4, 8, 16, 32)
+SEGMENT_CANDIDATES = (4, 8, 12, 16, 32)
 BATCH_Z_CANDIDATES = (8, 16, 24, 32, 48, 64, 96)
 _HERE = os.path.dirname(os.path.abspath(__file__))
 

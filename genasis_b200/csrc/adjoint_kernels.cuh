@@ -58,8 +58,20 @@ __device__ __forceinline__ void adj_flush(const AdjDesc& A, int D, long long bas
   }
 }
 
+// CTAs of 128 threads per SM that the reverse sweep's registers must allow:
+// 3 (168 registers) in the exact build; 4 (128 registers, more spills but 16
+// warps per SM) in the fast build, measured 3 % faster there at 128^3
+#ifndef GFX_ADJ_MIN_BLOCKS
+#if GFX_FAST_MATH
+#define GFX_ADJ_MIN_BLOCKS 4
+#else
+#define GFX_ADJ_MIN_BLOCKS 3
+#endif
+#endif
+
 template <int D, bool HLLC>
-__global__ void __launch_bounds__(128, 3) adj_face_kernel(const __grid_constant__ AdjDesc A,
+__global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
+    adj_face_kernel(const __grid_constant__ AdjDesc A,
                                                        const __grid_constant__ Phys ph) {
   constexpr int T1 = (D == 0) ? 1 : 0;
   constexpr int T2 = (D == 2) ? 1 : 2;
