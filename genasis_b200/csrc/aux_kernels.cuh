@@ -594,6 +594,66 @@ __global__ void check_state_kernel(Box b, Phys ph, const double* __restrict__ U,
   if (floor) atomicAdd(counts + 1, floor);
 }
 
+// The Sources records of one RK2 stage, over the ghost layout of S [10][nV]:
+//   S_u  = S_u + (B K_u) / dt, u < 6, every value (RecordDivergenceKernel,
+//          Step_RK_C_ASC__Kernel.f90:12-46, after the stage's divergence,
+//          Step_RK_C_ASC__Template.f90:1548-1595); K is that divergence alone,
+//          with zero ghosts, so the ghosts record zero;
+//   S_6  = S_6 - N (V . g) B          (Gravitational_G)
+//   S_7+d = S_7+d - N g_d B, d < 3    (Gravitational_S_D)
+//          on proper cells with the uniform gradient g = (0, 0, a)
+//          (ApplyGravity_F__Command.f90:23-264, the Sources halves of
+//          ApplyGravityMomentum and ApplyGravityEnergy; baryon mass 1);
+//          zero elsewhere, and zero everywhere without gravity.
+// FIRST: stage 1, where the records start from zero (the reference clears
+// them there).  N, V: the primitives of the stage's input state, from P
+// (compact) when given, else recovered from U as the stage recovers them.
+template <bool FIRST>
+__global__ void record_sources_kernel(Box b, Phys ph, const double* __restrict__ K,
+                                      const double* __restrict__ dt_ptr, double weight,
+                                      const double* __restrict__ U,
+                                      const double* __restrict__ P, double* __restrict__ S) {
+  const double dt = *dt_ptr;
+  const bool grav = ph.accel != 0.0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < b.nV;
+       v += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < 6; ++u) {
+      const double s = FIRST ? 0.0 : S[u * b.nV + v];
+      S[u * b.nV + v] = s + weight * K[u * b.nV + v] / dt;
+    }
+    double g[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) g[q] = FIRST ? 0.0 : S[(6 + q) * b.nV + v];
+    int i, j, k;
+    decode3(v, b.m[0], b.m[1], i, j, k);
+    i -= 2;
+    j -= 2;
+    k -= 2;
+    if (grav && i >= 0 && j >= 0 && k >= 0 && i < b.n[0] && j < b.n[1] && k < b.n[2]) {
+      Prim w;
+      if (P) {
+        const long long c = i + (long long)b.n[0] * (j + (long long)b.n[1] * k);
+        w.N = P[c];
+        w.V1 = P[b.nP + c];
+        w.V2 = P[2 * b.nP + c];
+        w.V3 = P[3 * b.nP + c];
+        w.E = P[4 * b.nP + c];
+      } else {
+        Cons c{U[v], U[b.nV + v], U[2 * b.nV + v], U[3 * b.nV + v], U[4 * b.nV + v]};
+        cons_to_prim(c, w, ph.nmin);
+      }
+      const double a = ph.accel;
+      g[0] = g[0] - w.N * (w.V1 * 0.0 + w.V2 * 0.0 + w.V3 * a) * weight;
+      g[1] = g[1] - w.N * 0.0 * weight;
+      g[2] = g[2] - w.N * 0.0 * weight;
+      g[3] = g[3] - w.N * a * weight;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) S[(6 + q) * b.nV + v] = g[q];
+  }
+}
+
 __global__ void reset_bits_kernel(unsigned long long* __restrict__ bits, int n, int* counter,
                                   int n_counters) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < n_counters;

@@ -204,6 +204,7 @@ struct gfx_fluid {
   int tile_y = kTileY;  // tile rows of the work list (8 or 16)
   unsigned long long* state_counts = nullptr;  // [2] for gfx_fluid_check_state
   double* partials = nullptr;                  // per-block sums of gfx_fluid_totals
+  double* Ksrc = nullptr;  // [6][nV]: a stage's divergence for gfx_fluid_step_sources
   double* wn = nullptr;  // [5][nP]: the primitives of the state the last stage 2 wrote
   const double* wn_of = nullptr;  // that state (null when unknown or since rewritten)
   // pipelined gfx_fluid_step_host: copy streams, per-slab events and counters
@@ -512,15 +513,44 @@ int run_features_wn(gfx_fluid* h, const double* U, cudaStream_t s) {
   return run_features(h, U, h->wn, s);
 }
 
+// The Sources records of RK2 stage `stage` (0, 1) into S [10][nV]: the
+// stage's divergence increment once more, from the input the fused stage
+// reads (U, or the compact primitives P when in_prim), by the increment
+// kernel into the scratch Ksrc (the same arithmetic, so the same K as the
+// stage's before its gravity term), then the records.  counter: a work
+// counter zeroed for this launch.
+int enqueue_sources(gfx_fluid* h, const double* U, const double* P, bool in_prim,
+                    const uint8_t* df, const double* dt_ptr, int stage, double* S, int* counter,
+                    cudaStream_t s) {
+  const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
+  const size_t bytes = 6 * (size_t)h->box.nV * sizeof(double);
+  CUDA_TRY(cudaMemsetAsync(h->Ksrc, 0, bytes, s));
+  BrickDesc d = make_desc(h, U, nullptr, h->Ksrc, in_prim ? P : nullptr, df, nullptr, dt_ptr,
+                          0.5, nullptr);
+  CUDA_TRY(launch_stage(MODE_INCREMENT, in_prim, hllc, false, d, nullptr, h->items, h->n_items,
+                        counter, h->ph, s));
+  const int blk = 256;
+  if (stage == 0)
+    record_sources_kernel<true><<<grid_for(h->box.nV, blk), blk, 0, s>>>(
+        h->box, h->ph, h->Ksrc, dt_ptr, 0.5, U, in_prim ? P : nullptr, S);
+  else
+    record_sources_kernel<false><<<grid_for(h->box.nV, blk), blk, 0, s>>>(
+        h->box, h->ph, h->Ksrc, dt_ptr, 0.5, U, in_prim ? P : nullptr, S);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 2;
+  return GFX_OK;
+}
+
 // The launches of one RK2 step on U (in place).  dt_ptr, skip: device scalars.
 // detect: whether the shock flags must be recomputed from U first.  ev (may
 // be null): 5 events recorded between the phases for gfx_fluid_step_timed.
 // from_wn: the step follows a step of the same evolve, whose stage 2 stored
 // the primitives of U: shock detection and stage 1 read them instead of
-// recovering them from U.
+// recovering them from U.  sources (may be null): [10][nV], the step's
+// Sources records (gfx_fluid_step_sources; needs h->Ksrc).
 int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
                  double* fluence, bool detect, cudaStream_t s, cudaEvent_t* ev = nullptr,
-                 bool from_wn = false) {
+                 bool from_wn = false, double* sources = nullptr) {
   const bool hllc = h->cfg.riemann_solver == GFX_RIEMANN_HLLC;
   const bool grav = h->cfg.uniform_acceleration != 0.0;
   reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
@@ -536,12 +566,19 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
   if (ev) CUDA_TRY(cudaEventRecord(ev[1], s));
   const uint8_t* df = hllc ? h->df : nullptr;
   const bool in_prim = from_wn || h->prims_pending;
-  BrickDesc d1 = make_desc(h, U, nullptr, nullptr,
-                           from_wn ? h->wn : (h->prims_pending ? h->Pst : nullptr), df, fluence,
-                           dt_ptr, 0.5, skip);
+  const double* P1 = from_wn ? h->wn : (h->prims_pending ? h->Pst : nullptr);
+  if (sources) {
+    int rc = enqueue_sources(h, U, P1, in_prim, df, dt_ptr, 0, sources, h->counters + 2, s);
+    if (rc) return rc;
+  }
+  BrickDesc d1 = make_desc(h, U, nullptr, nullptr, P1, df, fluence, dt_ptr, 0.5, skip);
   CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, hllc, grav, d1, nullptr, h->items, h->n_items,
                         h->counters, h->ph, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[2], s));
+  if (sources) {
+    int rc = enqueue_sources(h, U, h->Yp, true, df, dt_ptr, 1, sources, h->counters + 3, s);
+    if (rc) return rc;
+  }
   BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fluence, dt_ptr, 0.5, skip);
   d2.wn = h->wn;
   CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
@@ -966,6 +1003,7 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->partials);
   cudaFree(h->wn);
   cudaFree(h->slab_counters);
+  cudaFree(h->Ksrc);
   cudaFree(h->host_items);
   for (int j = 0; j < kMaxSlabs; ++j) {
     if (h->ev_in[j]) cudaEventDestroy(h->ev_in[j]);
@@ -1090,6 +1128,27 @@ int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* st
   h->launches += 1;
   const bool detect = (h->features == FEAT_PENDING);
   int rc = enqueue_step(h, U, h->dt_slot, nullptr, fluence, detect, s);
+  if (rc) return rc;
+  h->prims_pending = false;
+  h->features = FEAT_PENDING;
+  h->features_src = U;
+  h->wn_of = U;
+  return GFX_OK;
+}
+
+int gfx_fluid_step_sources(gfx_fluid* h, double* U, double dt, double* fluence,
+                           double* sources, void* stream) {
+  if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_sources")) return rc0;
+  if (!h || !U || !sources) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
+  if (!h->Ksrc && cudaMalloc(&h->Ksrc, 6 * (size_t)h->box.nV * sizeof(double)) != cudaSuccess)
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc sources scratch");
+  cudaStream_t s = (cudaStream_t)stream;
+  set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 1;
+  const bool detect = (h->features == FEAT_PENDING);
+  int rc = enqueue_step(h, U, h->dt_slot, nullptr, fluence, detect, s, nullptr, false, sources);
   if (rc) return rc;
   h->prims_pending = false;
   h->features = FEAT_PENDING;

@@ -22,6 +22,9 @@ import numpy as np
 from . import lib
 from .config import FluidConfig
 
+# Fields of the Sources records (GFX_N_SOURCES of the C header)
+N_SOURCES = 10
+
 
 def _torch():
     import torch  # noqa: WPS433 (device memory and streams only)
@@ -143,6 +146,19 @@ class FluidBox:
         self.call("gfx_fluid_step", self.h, _ptr(self.U), float(time_step), _ptr(fluence),
                  _stream())
 
+    def step_sources(self, time_step, fluence=None, sources=None):
+        """The step of `step` (the same state bit for bit) with the reference's
+        Sources records (Step_RK_C_ASC ApplyDivergence_C / RecordDivergenceKernel,
+        ApplyGravity_F): a [10, *shape] tensor of the divergence sources of
+        D, S_1, S_2, S_3, G, DS, then Gravitational_G and Gravitational_S_D 1-3."""
+        torch = _torch()
+        if sources is None:
+            sources = torch.empty((N_SOURCES,) + tuple(self.config.shape), dtype=torch.float64,
+                                  device=self.device)
+        self.call("gfx_fluid_step_sources", self.h, _ptr(self.U), float(time_step),
+                  _ptr(fluence), _ptr(sources), _stream())
+        return sources
+
     def step_host(self, U_host, time_step, fluence_host=None):
         """One step on a host (ideally pinned) tensor: copy in, step, copy out."""
         self.call("gfx_fluid_step_host", self.h, _ptr(U_host), float(time_step),
@@ -200,13 +216,22 @@ class Step_RK2_C_ASC:
     """Step_RK_C_ASC_Template % Compute (Step_RK_C_ASC__Template.f90:504-542)
     on a FluidBox's current."""
 
-    def __init__(self, box: FluidBox):
+    def __init__(self, box: FluidBox, record_sources=False):
         self.box = box
         self.boundary_fluence = box.new_fluence()
+        # the current's Sources (Sources_F) when the step records them
+        self.sources = None
+        if record_sources:
+            torch = _torch()
+            self.sources = torch.zeros((N_SOURCES,) + tuple(box.config.shape),
+                                       dtype=torch.float64, device=box.device)
 
     def compute(self, time, time_step):
         del time  # the RK2 stages of this fluid do not depend on the time
-        self.box.step(time_step, self.boundary_fluence)
+        if self.sources is not None:
+            self.box.step_sources(time_step, self.boundary_fluence, self.sources)
+        else:
+            self.box.step(time_step, self.boundary_fluence)
 
 
 class IncrementDivergence_FV:

@@ -47,6 +47,7 @@ SIGNATURES = {
     "gfx_fluid_increment": [P, P, P, D, D, P, P],
     "gfx_fluid_fluence_face_size": [P, ctypes.POINTER(SZ)],
     "gfx_fluid_step": [P, P, D, P, P],
+    "gfx_fluid_step_sources": [P, P, D, P, P, P],
     "gfx_fluid_step_host": [P, P, D, P],
     "gfx_fluid_timestep": [P, P, I, ctypes.POINTER(D), P],
     "gfx_fluid_evolve": [P, P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I), P],

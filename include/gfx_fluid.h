@@ -131,6 +131,26 @@ int gfx_fluid_fluence_face_size(const gfx_fluid *h, size_t *face_size);
 int gfx_fluid_step(gfx_fluid *h, double *U_dev, double dt, double *fluence_dev,
                    void *stream);
 
+/* gfx_fluid_step that also keeps the reference's Sources records of the step
+ * in sources_dev ([GFX_N_SOURCES][nV], ghost layout, overwritten):
+ *   fields 0-5  the divergence sources of D, S_1, S_2, S_3, G, DS: the sum over
+ *               the stages of B_s K_s / dt, K_s the stage's divergence
+ *               increment (ApplyDivergence_C and RecordDivergenceKernel,
+ *               Step_RK_C_ASC__Template.f90:1548-1595,
+ *               Step_RK_C_ASC__Kernel.f90:12-46); zero on ghosts;
+ *   field 6     Gravitational_G, fields 7-9 Gravitational_S_D (1:3): the sum
+ *               over the stages of -B_s N (V . g) and -B_s N g_d on proper
+ *               cells (ApplyGravity_F__Command.f90:23-264), zero elsewhere and
+ *               without gravity.
+ * These are Sources_F's fields 1-6, N_CONSERVED + 1 and N_CONSERVED + 9..11
+ * (Sources_F__Form.f90:157-167), in that order.  The state, fluence and
+ * shock flags are bit for bit those of gfx_fluid_step; the divergence of
+ * each stage is computed a second time for the records.  Allocates a
+ * [6][nV] scratch on the first call. */
+#define GFX_N_SOURCES 10
+int gfx_fluid_step_sources(gfx_fluid *h, double *U_dev, double dt, double *fluence_dev,
+                           double *sources_dev, void *stream);
+
 /* The same step with U in host memory (pinned for speed): copies in, steps,
  * copies out, and returns after the result is back on the host.  The copies
  * and the compute overlap over z slabs (bit-identical to gfx_fluid_step); the

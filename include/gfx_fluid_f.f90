@@ -58,7 +58,8 @@ module GFX_Fluid_C
     gfx_fluid_n_values, gfx_fluid_geometry, gfx_fluid_from_primitive, &
     gfx_fluid_to_primitive, gfx_fluid_detect_features, &
     gfx_fluid_clear_features, gfx_fluid_get_features, gfx_fluid_increment, &
-    gfx_fluid_fluence_face_size, gfx_fluid_step, gfx_fluid_step_host, &
+    gfx_fluid_fluence_face_size, gfx_fluid_step, gfx_fluid_step_sources, &
+    gfx_fluid_step_host, &
     gfx_fluid_timestep, gfx_fluid_evolve, gfx_fluid_step_timed, &
     gfx_fluid_kernel_launches, gfx_fluid_step_adjoint, gfx_fluid_step_branches, &
     gfx_fluid_set_tuning, gfx_fluid_batch_create, gfx_fluid_batch_destroy, &
@@ -163,6 +164,14 @@ module GFX_Fluid_C
       type ( c_ptr ), value :: Handle, Conserved_dev, Fluence_dev, Stream
       real ( c_double ), value :: TimeStep
     end function gfx_fluid_step
+
+    integer ( c_int ) function gfx_fluid_step_sources &
+      ( Handle, Conserved_dev, TimeStep, Fluence_dev, Sources_dev, Stream ) &
+      bind ( c, name = 'gfx_fluid_step_sources' )
+      import
+      type ( c_ptr ), value :: Handle, Conserved_dev, Fluence_dev, Sources_dev, Stream
+      real ( c_double ), value :: TimeStep
+    end function gfx_fluid_step_sources
 
     integer ( c_int ) function gfx_fluid_step_host &
       ( Handle, Conserved_host, TimeStep, Fluence_host ) &

@@ -733,19 +733,23 @@ void ora_increment(ora_fluid *f, double *K, double dt, double weight, double *fl
 
 /* ApplyGravity_F (ApplyGravity_F__Command.f90:23-264) with the uniform
  * potential gradient (0, 0, a) of Geometry_ASC__Kernel.f90:68-90. */
-static void apply_gravity(ora_fluid *f, double **Kc, double dt) {
+static void apply_gravity(ora_fluid *f, double **Kc, double dt, double weight, double *src) {
   const double a = f->c.uniform_acceleration;
   if (a == 0.0) return;
   const double M = f->mass;
   const double grad[3] = {0.0, 0.0, a};
   int g = f->g;
+  /* Sources_F: Gravitational_G, then Gravitational_S_D (1:3) */
+  double *SG = src ? src + (size_t)NCONS * f->nV : NULL;
   for (int d = 0; d < 3; ++d) {
+    double *SS = src ? src + (size_t)(NCONS + 1 + d) * f->nV : NULL;
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = g; k < g + f->n[2]; ++k)
       for (int j = g; j < g + f->n[1]; ++j)
         for (int i = g; i < g + f->n[0]; ++i) {
           size_t iV = idx3(f, i, j, k);
           Kc[1 + d][iV] = Kc[1 + d][iV] - M * f->D[iV] * grad[d] * dt;
+          if (SS) SS[iV] = SS[iV] - M * f->D[iV] * grad[d] * weight;
         }
   }
 #pragma omp parallel for collapse(2) schedule(static)
@@ -757,7 +761,29 @@ static void apply_gravity(ora_fluid *f, double **Kc, double dt) {
                                     (f->V[0][iV] * grad[0] + f->V[1][iV] * grad[1] +
                                      f->V[2][iV] * grad[2]) *
                                     dt;
+        if (SG)
+          SG[iV] = SG[iV] - M * f->D[iV] *
+                                (f->V[0][iV] * grad[0] + f->V[1][iV] * grad[1] +
+                                 f->V[2][iV] * grad[2]) *
+                                weight;
       }
+}
+
+/* RecordDivergenceKernel (Step_RK_C_ASC__Kernel.f90:12-46) as
+ * ApplyDivergence_C calls it after the stage's divergence
+ * (Step_RK_C_ASC__Template.f90:1548-1595): the records are cleared in stage
+ * 1, then S = S + Weight_RK * K / dt over every value of each conserved
+ * field.  In stage 1 the gravitational records are cleared too
+ * (ApplyGravity_F__Command.f90:68-92). */
+static void record_divergence(ora_fluid *f, double **Kc, double dt, double weight, int s,
+                              double *src) {
+  const long long n = (long long)f->nV;
+  if (s == 0) memset(src, 0, sizeof(double) * (NCONS + 4) * f->nV);
+  for (int u = 0; u < NCONS; ++u) {
+    double *S = src + (size_t)u * f->nV, *K = Kc[u];
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < n; ++i) S[i] = S[i] + weight * K[i] / dt;
+  }
 }
 
 /* ---------------------------------------------------------------------- */
@@ -924,15 +950,22 @@ static void multiply_add(double **A, double **B, double c, size_t nV) {
 }
 
 /* ComputeStage_C (Step_RK_C_ASC__Template.f90:1148-1260) for stage s. */
-static void compute_stage(ora_fluid *f, int s, double dt, double weight, double *fluence) {
+static void compute_stage(ora_fluid *f, int s, double dt, double weight, double *fluence,
+                          double *src) {
   double **Kc = f->K[s];
   for (int u = 0; u < NCONS; ++u) memset(Kc[u], 0, sizeof(double) * f->nV);
   for (int d = 0; d < 3; ++d) compute_direction(f, d, Kc, dt, weight, fluence);
-  apply_gravity(f, Kc, dt);
+  if (src) record_divergence(f, Kc, dt, weight, s, src);
+  apply_gravity(f, Kc, dt, weight, src);
   exchange_ghosts(f, Kc, NCONS);
 }
 
-void ora_step(ora_fluid *f, double dt, double *fluence) {
+void ora_step(ora_fluid *f, double dt, double *fluence) { ora_step_sources(f, dt, fluence, NULL); }
+
+/* src (may be NULL): [NCONS + 4][nV], the step's Sources records -- the
+ * divergence sources of the conserved fields, then Gravitational_G and
+ * Gravitational_S_D (1:3), Sources_F__Form.f90:157-167. */
+void ora_step_sources(ora_fluid *f, double dt, double *fluence, double *src) {
   const double A21 = 1.0, B[2] = {0.5, 0.5};
   double *cur[NCONS];
   cons_fields(f, cur);
@@ -940,13 +973,13 @@ void ora_step(ora_fluid *f, double dt, double *fluence) {
   /* LoadSolution: Solution = Current conserved */
   copy_fields(f->Sol, cur, f->nV);
   /* stage 1 */
-  compute_stage(f, 0, dt, B[0], fluence);
+  compute_stage(f, 0, dt, B[0], fluence, src);
   /* stage 2: Y = Solution; Y += A21 K1; StoreSolution_C(Y) without features */
   copy_fields(f->Y, f->Sol, f->nV);
   multiply_add(f->Y, f->K[0], A21, f->nV);
   copy_fields(cur, f->Y, f->nV);
   cons_to_prim_all(f);
-  compute_stage(f, 1, dt, B[1], fluence);
+  compute_stage(f, 1, dt, B[1], fluence, src);
   /* assemble: Solution += B_s K_s */
   multiply_add(f->Sol, f->K[0], B[0], f->nV);
   multiply_add(f->Sol, f->K[1], B[1], f->nV);

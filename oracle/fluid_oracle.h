@@ -75,6 +75,8 @@ void ora_increment(ora_fluid *f, double *K, double dt, double weight_rk,
                    double *fluence);
 /* Step_RK2_C_ASC % Compute: one RK2 step of size dt. fluence may be NULL. */
 void ora_step(ora_fluid *f, double dt, double *fluence);
+/* ora_step that also keeps the Sources records in src ([10][nV]). */
+void ora_step_sources(ora_fluid *f, double dt, double *fluence, double *src);
 /* Integrator_C_PS ComputeTimeStep: Courant * CFL dt, ramped by iCycle. */
 double ora_timestep(const ora_fluid *f, int i_cycle);
 /* Max inverse time step over proper cells (before Courant / ramp). */

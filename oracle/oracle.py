@@ -71,6 +71,7 @@ def _load():
     lib.ora_detect_features.argtypes = [P]
     lib.ora_increment.argtypes = [P, P, D, D, P]
     lib.ora_step.argtypes = [P, D, P]
+    lib.ora_step_sources.argtypes = [P, D, P, P]
     lib.ora_timestep.restype = D
     lib.ora_timestep.argtypes = [P, ctypes.c_int]
     lib.ora_inverse_timestep.restype = D
@@ -192,6 +193,14 @@ class Oracle:
     def step(self, dt, fluence=None):
         fl = _ptr(fluence) if fluence is not None else None
         self.lib.ora_step(self.h, float(dt), fl)
+
+    def step_sources(self, dt, fluence=None):
+        """One step; returns its Sources records [10][nV]: the divergence
+        sources of the six conserved fields, Gravitational_G, Gravitational_S_D."""
+        fl = _ptr(fluence) if fluence is not None else None
+        src = np.zeros((10, self.nV))
+        self.lib.ora_step_sources(self.h, float(dt), fl, _ptr(src))
+        return src
 
     def timestep(self, i_cycle):
         return float(self.lib.ora_timestep(self.h, int(i_cycle)))
