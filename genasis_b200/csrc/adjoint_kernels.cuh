@@ -215,6 +215,117 @@ __global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
   }
 }
 
+// L^T along x with one lane per face.  x pencils are contiguous, so a thread
+// sweeping a segment of one (adj_face_kernel<0>) strides its warp's loads and
+// atomic adds over many cache lines; here a warp takes kAdjXFaces
+// consecutive faces x0 .. x0 + 28 of one pencil instead.  Lane L holds cell
+// c = x0 - 2 + L: its primitives and lamK come in coalesced, the stencil
+// neighbours by shuffles.  Lanes 1 .. 30 compute the slope of their cell,
+// lanes 2 .. 30 the adjoint of face c (between cells c - 1 and c); the
+// adjoints of the face states go back through the slopes of cells c - 1 and
+// c to the cells c - 2 .. c + 1, and every lane adds its cell's sum into
+// lamW with one coalesced atomic add per field (the three cells at each end
+// of the warp's range are shared with the neighbouring warp).  A cell's sum
+// is formed in the order of the sweep: face c, slope c - 1, face c + 1,
+// slope c, slope c + 1.
+constexpr int kAdjXFaces = 29;
+
+template <bool HLLC>
+__global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
+    adj_face_x_kernel(const __grid_constant__ AdjDesc A, const __grid_constant__ Phys ph) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int n0 = A.n[0], n1 = A.n[1], n2 = A.n[2];
+  const int chunks = (n0 + 1 + kAdjXFaces - 1) / kAdjXFaces;
+  const long long warps = (long long)chunks * n1 * n2;
+  const int lane = threadIdx.x & 31;
+  const AxisGeo& G = A.geo[0];
+  const long long first = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long stride = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long wi = first; wi < warps; wi += stride) {  // uniform over the warp
+    const int chunk = (int)(wi % chunks);
+    const long long row = wi / chunks;
+    const long long base = row * n0;  // row = i1 + n1 i2
+    const int c = chunk * kAdjXFaces - 2 + lane;
+    // the cell's primitives (the boundary image for a ghost; lanes past the
+    // ghosts read a mapped proper cell and contribute nothing)
+    double w[5];
+    adj_load(A, 0, base, 1, c, w);
+    // the slope of the cell (needs c in [-1, n0] for its tables: clamped for
+    // the lanes whose slope no face uses)
+    const int tt = max(-1, min(c, n0)) + 2;
+    const double dxl = __ldg(G.dXI + tt), dxr = __ldg(G.dXI + tt + 1);
+    const double sql = __ldg(G.SQ + tt), sqr = __ldg(G.SQ + tt + 1), cden = __ldg(G.CDEN + tt);
+    const double rdxl = __ldg(G.RDXI + tt), rdxr = __ldg(G.RDXI + tt + 1),
+                 rcden = __ldg(G.RCDEN + tt);
+    double wm[5], sl[5], sm[5];
+    int branches = 0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      wm[q] = __shfl_up_sync(FULL, w[q], 1);
+      const double wp = __shfl_down_sync(FULL, w[q], 1);
+      int br;
+      sl[q] = limited_slope_branch(wm[q], w[q], wp, dxl, dxr, sql, sqr, cden, rdxl, rdxr, rcden,
+                                   ph.theta, ph.use_limiter, br);
+      branches |= br << (2 * q);
+      sm[q] = __shfl_up_sync(FULL, sl[q], 1);
+    }
+    // lamK of the cell times dt A / V, and the face's flux adjoint
+    double lk[5];
+    if (c >= 0 && c < n0) {
+      const double k = A.dt * __ldg(G.RW + c + 2) * A.kscale;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) lk[q] = k * __ldg(A.lamK + base + c + q * A.nP);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) lk[q] = 0.0;
+    }
+    const bool face = lane >= 2 && lane <= 30 && c <= n0;
+    const int fc = max(0, min(c, n0));
+    const double wr = __ldg(G.WR + fc + 1), wl = __ldg(G.WL + fc + 2);
+    double ll[5], lr[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const double lkm = __shfl_up_sync(FULL, lk[q], 1);
+      ll[q] = lk[q] - lkm;  // the flux adjoint lF, until the call below
+      lr[q] = 0.0;
+    }
+    if (face) {
+      double l[5], r[5], lF[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        l[q] = wm[q] + wr * sm[q];
+        r[q] = w[q] - wl * sl[q];
+        lF[q] = ll[q];
+        ll[q] = 0.0;
+      }
+      bool diff = false;
+      if (HLLC && A.df != nullptr && c < n0) diff = A.df[base + c] & 1;
+      flux_adjoint<0, HLLC>(l, r, diff, lF, ph, ll, lr);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) ll[q] = 0.0;
+    }
+    // face c + 1 (lane + 1) gives this cell ll and the slope adjoint wr ll;
+    // then the slope of every cell goes back to its three cells
+    double gl[5], gr[5], a[5], ls[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double llp = __shfl_down_sync(FULL, ll[q], 1);
+      double wllp = __shfl_down_sync(FULL, wr * ll[q], 1);
+      if (lane == 31) llp = wllp = 0.0;
+      ls[q] = -wl * lr[q] + wllp;
+      slope_coeffs((branches >> (2 * q)) & 3, sql, sqr, rdxl, rdxr, rcden, ph.theta, gl[q],
+                   gr[q]);
+      double from_left = __shfl_up_sync(FULL, gr[q] * ls[q], 1);
+      double from_right = __shfl_down_sync(FULL, gl[q] * ls[q], 1);
+      if (lane == 0) from_left = 0.0;
+      if (lane == 31) from_right = 0.0;
+      a[q] = (((lr[q] + from_left) + llp) + (gl[q] - gr[q]) * ls[q]) - from_right;
+    }
+    adj_flush(A, 0, base, 1, c, a);
+  }
+}
+
 // Primitives of the proper cells of U (ghost layout) into a compact array:
 // the stage-1 input W0 of the step.
 __device__ __forceinline__ long long ghost_index(const Box& b, long long c) {

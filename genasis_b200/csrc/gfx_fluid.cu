@@ -1992,7 +1992,14 @@ cudaError_t launch_adj_face(const AdjDesc& A, bool hllc, const Phys& ph, cudaStr
   constexpr int T2 = (D == 2) ? 1 : 2;
   const long long total = (long long)A.nseg * A.n[T1] * A.n[T2];
   const int blk = 128;
-  if (hllc)
+  if constexpr (D == 0) {  // one lane per face, a warp per kAdjXFaces faces of a pencil
+    const long long lanes =
+        32LL * ((A.n[0] + 1 + kAdjXFaces - 1) / kAdjXFaces) * A.n[1] * A.n[2];
+    if (hllc)
+      adj_face_x_kernel<true><<<grid_for(lanes, blk), blk, 0, s>>>(A, ph);
+    else
+      adj_face_x_kernel<false><<<grid_for(lanes, blk), blk, 0, s>>>(A, ph);
+  } else if (hllc)
     adj_face_kernel<D, true><<<grid_for(total, blk), blk, 0, s>>>(A, ph);
   else
     adj_face_kernel<D, false><<<grid_for(total, blk), blk, 0, s>>>(A, ph);
