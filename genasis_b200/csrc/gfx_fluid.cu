@@ -740,16 +740,15 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
   cudaStream_t sc = h->host_stream, si = h->copy_in, so = h->copy_out;
   double* U = h->U_stage;
   const size_t nV = (size_t)b.nV, plane = (size_t)b.m[0] * b.m[1];
+  // planes [p0, p1) of the first nf fields: one 2-D copy whose rows are the
+  // fields (pitch nV values on both sides), so that a slab is one transfer
   auto copy = [&](cudaStream_t st, int nf, int p0, int p1, cudaMemcpyKind kind) -> cudaError_t {
-    for (int q = 0; q < nf; ++q) {
-      const size_t off = q * nV + (size_t)p0 * plane;
-      double* dst = (kind == cudaMemcpyHostToDevice) ? U + off : U_host + off;
-      const double* src = (kind == cudaMemcpyHostToDevice) ? U_host + off : U + off;
-      cudaError_t e = cudaMemcpyAsync(dst, src, (size_t)(p1 - p0) * plane * sizeof(double),
-                                      kind, st);
-      if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    if (p1 <= p0) return cudaSuccess;
+    const size_t off = (size_t)p0 * plane;
+    double* dst = (kind == cudaMemcpyHostToDevice) ? U + off : U_host + off;
+    const double* src = (kind == cudaMemcpyHostToDevice) ? U_host + off : U + off;
+    return cudaMemcpy2DAsync(dst, nV * sizeof(double), src, nV * sizeof(double),
+                             (size_t)(p1 - p0) * plane * sizeof(double), nf, kind, st);
   };
   // inputs: the top planes first (a periodic z axis reads them from slab 0),
   // then the slabs; plane index P = z + 2 of the ghost layout

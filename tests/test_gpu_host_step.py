@@ -2,13 +2,21 @@
 computed and copied back on three streams) gives the device step's result
 bit for bit, state and boundary fluence, over consecutive steps, for every
 kind of z boundary, with thin first slabs and with slabs of several chunks
-(tall bricks)."""
+(tall bricks).
+
+The slabs cut z into pencils of their own.  The exact build rounds every
+operation separately, so where a pencil starts does not change a bit.  The
+fast build lets the compiler fuse multiply-adds, and the first face of a
+pencil (computed once per work item, out of line) may fuse differently from
+the faces of the plane loop; there the two paths agree to the last bits,
+within 1e-14 of each quantity per run of four steps."""
 import numpy as np
 import pytest
 
 from genasis_b200 import problems
 from genasis_b200.config import FluidConfig
-from tests.gpu_helpers import to_np
+from genasis_b200 import lib
+from tests.gpu_helpers import quantity_errors, to_np
 
 pytestmark = pytest.mark.gpu
 
@@ -58,7 +66,14 @@ def test_host_step_matches_the_device_step(name, z_chunk):
         dev.step(dt, fl_dev)
         hst.step_host(host, dt, fl_host)
         torch.cuda.synchronize()
-        assert torch.equal(host, dev.U.cpu()), (name, z_chunk, i)
-        assert np.array_equal(fl_host.numpy(), to_np(fl_dev)), (name, z_chunk, i)
+        if lib.default_variant() == "exact":
+            assert torch.equal(host, dev.U.cpu()), (name, z_chunk, i)
+            assert np.array_equal(fl_host.numpy(), to_np(fl_dev)), (name, z_chunk, i)
+        else:
+            every = (slice(None),) * 3
+            q = quantity_errors(host.numpy(), to_np(dev.U), every)
+            assert max(q) <= 1e-14, (name, z_chunk, i, q)
+            f = np.abs(fl_host.numpy() - to_np(fl_dev)).max()
+            assert f <= 1e-14 * max(np.abs(to_np(fl_dev)).max(), 1e-300), (name, z_chunk, i, f)
     dev.close()
     hst.close()
