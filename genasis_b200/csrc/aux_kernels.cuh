@@ -307,24 +307,57 @@ inline dim3 detect_grid(const Box& b, int k0, int k1) {
               (k1 - k0 + kDetKZ - 1) / kDetKZ);
 }
 
-// Shock bits (detect_shock_cell) and DIFFUSIVE_FLUX_I flags (detect_flags_cell)
-// of the proper cells of planes [k0, k1) in one pass, from the conserved state
-// U or (PST) from the compact primitives Pst (N, V1, V2, V3, E).  For every
-// plane kk each thread recovers pressure and velocities of its halo-tile
-// cell (its loads for plane kk + 1 are issued before the CTA synchronises),
-// forms the cell's shock bits from the -x and -y neighbours in shared memory
-// and the -z neighbour kept in registers, and the CTA keeps three planes of
-// bits in a ring; the flags of plane kk - 1 (threads 0-255, one per tile
-// cell) then read bits of planes kk - 2 to kk only.  A bit that no flag reads
-// (x at the left halo column, y at the bottom halo row, z at the first
-// plane) is left zero, and so is every bit outside the brick, which only
-// cells without flags would read.  Reads the state of planes k0 - 1 to k1
-// (those that exist); writes df of planes [k0, k1).
+// The state of one brick as the feature detection reads it: the compact
+// primitives (PST: E, V1, V2, V3 at N's place skipped) or the conserved
+// fields of the ghost layout, by proper coordinates; and its flags.  Offsets
+// fit in 32 bits (every brick has fewer than 2^31 values).
 template <bool PST>
-__global__ void __launch_bounds__(kDetThreads, 3)
-    detect_features_kernel(Box b, Phys ph, const double* __restrict__ U,
-                           const double* __restrict__ Pst, uint8_t* __restrict__ df, int k0,
-                           int k1) {
+struct DetectBrick {
+  const double* F[5];
+  int pitch, plane, gh;
+  int n0, n1;
+  uint8_t* df;
+  __device__ DetectBrick(const Box& b, const double* U, const double* Pst, uint8_t* df_)
+      : pitch(PST ? b.n[0] : b.m[0]), plane(PST ? b.n[0] * b.n[1] : b.m[0] * b.m[1]),
+        gh(PST ? 0 : 2), n0(b.n[0]), n1(b.n[1]), df(df_) {
+    const long long fs = PST ? b.nP : b.nV;
+    F[0] = PST ? Pst + 4 * fs : U;  // E, or D
+    F[1] = (PST ? Pst : U) + fs;
+    F[2] = F[1] + fs;
+    F[3] = F[2] + fs;
+    F[4] = F[3] + fs;  // G (U only)
+  }
+  __device__ __forceinline__ void load(int i, int j, int k, double* raw) const {
+    const int o = (i + gh) + pitch * (j + gh) + plane * (k + gh);
+    raw[0] = F[0][o];
+    raw[1] = F[1][o];
+    raw[2] = F[2][o];
+    raw[3] = F[3][o];
+    if (!PST) raw[4] = F[4][o];
+  }
+  __device__ __forceinline__ uint8_t* flags(int i, int j, int k) const {
+    return df + (i + n0 * (j + n1 * k));
+  }
+};
+
+// Shock bits (detect_shock_cell) and DIFFUSIVE_FLUX_I flags (detect_flags_cell)
+// of the proper cells of planes [k0, k1) of a box of n0 x n1 x n2 cells in one
+// pass, from the state that `src` reads (a brick, or a chart of bricks by
+// its global coordinates; raw values: E, V1, V2, V3 with PST, else D, S1,
+// S2, S3, G).  For every plane kk each thread recovers pressure and
+// velocities of its halo-tile cell (its loads for plane kk + 1 are issued
+// before the CTA synchronises), forms the cell's shock bits from the -x and
+// -y neighbours in shared memory and the -z neighbour kept in registers, and
+// the CTA keeps three planes of bits in a ring; the flags of plane kk - 1
+// (threads 0-255, one per tile cell) then read bits of planes kk - 2 to kk
+// only.  A bit that no flag reads (x at the left halo column, y at the bottom
+// halo row, z at the first plane) is left zero, and so is every bit outside
+// the box, which only cells without flags would read.  Reads the state of
+// planes k0 - 1 to k1 (those that exist); writes the flags of planes
+// [k0, k1).
+template <bool PST, class Src>
+__device__ __forceinline__ void detect_tile(const Src& src, const Phys& ph, int n0, int n1,
+                                            int n2, int k0, int k1) {
   constexpr int RX = kDetRX, NR = kDetNR;
   __shared__ double sP[NR], sV1[NR], sV2[NR];
   __shared__ uint8_t sS[3][NR];
@@ -333,46 +366,26 @@ __global__ void __launch_bounds__(kDetThreads, 3)
   const int kb = k0 + blockIdx.z * kDetKZ;
   const int ke = min(kb + kDetKZ, k1);
   const double thr = ph.shock_threshold;
-  // the input fields (N is not needed from Pst) and their layout: compact
-  // proper cells, or the ghost layout of U; offsets fit in 32 bits (every
-  // brick has fewer than 2^31 values)
-  const long long fs = PST ? b.nP : b.nV;
-  const double* F0 = PST ? Pst + 4 * fs : U;  // E, or D
-  const double* F1 = (PST ? Pst : U) + fs;
-  const double* F2 = F1 + fs;
-  const double* F3 = F2 + fs;
-  const double* F4 = F3 + fs;  // G (U only)
-  const int plane = PST ? b.n[0] * b.n[1] : b.m[0] * b.m[1];
   // the halo-tile cell of this thread
   const int rx = tid % RX, ry = tid / RX;
   const int gi = i0 - 1 + rx, gj = j0 - 1 + ry;
-  const bool ok = tid < NR && gi >= 0 && gj >= 0 && gi < b.n[0] && gj < b.n[1];
+  const bool ok = tid < NR && gi >= 0 && gj >= 0 && gi < n0 && gj < n1;
   const bool has_xm = rx >= 1 && gi >= 1, has_ym = ry >= 1 && gj >= 1;
-  const int gh = PST ? 0 : 2;
-  int off = (gi + gh) + (PST ? b.n[0] : b.m[0]) * (gj + gh) + plane * (kb - 1 + gh);
   double raw[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   auto fetch = [&](int kk) {
-    if (ok && kk >= 0 && kk < b.n[2]) {
-      raw[0] = F0[off];
-      raw[1] = F1[off];
-      raw[2] = F2[off];
-      raw[3] = F3[off];
-      if (!PST) raw[4] = F4[off];
-    }
+    if (ok && kk >= 0 && kk < n2) src.load(gi, gj, kk, raw);
   };
   fetch(kb - 1);
   double Pz = 0.0, Vz = 0.0;  // the plane below
   // the output cell of this thread (threads 0-255)
   const int ox = tid % kDetTX, oy = tid / kDetTX;
   const int i = i0 + ox, j = j0 + oy, ro = (ox + 1) + RX * (oy + 1);
-  const bool out_in = tid < kDetTX * kDetTY && i < b.n[0] && j < b.n[1];
-  const bool inner_xy = i >= 1 && j >= 1 && i <= b.n[0] - 2 && j <= b.n[1] - 2;
-  const int cplane = b.n[0] * b.n[1];
-  int dfo = i + b.n[0] * j + cplane * (kb - 2);  // df offset of (i, j, kk - 1)
+  const bool out_in = tid < kDetTX * kDetTY && i < n0 && j < n1;
+  const bool inner_xy = i >= 1 && j >= 1 && i <= n0 - 2 && j <= n1 - 2;
   // the ring slots of planes kk, kk - 1 and kk - 2
   uint8_t *s_new = sS[0], *s_cur = sS[2], *s_old = sS[1];
-  for (int kk = kb - 1; kk <= ke; ++kk, dfo += cplane) {
-    const bool live = ok && kk >= 0 && kk < b.n[2];
+  for (int kk = kb - 1; kk <= ke; ++kk) {
+    const bool live = ok && kk >= 0 && kk < n2;
     double P = 0.0, V1 = 0.0, V2 = 0.0, V3 = 0.0;
     if (live) {
       if (PST) {
@@ -390,7 +403,6 @@ __global__ void __launch_bounds__(kDetThreads, 3)
         V3 = w.V3;
       }
     }
-    off += plane;
     if (kk < ke) fetch(kk + 1);
     if (tid < NR) {
       sP[tid] = P;
@@ -413,7 +425,7 @@ __global__ void __launch_bounds__(kDetThreads, 3)
     const int k = kk - 1;
     if (k >= kb && out_in) {
       uint8_t bits = 0;
-      if (inner_xy && k >= 1 && k <= b.n[2] - 2) {
+      if (inner_xy && k >= 1 && k <= n2 - 2) {
         const uint8_t* m = s_old;  // plane k - 1
         const uint8_t* c = s_cur;
         const uint8_t* p = s_new;
@@ -426,13 +438,24 @@ __global__ void __launch_bounds__(kDetThreads, 3)
         if (((s0 | sxp | sym | sxp_ym) & 1) || ((s0 | szp | sym | szp_ym) & 4)) bits |= 2;
         if (((s0 | sxp | szm | sxp_zm) & 1) || ((s0 | syp | szm | syp_zm) & 2)) bits |= 4;
       }
-      df[dfo] = bits;
+      *src.flags(i, j, k) = bits;
     }
     uint8_t* t = s_old;
     s_old = s_cur;
     s_cur = s_new;
     s_new = t;
   }
+}
+
+// The features of one brick (detect_tile over its planes [k0, k1)), from the
+// conserved state U or (PST) from the compact primitives Pst (N, V1, V2, V3, E).
+template <bool PST>
+__global__ void __launch_bounds__(kDetThreads, 3)
+    detect_features_kernel(Box b, Phys ph, const double* __restrict__ U,
+                           const double* __restrict__ Pst, uint8_t* __restrict__ df, int k0,
+                           int k1) {
+  const DetectBrick<PST> src(b, U, Pst, df);
+  detect_tile<PST>(src, ph, b.n[0], b.n[1], b.n[2], k0, k1);
 }
 
 __global__ void batch_detect_shock_kernel(const BatchBrick* __restrict__ bb, int n,

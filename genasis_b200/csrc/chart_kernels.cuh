@@ -25,7 +25,6 @@ struct ChartBrick {
   const double* prim;   // initial primitives, ghost layout (chart_from_primitive)
   double* Pst;          // the kept primitives of the proper cells, compact
   const double* wn;     // primitives the last stage 2 stored, compact
-  uint8_t* sb;          // shock bits, compact
   uint8_t* df;          // DIFFUSIVE_FLUX_I bits, compact
   long long v_off;      // prefix sum of nV over the bricks
   long long c_off;      // prefix sum of nP
@@ -152,96 +151,63 @@ __device__ __forceinline__ void chart_p_v(const ChartBrick& B, const Phys& ph, c
   v[2] = w.V3;
 }
 
-// DetectShocks_CSL_Kernel (FluidFeatures_P__Kernel.f90:12-186) on the proper
-// cells of every brick: bit e of sb = shock along e between the cell and the
-// one below it, across a face inside the chart into the neighbouring brick
-// (the reference's ghost layer holds that cell); 0 on the chart's own
-// boundary, as on a single brick (no cell that keeps flags reads it).
+// The state of a chart of equal bricks (nbx x nby x nbz of bn0 x bn1 x bn2
+// cells, brick b = ix + nbx (iy + nby iz)) as the feature detection reads
+// it, by the chart's global proper coordinates: the primitives the last
+// stage 2 stored (PST), or the conserved state; and the bricks' flags.
 template <bool PST>
-__global__ void chart_detect_shock_kernel(const ChartBrick* __restrict__ cb, int n,
-                                          long long total, Phys ph, const int* skip) {
-  if (skip && *skip) return;
-  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
-       x += (long long)gridDim.x * blockDim.x) {
-    const int b = chart_find(cb, n, x, true);
-    const ChartBrick& B = cb[b];
-    const long long c = x - B.c_off;
-    int t[3];
-    decode3(c, B.box.n[0], B.box.n[1], t[0], t[1], t[2]);
-    double P0, v0[3];
-    chart_p_v<PST>(B, ph, t, P0, v0);
-    uint8_t bits = 0;
-#pragma unroll
-    for (int e = 0; e < 3; ++e) {
-      int q[3] = {t[0], t[1], t[2]};
-      q[e] -= 1;
-      if (q[e] < 0 && B.box.bc[e][0] != BC_NEIGHBOR) continue;
-      double P1, v1[3];
-      if (q[e] >= 0) {
-        chart_p_v<PST>(B, ph, q, P1, v1);
-      } else {
-        const ChartBrick& S = cb[chart_owner(cb, b, q)];
-        chart_p_v<PST>(S, ph, q, P1, v1);
-      }
-      if (shock_between(P0, P1, v0[e] - v1[e], ph.shock_threshold)) bits |= (uint8_t)(1u << e);
-    }
-    B.sb[c] = bits;
+struct DetectChart {
+  const ChartBrick* cb;
+  int nbx, nby, bn0, bn1, bn2;
+  __device__ __forceinline__ const ChartBrick& brick(int i, int j, int k, int& li, int& lj,
+                                                     int& lk) const {
+    const int bx = i / bn0, by = j / bn1, bz = k / bn2;
+    li = i - bx * bn0;
+    lj = j - by * bn1;
+    lk = k - bz * bn2;
+    return cb[bx + nbx * (by + nby * bz)];
   }
-}
+  __device__ __forceinline__ void load(int i, int j, int k, double* raw) const {
+    int li, lj, lk;
+    const ChartBrick& B = brick(i, j, k, li, lj, lk);
+    if (PST) {
+      const long long nP = B.box.nP, o = li + (long long)bn0 * (lj + (long long)bn1 * lk);
+      raw[0] = B.wn[4 * nP + o];
+      raw[1] = B.wn[nP + o];
+      raw[2] = B.wn[2 * nP + o];
+      raw[3] = B.wn[3 * nP + o];
+    } else {
+      const int c[3] = {li, lj, lk};
+      const long long nV = B.box.nV, o = ghost_index(B.box, c);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) raw[q] = B.U[q * nV + o];
+    }
+  }
+  __device__ __forceinline__ uint8_t* flags(int i, int j, int k) const {
+    int li, lj, lk;
+    const ChartBrick& B = brick(i, j, k, li, lj, lk);
+    return B.df + (li + (long long)bn0 * (lj + (long long)bn1 * lk));
+  }
+};
 
-// DIFFUSIVE_FLUX_I flags after ClearBoundary_CSL_Kernel (FluidFeatures_P__
-// Kernel.f90:189-313), which the reference applies on the faces of the
-// chart's boundary only (FluidFeatures_P__Form.f90:313-336: InnerBoundary =
-// iaBrick == 1, OuterBoundary = iaBrick == nBricks): a cell keeps flags
-// unless it is within one cell of a chart face, and flag d is set by a shock
-// along e != d at x, x + e_e, x - e_d or x + e_e - e_d, which may lie in the
-// neighbouring or the diagonal brick.
-__global__ void chart_detect_flags_kernel(const ChartBrick* __restrict__ cb, int n,
-                                          long long total, const int* skip) {
+// DetectShocks_CSL_Kernel and the DIFFUSIVE_FLUX_I flags after
+// ClearBoundary_CSL_Kernel (FluidFeatures_P__Kernel.f90:12-313) on a chart of
+// equal bricks: the single brick's tiled pass (detect_tile) over the chart's
+// global cells, each value read from the brick that holds it.  The reference
+// applies ClearBoundary on the faces of the chart's boundary only
+// (FluidFeatures_P__Form.f90:313-336: InnerBoundary = iaBrick == 1,
+// OuterBoundary = iaBrick == nBricks), which in the chart's global
+// coordinates is the single brick's rule: no flags within one cell of a chart
+// face (periodic ones included), and shock bits only between cells of the
+// chart, so that across a face inside the chart the bits and flags see the
+// neighbouring and the diagonal bricks.  Grid: tiles of the whole chart.
+template <bool PST>
+__global__ void __launch_bounds__(kDetThreads, 3)
+    chart_detect_features_kernel(const ChartBrick* __restrict__ cb, int nbx, int nby, int nbz,
+                                 Phys ph, const int* skip) {
   if (skip && *skip) return;
-  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
-       x += (long long)gridDim.x * blockDim.x) {
-    const int b = chart_find(cb, n, x, true);
-    const ChartBrick& B = cb[b];
-    const long long c = x - B.c_off;
-    int t[3];
-    decode3(c, B.box.n[0], B.box.n[1], t[0], t[1], t[2]);
-    bool keep = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-      if ((t[d] < 1 && B.box.bc[d][0] != BC_NEIGHBOR) ||
-          (t[d] > B.box.n[d] - 2 && B.box.bc[d][1] != BC_NEIGHBOR))
-        keep = false;
-    uint8_t bits = 0;
-    if (keep) {
-      // reads reach one cell either way: inside the brick (all but its outer
-      // layer) they index its own bits, else they cross into the neighbours
-      const bool inside = t[0] >= 1 && t[1] >= 1 && t[2] >= 1 && t[0] <= B.box.n[0] - 2 &&
-                          t[1] <= B.box.n[1] - 2 && t[2] <= B.box.n[2] - 2;
-      const long long sy = B.box.n[0], sz = (long long)B.box.n[0] * B.box.n[1];
-      auto bit = [&](int e, int dx, int dy, int dz) -> bool {
-        if (inside) return (B.sb[c + dx + dy * sy + dz * sz] >> e) & 1;
-        int q[3] = {t[0] + dx, t[1] + dy, t[2] + dz};
-        const ChartBrick& S = cb[chart_owner(cb, b, q)];
-        if (!chart_inside(S.box, q)) return false;
-        return (S.sb[q[0] + (long long)S.box.n[0] * (q[1] + (long long)S.box.n[1] * q[2])] >>
-                e) & 1;
-      };
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-          if (e == d) continue;
-          const int ex = e == 0, ey = e == 1, ez = e == 2;
-          const int dx = d == 0, dy = d == 1, dz = d == 2;
-          if (bit(e, 0, 0, 0) || bit(e, ex, ey, ez) || bit(e, -dx, -dy, -dz) ||
-              bit(e, ex - dx, ey - dy, ez - dz))
-            bits |= (uint8_t)(1u << d);
-        }
-      }
-    }
-    B.df[c] = bits;
-  }
+  const DetectChart<PST> src{cb, nbx, nby, cb[0].box.n[0], cb[0].box.n[1], cb[0].box.n[2]};
+  detect_tile<PST>(src, ph, nbx * src.bn0, nby * src.bn1, nbz * src.bn2, 0, nbz * src.bn2);
 }
 
 // Ghost values at the end of a step: an exchange-reachable ghost takes the

@@ -310,6 +310,14 @@ cudaError_t launch_stage_linear(int mode, bool in_prim, bool hllc, bool grav, in
 
 // The chart variants (16-row tiles): stage 1 from conserved values or kept
 // primitives, stage 2, with or without HLLC and gravity.
+// Tile rows of a chart's work items: the height each build's autotuned
+// single bricks choose (8-row tiles, two CTAs per SM, in the fast build)
+#if GFX_FAST_MATH
+constexpr int kChartTileY = 8;
+#else
+constexpr int kChartTileY = kTileY;
+#endif
+
 cudaError_t launch_stage_chart(int mode, bool in_prim, bool hllc, bool grav,
                                const BrickDesc* many, const WorkItem* items, int n_items,
                                int* counter, const Phys& ph, cudaStream_t s) {
@@ -317,9 +325,8 @@ cudaError_t launch_stage_chart(int mode, bool in_prim, bool hllc, bool grav,
   memset(&none, 0, sizeof(none));
 #define GFX_CSTAGE(M, IP, HC, GR)                                                          \
   if (mode == M && in_prim == IP && hllc == HC && grav == GR)                            \
-    return launch_stage_t<M, IP, HC, GR, 5, BAT_CHART, false, kTileY>(none, many, items,  \
-                                                                      n_items, counter,   \
-                                                                      ph, s);
+    return launch_stage_t<M, IP, HC, GR, 5, BAT_CHART, false, kChartTileY>(               \
+        none, many, items, n_items, counter, ph, s);
   GFX_CSTAGE(MODE_STAGE1, false, false, false)
   GFX_CSTAGE(MODE_STAGE1, false, true, false)
   GFX_CSTAGE(MODE_STAGE1, false, false, true)
@@ -2273,6 +2280,23 @@ int chart_initial_dt(gfx_fluid_chart* C, Clock* dc, int clip, cudaStream_t s) {
   return GFX_OK;
 }
 
+// The shock features of the whole chart in one tiled launch, from the
+// primitives the last stage 2 stored (from_wn) or from the conserved states.
+cudaError_t launch_chart_features(const gfx_fluid_chart* C, bool from_wn, const int* skip,
+                                  cudaStream_t s) {
+  const Box& b0 = C->h[0]->box;
+  Box chart = b0;
+  for (int a = 0; a < 3; ++a) chart.n[a] = b0.n[a] * C->nbk[a];
+  const dim3 grid = detect_grid(chart, 0, chart.n[2]);
+  if (from_wn)
+    chart_detect_features_kernel<true><<<grid, kDetThreads, 0, s>>>(C->cb, C->nbk[0], C->nbk[1],
+                                                                    C->nbk[2], C->ph, skip);
+  else
+    chart_detect_features_kernel<false><<<grid, kDetThreads, 0, s>>>(
+        C->cb, C->nbk[0], C->nbk[1], C->nbk[2], C->ph, skip);
+  return cudaGetLastError();
+}
+
 // The launches of one RK2 step of every brick (dt and the skip flag in the
 // chart's clock): features (across brick faces), stage 1, stage 2, ghosts.
 int enqueue_chart_step(gfx_fluid_chart* C, bool detect, bool from_wn, cudaStream_t s) {
@@ -2282,16 +2306,8 @@ int enqueue_chart_step(gfx_fluid_chart* C, bool detect, bool from_wn, cudaStream
   CUDA_TRY(cudaGetLastError());
   C->launches += 1;
   if (C->hllc && detect) {
-    if (from_wn)
-      chart_detect_shock_kernel<true><<<grid_for(C->total_c, blk), blk, 0, s>>>(
-          C->cb, C->n, C->total_c, C->ph, skip);
-    else
-      chart_detect_shock_kernel<false><<<grid_for(C->total_c, blk), blk, 0, s>>>(
-          C->cb, C->n, C->total_c, C->ph, skip);
-    chart_detect_flags_kernel<<<grid_for(C->total_c, blk), blk, 0, s>>>(C->cb, C->n,
-                                                                        C->total_c, skip);
-    CUDA_TRY(cudaGetLastError());
-    C->launches += 2;
+    CUDA_TRY(launch_chart_features(C, from_wn, skip, s));
+    C->launches += 1;
   }
   const bool in_prim = C->prims_pending || from_wn;
   const BrickDesc* d1 = C->prims_pending ? C->d1p : (from_wn ? C->d1w : C->d1);
@@ -2405,13 +2421,13 @@ int gfx_fluid_chart_create(const gfx_fluid_config* cfg, const int n_bricks[3],
     h->chart = C;
     C->h.push_back(h);
     if (b == 0) C->ph = h->ph;
-    // work items of 32 x 16 columns, z chunks of 32 planes, longest first
+    // work items of 32 x kChartTileY columns, z chunks of 32 planes, longest first
     const int len = std::min(nb[2], 32);
     for (int z = 0; z < nb[2]; z += len)
-      for (int y = 0; y < nb[1]; y += kTileY)
+      for (int y = 0; y < nb[1]; y += kChartTileY)
         for (int x = 0; x < nb[0]; x += TX) {
           items.push_back({b, x, y, z, std::min(nb[2], z + len)});
-          work.push_back((long long)std::min(TX, nb[0] - x) * std::min(kTileY, nb[1] - y) *
+          work.push_back((long long)std::min(TX, nb[0] - x) * std::min(kChartTileY, nb[1] - y) *
                          (std::min(nb[2], z + len) - z));
         }
   }
@@ -2514,7 +2530,6 @@ int gfx_fluid_chart_bind(gfx_fluid_chart* C, double* const* U) {
     c.U = U[b];
     c.Pst = h->Pst;
     c.wn = h->wn;
-    c.sb = h->sb;
     c.df = h->df;
     c.v_off = C->total_v;
     c.c_off = C->total_c;
@@ -2566,13 +2581,8 @@ int gfx_fluid_chart_set_conserved(gfx_fluid_chart* C, void* stream) {
   C->wn_valid = false;
   CUDA_TRY(cudaMemsetAsync(&C->clock[0].done, 0, sizeof(int), s));
   if (C->hllc) {
-    const int blk = 256;
-    chart_detect_shock_kernel<false><<<grid_for(C->total_c, blk), blk, 0, s>>>(
-        C->cb, C->n, C->total_c, C->ph, nullptr);
-    chart_detect_flags_kernel<<<grid_for(C->total_c, blk), blk, 0, s>>>(C->cb, C->n,
-                                                                        C->total_c, nullptr);
-    CUDA_TRY(cudaGetLastError());
-    C->launches += 2;
+    CUDA_TRY(launch_chart_features(C, false, nullptr, s));
+    C->launches += 1;
   }
   C->features = FEAT_VALID;
   return GFX_OK;

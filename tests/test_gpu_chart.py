@@ -10,7 +10,12 @@ The reference (Chart_SLD__Form.f90:131-1097) exchanges the ghost layers of
 faces and edges between bricks, clears the shock flags on the chart's
 boundary only (FluidFeatures_P__Form.f90:313-336) and records the boundary
 fluence on the chart's faces only (IncrementDivergence_FV__Form.f90:
-1002-1069): a decomposition must not change any result."""
+1002-1069): a decomposition must not change any result.
+
+The bit-level claims are the exact build's, so these tests pin it.  The fast
+build lets the compiler fuse multiply-adds, and a brick's kernels may fuse
+differently from the whole chart's; there the chart agrees with the single
+brick to the last bits (the last test)."""
 import numpy as np
 import pytest
 
@@ -57,9 +62,9 @@ IDS = [c[0] for c in CASES]
 
 
 def _pair(cfg, prim, n_bricks):
-    box = FluidBox(cfg)
+    box = FluidBox(cfg, variant="exact")
     box.compute_from_primitive(prim)
-    chart = FluidChart(cfg, n_bricks)
+    chart = FluidChart(cfg, n_bricks, variant="exact")
     chart.from_primitive(prim)
     return box, chart
 
@@ -178,7 +183,7 @@ def test_chart_matches_the_oracle_free_run():
     from oracle.oracle import Oracle
 
     name, cfg, prim, n_bricks = CASES[2]
-    chart = FluidChart(cfg, n_bricks)
+    chart = FluidChart(cfg, n_bricks, variant="exact")
     chart.from_primitive(prim)
     o = Oracle(cfg)
     o.set_primitive(prim)
@@ -210,4 +215,23 @@ def test_chart_rejects_uneven_bricks_and_single_brick_calls():
     chart.call("gfx_fluid_chart_brick", chart.h, 0, ctypes.byref(h), None)
     rc = lib.load().gfx_fluid_step(h, ctypes.c_void_p(chart.U[0].data_ptr()), 1e-3, None, None)
     assert rc == -1 and "chart" in lib.last_error()
+    chart.close()
+
+
+def test_chart_on_the_fast_build_stays_within_the_last_bits():
+    from tests.gpu_helpers import quantity_errors
+
+    name, cfg, prim, n_bricks = CASES[0]
+    box = FluidBox(cfg, variant="fast")
+    box.compute_from_primitive(prim)
+    chart = FluidChart(cfg, n_bricks, variant="fast")
+    chart.from_primitive(prim)
+    for i in range(5):
+        dt = box.compute_time_step(i)
+        assert chart.compute_time_step(i) == pytest.approx(dt, rel=1e-14), (name, i)
+        box.step(dt)
+        chart.step(dt)
+        q = quantity_errors(chart.gather(), box.U.detach().cpu().numpy(), cfg.proper)
+        assert max(q) <= 1e-13, (name, i, q)
+    box.close()
     chart.close()
