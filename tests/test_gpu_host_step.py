@@ -15,7 +15,6 @@ import pytest
 
 from genasis_b200 import problems
 from genasis_b200.config import FluidConfig
-from genasis_b200 import lib
 from tests.gpu_helpers import quantity_errors, to_np
 
 pytestmark = pytest.mark.gpu
@@ -46,15 +45,16 @@ def _cases():
 CASES = _cases()
 
 
+@pytest.mark.parametrize("variant", ["exact", "fast"])
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("z_chunk", [4, 16, 0])
-def test_host_step_matches_the_device_step(name, z_chunk):
+def test_host_step_matches_the_device_step(name, z_chunk, variant):
     import torch
 
     from genasis_b200.fluid import FluidBox
 
     cfg, prim = CASES[name]
-    dev, hst = FluidBox(cfg), FluidBox(cfg)
+    dev, hst = FluidBox(cfg, variant=variant), FluidBox(cfg, variant=variant)
     for box in (dev, hst):
         box.set_tuning(z_chunk, 0)
         box.compute_from_primitive(prim)
@@ -66,7 +66,7 @@ def test_host_step_matches_the_device_step(name, z_chunk):
         dev.step(dt, fl_dev)
         hst.step_host(host, dt, fl_host)
         torch.cuda.synchronize()
-        if lib.default_variant() == "exact":
+        if variant == "exact":
             assert torch.equal(host, dev.U.cpu()), (name, z_chunk, i)
             assert np.array_equal(fl_host.numpy(), to_np(fl_dev)), (name, z_chunk, i)
         else:
