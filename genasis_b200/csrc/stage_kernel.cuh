@@ -315,18 +315,22 @@ __device__ __forceinline__ void finish_cell(const Phys& ph, double* dst, int str
 // of the linked brick's cell (chart bricks), else 0 (the ghost layer of a
 // chart boundary, which ClearBoundary clears).
 template <bool CH>
-__device__ __forceinline__ bool df_bit(const BrickDesc& B, int d, int gx, int gy, int gz) {
-  if (B.df == nullptr) return false;
+__device__ __forceinline__ unsigned df_byte(const BrickDesc& B, int gx, int gy, int gz) {
+  if (B.df == nullptr) return 0;
   if (gx < 0 || gy < 0 || gz < 0 || gx >= B.n[0] || gy >= B.n[1] || gz >= B.n[2]) {
-    if (!CH) return false;
+    if (!CH) return 0;
     int c[3] = {gx, gy, gz};
     const BrickDesc& S = cell_owner<true>(B, c);
     if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= S.n[0] || c[1] >= S.n[1] ||
         c[2] >= S.n[2])
-      return false;
-    return (S.df[c[0] + (long long)S.n[0] * (c[1] + (long long)S.n[1] * c[2])] >> d) & 1;
+      return 0;
+    return S.df[c[0] + (long long)S.n[0] * (c[1] + (long long)S.n[1] * c[2])];
   }
-  return (B.df[gx + (long long)B.n[0] * (gy + (long long)B.n[1] * gz)] >> d) & 1;
+  return B.df[gx + (long long)B.n[0] * (gy + (long long)B.n[1] * gz)];
+}
+template <bool CH>
+__device__ __forceinline__ bool df_bit(const BrickDesc& B, int d, int gx, int gy, int gz) {
+  return (df_byte<CH>(B, gx, gy, gz) >> d) & 1;
 }
 
 // Whether face `side` of axis a records the boundary fluence: every face of
@@ -487,15 +491,15 @@ __device__ __forceinline__ void z_slope(const AxisGeo& GZ, const Phys& ph, int p
 }
 
 // Flux through the z face between planes p-1 (values a, slopes sm_) and p
-// (values b, slopes sp) of the own column (gx, gy), with its boundary fluence.
+// (values b, slopes sp) of the own column (gx, gy), with its boundary fluence;
+// diff: the face's DIFFUSIVE_FLUX_I bit (z bit of cell p).
 template <bool HLLC, int NF, bool CH>
 __device__ __forceinline__ void z_face_lr(const BrickDesc& B, const Phys& ph, int p,
                                           const double* l, const double* r, int gx, int gy,
-                                          bool own, double dt, double* F) {
+                                          bool own, double dt, bool diff, double* F) {
   FaceState L, R;
   face_state<NF>(l[0], l[1], l[2], l[3], l[4], ph, L);
   face_state<NF>(r[0], r[1], r[2], r[3], r[4], ph, R);
-  const bool diff = HLLC && df_bit<CH>(B, 2, gx, gy, p);
   riemann_flux<2, HLLC, NF>(L, R, diff, F);
   if (own && (p == 0 || p == B.n[2]) && B.fluence &&
       (!CH || records_fluence(B, 2, p == 0 ? 0 : 1)))
@@ -507,12 +511,13 @@ template <bool HLLC, int NF, bool CH>
 __device__ __forceinline__ void z_face(const BrickDesc& B, const Phys& ph, int p,
                                        const double* a, int sa, const double* sm_, int ssm,
                                        const double* b, int sb, const double* sp, int ssp,
-                                       int gx, int gy, bool own, double dt, double* F) {
+                                       int gx, int gy, bool own, double dt, bool diff,
+                                       double* F) {
   const AxisGeo& GZ = B.geo[2];
   double l[5], r[5];
   face_prims(a, sm_, sa, b, sp, sb, ssm, ssp, __ldg(GZ.WR + p + 1), __ldg(GZ.WL + p + 2), l,
              r);
-  z_face_lr<HLLC, NF, CH>(B, ph, p, l, r, gx, gy, own, dt, F);
+  z_face_lr<HLLC, NF, CH>(B, ph, p, l, r, gx, gy, own, dt, diff, F);
 }
 
 // PARABOLIC: inner and outer face values of the 5 primitives of the own
@@ -559,11 +564,12 @@ __device__ __noinline__ void stage_prologue(const BrickDesc& B, const Phys& ph, 
   else
     z_slope(B.geo[2], ph, z0, cslot(z0 - 1), NT, cslot(z0), NT, fc, FS, s_0);
   double F[NF];
+  const bool diff = HLLC && df_bit<CH>(B, 2, gx, gy, z0);
   if (PARAB)
-    z_face_lr<HLLC, NF, CH>(B, ph, z0, s_m, vI0, gx, gy, own, dt, F);
+    z_face_lr<HLLC, NF, CH>(B, ph, z0, s_m, vI0, gx, gy, own, dt, diff, F);
   else
     z_face<HLLC, NF, CH>(B, ph, z0, cslot(z0 - 1), NT, s_m, 1, cslot(z0), NT, s_0, 1, gx, gy, own,
-                     dt, F);
+                         dt, diff, F);
 #pragma unroll
   for (int q = 0; q < 5; ++q) zss[q * NT + tid] = s_0[q];
 #pragma unroll
@@ -605,6 +611,11 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
   constexpr bool HS = SL::HS;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
+  // HLLC: the DIFFUSIVE_FLUX_I bytes of the cells (x0 .. x0 + TX, y0 .. y0 + TY)
+  // of plane k, the cells after every x and y face of the tile
+  constexpr int NDF = (TX + 1) * (TYt + 1);
+  static_assert(NDF <= 2 * NT, "two flag bytes per thread at most");
+  __shared__ uint8_t s_df[HLLC ? NDF : 1];
   __shared__ BrickDesc s_desc;
   constexpr int LX = TX + 4, LY = TY + 4;
 
@@ -734,6 +745,15 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         for (int q = 0; q < 5; ++q) full[q * FS + c_off] = src[q * NT];
       }
       copy_cell_async<IN_PRIM, CH>(B, cslot(k + 2), NT, gx, gy, k + 2);
+      // the flag bytes of plane k for the x / y faces and of plane k+1 for the
+      // own column's z face: loaded now, used after the slope phase
+      unsigned dfa = 0, dfb = 0, dfz = 0;
+      if (HLLC) {
+        dfa = df_byte<CH>(B, x0 + tid % (TX + 1), y0 + tid / (TX + 1), k);
+        if (tid + NT < NDF)
+          dfb = df_byte<CH>(B, x0 + (tid + NT) % (TX + 1), y0 + (tid + NT) / (TX + 1), k);
+        dfz = df_byte<CH>(B, gx, gy, k + 1);
+      }
       if (tid < NH) {
         if (hx >= -FR && hx < TX + FR && hy >= -FR && hy < TY + FR) {  // in the ring
           const int o = (hy + FR) * FW + (hx + FR);
@@ -765,6 +785,10 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       finish_cell<IN_PRIM>(ph, cslot(k + 2), NT, cell_flips<CH>(B, gx, gy, k + 2));
       if (tid < NH && k + 1 < z1)
         finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips<CH>(B, x0 + hx, y0 + hy, k + 1));
+      if (HLLC) {
+        s_df[tid] = (uint8_t)dfa;
+        if (tid + NT < NDF) s_df[tid + NT] = (uint8_t)dfb;
+      }
       __syncthreads();
 
       // (3) faces: x [TY][TX+1], y [TY+1][TX] of plane k, one code path for
@@ -827,7 +851,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             to_normal_frame_y(L);
             to_normal_frame_y(R);
           }
-          const bool diff = HLLC && df_bit<CH>(B, isx ? 0 : 1, cx, cy, k);
+          const bool diff = HLLC && ((s_df[ly * (TX + 1) + lx] >> (isx ? 0 : 1)) & 1);
           double F[NF];
           riemann_flux<0, HLLC, NF>(L, R, diff, F);
           if (!isx) {
@@ -868,11 +892,12 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         z_parabolic(B, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zI, zsn);
 #pragma unroll
         for (int q = 0; q < 5; ++q) zl[q] = zss[q * NT + tid];
-        z_face_lr<HLLC, NF, CH>(B, ph, k + 1, zl, zI, gx, gy, own, dt, zfn);
+        z_face_lr<HLLC, NF, CH>(B, ph, k + 1, zl, zI, gx, gy, own, dt, HLLC && ((dfz >> 2) & 1),
+                                zfn);
       } else {
         z_slope(GZ, ph, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
         z_face<HLLC, NF, CH>(B, ph, k + 1, full + c_off, FS, zss + tid, NT, cslot(k + 1), NT, zsn,
-                         1, gx, gy, own, dt, zfn);
+                             1, gx, gy, own, dt, HLLC && ((dfz >> 2) & 1), zfn);
       }
       __syncthreads();
 
