@@ -611,11 +611,16 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
   constexpr bool HS = SL::HS;
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
-  // HLLC: the DIFFUSIVE_FLUX_I bytes of the cells (x0 .. x0 + TX, y0 .. y0 + TY)
-  // of plane k, the cells after every x and y face of the tile
+  // HLLC on 8-row tiles (DFS): the DIFFUSIVE_FLUX_I bytes of the cells
+  // (x0 .. x0 + TX, y0 .. y0 + TY) of plane k, the cells after every x and y
+  // face of the tile, loaded at the start of the plane and kept here, so that
+  // no face waits on a global load.  The three registers that carry them
+  // across the slope phase would spill on 16-row tiles (512 threads at the
+  // 128-register cap), which keep one load per face.
+  constexpr bool DFS = HLLC && TYt == 8;
   constexpr int NDF = (TX + 1) * (TYt + 1);
   static_assert(NDF <= 2 * NT, "two flag bytes per thread at most");
-  __shared__ uint8_t s_df[HLLC ? NDF : 1];
+  __shared__ uint8_t s_df[DFS ? NDF : 1];
   __shared__ BrickDesc s_desc;
   constexpr int LX = TX + 4, LY = TY + 4;
 
@@ -748,7 +753,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       // the flag bytes of plane k for the x / y faces and of plane k+1 for the
       // own column's z face: loaded now, used after the slope phase
       unsigned dfa = 0, dfb = 0, dfz = 0;
-      if (HLLC) {
+      if (DFS) {
         dfa = df_byte<CH>(B, x0 + tid % (TX + 1), y0 + tid / (TX + 1), k);
         if (tid + NT < NDF)
           dfb = df_byte<CH>(B, x0 + (tid + NT) % (TX + 1), y0 + (tid + NT) / (TX + 1), k);
@@ -785,7 +790,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
       finish_cell<IN_PRIM>(ph, cslot(k + 2), NT, cell_flips<CH>(B, gx, gy, k + 2));
       if (tid < NH && k + 1 < z1)
         finish_cell<IN_PRIM>(ph, hbuf + tid, NH, cell_flips<CH>(B, x0 + hx, y0 + hy, k + 1));
-      if (HLLC) {
+      if (DFS) {
         s_df[tid] = (uint8_t)dfa;
         if (tid + NT < NDF) s_df[tid + NT] = (uint8_t)dfb;
       }
@@ -851,7 +856,9 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             to_normal_frame_y(L);
             to_normal_frame_y(R);
           }
-          const bool diff = HLLC && ((s_df[ly * (TX + 1) + lx] >> (isx ? 0 : 1)) & 1);
+          const bool diff =
+              HLLC && (DFS ? ((s_df[ly * (TX + 1) + lx] >> (isx ? 0 : 1)) & 1)
+                           : df_bit<CH>(B, isx ? 0 : 1, cx, cy, k));
           double F[NF];
           riemann_flux<0, HLLC, NF>(L, R, diff, F);
           if (!isx) {
@@ -892,12 +899,15 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
         z_parabolic(B, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zI, zsn);
 #pragma unroll
         for (int q = 0; q < 5; ++q) zl[q] = zss[q * NT + tid];
-        z_face_lr<HLLC, NF, CH>(B, ph, k + 1, zl, zI, gx, gy, own, dt, HLLC && ((dfz >> 2) & 1),
+        z_face_lr<HLLC, NF, CH>(B, ph, k + 1, zl, zI, gx, gy, own, dt,
+                                HLLC && (DFS ? (dfz >> 2) & 1 : df_bit<CH>(B, 2, gx, gy, k + 1)),
                                 zfn);
       } else {
         z_slope(GZ, ph, k + 1, full + c_off, FS, cslot(k + 1), NT, cslot(k + 2), NT, zsn);
         z_face<HLLC, NF, CH>(B, ph, k + 1, full + c_off, FS, zss + tid, NT, cslot(k + 1), NT, zsn,
-                             1, gx, gy, own, dt, HLLC && ((dfz >> 2) & 1), zfn);
+                             1, gx, gy, own, dt,
+                             HLLC && (DFS ? (dfz >> 2) & 1 : df_bit<CH>(B, 2, gx, gy, k + 1)),
+                             zfn);
       }
       __syncthreads();
 
