@@ -909,6 +909,24 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
                              HLLC && (DFS ? (dfz >> 2) & 1 : df_bit<CH>(B, 2, gx, gy, k + 1)),
                              zfn);
       }
+      // 8-row tiles (EPI): the update's own inputs (U^n of the cell in
+      // stage 1, U^n + K1/2 in stage 2), loaded before the barrier so that
+      // their latency passes while the CTA synchronises; 16-row tiles, at the
+      // register cap, load them in the update
+      constexpr bool EPI = TYt == 8 && MODE != MODE_INCREMENT;
+      double ein[5];
+      if (EPI && own) {
+        if (MODE == MODE_STAGE1) {
+          const long long g =
+              (gx + 2) + (long long)B.m[0] * ((gy + 2) + (long long)B.m[1] * (k + 2));
+#pragma unroll
+          for (int q = 0; q < 5; ++q) ein[q] = __ldg(B.U_in + q * B.nV + g);
+        } else {
+          const long long c = gx + (long long)n0 * (gy + (long long)n1 * k);
+#pragma unroll
+          for (int q = 0; q < 5; ++q) ein[q] = __ldg(B.H + q * B.nP + c);
+        }
+      }
       __syncthreads();
 
       // (5) cell update and stage epilogue
@@ -970,13 +988,17 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
           if (MODE == MODE_STAGE1) {
             Cons u;
             {
-              const double* U = B.U_in;
               Cons raw;
-              raw.D = __ldg(U + gidx);
-              raw.S1 = __ldg(U + B.nV + gidx);
-              raw.S2 = __ldg(U + 2 * B.nV + gidx);
-              raw.S3 = __ldg(U + 3 * B.nV + gidx);
-              raw.G = __ldg(U + 4 * B.nV + gidx);
+              if (EPI) {
+                raw = Cons{ein[0], ein[1], ein[2], ein[3], ein[4]};
+              } else {
+                const double* U = B.U_in;
+                raw.D = __ldg(U + gidx);
+                raw.S1 = __ldg(U + B.nV + gidx);
+                raw.S2 = __ldg(U + 2 * B.nV + gidx);
+                raw.S3 = __ldg(U + 3 * B.nV + gidx);
+                raw.G = __ldg(U + 4 * B.nV + gidx);
+              }
               if (IN_PRIM) {
                 u = raw;
               } else {
@@ -1001,10 +1023,13 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             Y[3 * B.nP + cidx] = wy.V3;
             Y[4 * B.nP + cidx] = wy.E;
           } else {  // MODE_STAGE2: Solution + B2 K2, then ComputeFromConserved
-            const double* H = B.H;
-            Cons u{H[cidx] + 0.5 * Kc[0], H[B.nP + cidx] + 0.5 * Kc[1],
-                   H[2 * B.nP + cidx] + 0.5 * Kc[2], H[3 * B.nP + cidx] + 0.5 * Kc[3],
-                   H[4 * B.nP + cidx] + 0.5 * Kc[4]};
+            if (!EPI) {
+              const double* H = B.H;
+#pragma unroll
+              for (int q = 0; q < 5; ++q) ein[q] = H[q * B.nP + cidx];
+            }
+            Cons u{ein[0] + 0.5 * Kc[0], ein[1] + 0.5 * Kc[1], ein[2] + 0.5 * Kc[2],
+                   ein[3] + 0.5 * Kc[3], ein[4] + 0.5 * Kc[4]};
             Prim w;
             cons_to_prim(u, w, ph.nmin);
             double P, CS, SB;
