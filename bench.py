@@ -290,14 +290,16 @@ def pipe_use(kernel):
 def _timed_evolve(box, steps, warmup, local, world):
     """Warm-up cycles (they also capture the cycle graph), then `steps` cycles
     of gfx_fluid_evolve timed with CUDA events on the launching stream between
-    barriers, with the clocks sampled meanwhile."""
+    barriers, with the clocks sampled meanwhile.  The sampler starts before
+    the warm-up, so that the device is busy up to the timed region (no idle
+    gap for the clocks to drop in, and nvidia-smi's start-up stays outside)."""
     import torch
 
     stream = torch.cuda.current_stream()
-    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
-    torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
+    t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
+    torch.cuda.synchronize()
     launches0 = box.kernel_launches()
     barrier(world)
     torch.cuda.synchronize()
