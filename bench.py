@@ -860,10 +860,15 @@ def rt_result(steps=200, warmup=3, adjoint_steps=10, variant="exact"):
     dt = box.compute_time_step(cyc2)
     roof = stage_roofline(box, cells, dt, 5)
     def adjoint_cost(bx, U0, dts):
-        # an untimed forward first: its checkpoints take their memory from the
-        # allocator once, so that the timed forward measures the steps
+        # an untimed forward and adjoint first: the checkpoints, the adjoint's
+        # workspace (20 values per cell, allocated by the handle's first
+        # adjoint step) and the adjoint arrays take their memory once, so that
+        # the timed run measures the steps
         final, cps = run_forward(bx, U0, dts, True)
-        del final, cps
+        lam = torch.zeros_like(final)
+        lam[0] = 2.0 * final[0] * dv
+        grad = run_adjoint(bx, cps, dts, lam, True)
+        del final, cps, lam, grad
         torch.cuda.synchronize()
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         e[0].record()
