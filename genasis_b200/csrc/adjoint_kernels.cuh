@@ -230,8 +230,10 @@ __global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
 // slope c, slope c + 1.
 constexpr int kAdjXFaces = 29;
 
+// Four CTAs of 128 threads per SM on both builds: a lane holds one cell, not
+// the sweep's stencil window, and fits 128 registers without spills.
 template <bool HLLC>
-__global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, 4)
     adj_face_x_kernel(const __grid_constant__ AdjDesc A, const __grid_constant__ Phys ph) {
   constexpr unsigned FULL = 0xffffffffu;
   const int n0 = A.n[0], n1 = A.n[1], n2 = A.n[2];
