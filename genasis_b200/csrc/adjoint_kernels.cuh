@@ -47,32 +47,36 @@ __device__ __forceinline__ void adj_load(const AdjDesc& A, int D, long long base
 }
 
 __device__ __forceinline__ void adj_flush(const AdjDesc& A, int D, long long base, long long sD,
-                                          int c, const double* a) {
+                                          int c, const double* a, int stride = 1) {
   bool neg;
   const int s = bc_map(c, A.n[D], A.bc[D][0], A.bc[D][1], neg);
   double* p = A.lamW + base + s * sD;
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
-    const double v = (neg && q == 1 + D) ? -a[q] : a[q];
+    const double v = (neg && q == 1 + D) ? -a[q * stride] : a[q * stride];
     if (v != 0.0) atomicAdd(p + q * A.nP, v);
   }
 }
 
-// CTAs of 128 threads per SM that the reverse sweep's registers must allow:
-// 3 (168 registers) in the exact build; 4 (128 registers, more spills but 16
-// warps per SM) in the fast build, measured 3 % faster there at 128^3
+// CTAs of 128 threads per SM that the y / z sweep's registers must allow,
+// its accumulators living in shared memory (25.6 KB a CTA): 4 in the exact
+// build (128 registers, 48 B of spills), 5 in the fast build (96 registers);
+// measured at 128^3 against 3 and 4 (y / z launches 235 -> 222 us exact,
+// 195 -> 189 us fast)
 #ifndef GFX_ADJ_MIN_BLOCKS
 #if GFX_FAST_MATH
-#define GFX_ADJ_MIN_BLOCKS 4
+#define GFX_ADJ_MIN_BLOCKS 5
 #else
-#define GFX_ADJ_MIN_BLOCKS 3
+#define GFX_ADJ_MIN_BLOCKS 4
 #endif
 #endif
 
+constexpr int kAdjThreads = 128;  // threads of an L^T block
+
 template <int D, bool HLLC>
-__global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
-    adj_face_kernel(const __grid_constant__ AdjDesc A,
-                                                       const __grid_constant__ Phys ph) {
+__global__ void __launch_bounds__(kAdjThreads, GFX_ADJ_MIN_BLOCKS)
+    adj_face_kernel(const __grid_constant__ AdjDesc A, const __grid_constant__ Phys ph) {
+  __shared__ double s_adj[25 * kAdjThreads];
   constexpr int T1 = (D == 0) ? 1 : 0;
   constexpr int T2 = (D == 2) ? 1 : 2;
   const int nD = A.n[D], n1 = A.n[T1], n2 = A.n[T2];
@@ -116,6 +120,7 @@ __global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
       }
     };
     // adjoint of the slopes of cell c into its stencil cells c - 1, c, c + 1
+    // (the accumulators' columns, stride kAdjThreads)
     auto slope_back = [&](int branches, int c, const double* ls, double* am, double* a0,
                           double* ap) {
       const int tt = c + 2;
@@ -126,9 +131,10 @@ __global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
       for (int q = 0; q < 5; ++q) {
         double gl, gr;
         slope_coeffs((branches >> (2 * q)) & 3, sql, sqr, rdxl, rdxr, rcden, ph.theta, gl, gr);
-        am[q] -= gl * ls[q];
-        a0[q] += (gl - gr) * ls[q];
-        ap[q] += gr * ls[q];
+        const double l = ls[q * kAdjThreads];
+        am[q * kAdjThreads] -= gl * l;
+        a0[q * kAdjThreads] += (gl - gr) * l;
+        ap[q * kAdjThreads] += gr * l;
       }
     };
     auto load_lamk = [&](int c, double* out) {
@@ -143,22 +149,34 @@ __global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
       }
     };
 
+    // in registers: the stencil window and the slopes; in shared memory, one
+    // column per thread ([element][thread]): the adjoint accumulators of the
+    // cells i - 2, i - 1, i (a ring of three slots, slot (c + 3) % 3 for cell
+    // c), the slope adjoint of cell i - 1 and lamK of cell i - 1, so that
+    // little stays live across the flux adjoint
+    double* my = s_adj + threadIdx.x;
+    auto acc = [&](int c) { return my + ((c + 3) % 3) * 5 * kAdjThreads; };
+    double* LS = my + 15 * kAdjThreads;
+    double* LK = my + 20 * kAdjThreads;
     double wm2[5], wm1[5], w0[5], wp1[5];
     double sm1[5], s0v[5];
-    double am2[5], am1[5], a0[5];
-    double lsm1[5], lkm1[5], lk0[5];
     int bm1, b0;  // limiter branches of slope(i - 1), slope(i)
     adj_load(A, D, base, sD, s0 - 2, wm2);
     adj_load(A, D, base, sD, s0 - 1, wm1);
     adj_load(A, D, base, sD, s0, w0);
     slope(wm2, wm1, w0, s0 - 1, sm1, bm1);
-    load_lamk(s0 - 1, lkm1);
+    {
+      double lk[5];
+      load_lamk(s0 - 1, lk);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) LK[q * kAdjThreads] = lk[q];
+    }
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      am2[q] = 0.0;
-      am1[q] = 0.0;
-      a0[q] = 0.0;
-      lsm1[q] = 0.0;
+      acc(s0 - 2)[q * kAdjThreads] = 0.0;
+      acc(s0 - 1)[q * kAdjThreads] = 0.0;
+      acc(s0)[q * kAdjThreads] = 0.0;
+      LS[q * kAdjThreads] = 0.0;
     }
     for (int i = s0; i < s1; ++i) {
       adj_load(A, D, base, sD, i + 1, wp1);
@@ -170,48 +188,51 @@ __global__ void __launch_bounds__(128, GFX_ADJ_MIN_BLOCKS)
         l[q] = wm1[q] + wr * sm1[q];
         r[q] = w0[q] - wl * s0v[q];
       }
-      load_lamk(i, lk0);
       // face i is the inner face of cell i and the outer face of cell i - 1
       double lF[5], ll[5], lr[5];
+      {
+        double lk0[5];
+        load_lamk(i, lk0);
 #pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        lF[q] = lk0[q] - lkm1[q];
-        ll[q] = 0.0;
-        lr[q] = 0.0;
+        for (int q = 0; q < 5; ++q) {
+          lF[q] = lk0[q] - LK[q * kAdjThreads];
+          LK[q * kAdjThreads] = lk0[q];
+          ll[q] = 0.0;
+          lr[q] = 0.0;
+        }
       }
       bool diff = false;
       if (HLLC && A.df != nullptr && i < nD) diff = (A.df[base + i * sD] >> D) & 1;
       flux_adjoint<D, HLLC>(l, r, diff, lF, ph, ll, lr);
+      double* am2 = acc(i - 2);
+      double* am1 = acc(i - 1);
+      double* a0 = acc(i);
       double ls0[5];
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        am1[q] += ll[q];
-        lsm1[q] += wr * ll[q];
-        a0[q] += lr[q];
+        am1[q * kAdjThreads] += ll[q];
+        LS[q * kAdjThreads] += wr * ll[q];
+        a0[q * kAdjThreads] += lr[q];
         ls0[q] = -wl * lr[q];
       }
       // slope(i - 1) has all of this segment's contributions
-      slope_back(bm1, i - 1, lsm1, am2, am1, a0);
-      adj_flush(A, D, base, sD, i - 2, am2);
+      slope_back(bm1, i - 1, LS, am2, am1, a0);
+      adj_flush(A, D, base, sD, i - 2, am2, kAdjThreads);
       bm1 = b0;
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        wm2[q] = wm1[q];
+        am2[q * kAdjThreads] = 0.0;  // the slot of cell i + 1
+        LS[q * kAdjThreads] = ls0[q];
         wm1[q] = w0[q];
         w0[q] = wp1[q];
         sm1[q] = s0v[q];
-        lsm1[q] = ls0[q];
-        am2[q] = am1[q];
-        am1[q] = a0[q];
-        a0[q] = 0.0;
-        lkm1[q] = lk0[q];
       }
     }
     // the last slope of the segment: cells s1 - 2, s1 - 1, s1
-    slope_back(bm1, s1 - 1, lsm1, am2, am1, a0);
-    adj_flush(A, D, base, sD, s1 - 2, am2);
-    adj_flush(A, D, base, sD, s1 - 1, am1);
-    adj_flush(A, D, base, sD, s1, a0);
+    slope_back(bm1, s1 - 1, LS, acc(s1 - 2), acc(s1 - 1), acc(s1));
+    adj_flush(A, D, base, sD, s1 - 2, acc(s1 - 2), kAdjThreads);
+    adj_flush(A, D, base, sD, s1 - 1, acc(s1 - 1), kAdjThreads);
+    adj_flush(A, D, base, sD, s1, acc(s1), kAdjThreads);
   }
 }
 

@@ -2085,15 +2085,16 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
     h->launches += 1;
     feat = df;
   }
-  // forward recomputation from the checkpoint: W0, stage 1 (W1 into Yp) and,
-  // without U^n+1 from the caller, stage 2
-  adj_prims_kernel<<<grid_for(b.nP, blk), blk, 0, s>>>(b, h->ph, U_n, W0);
+  // forward recomputation from the checkpoint: stage 1 (which also stores the
+  // primitives W0 of U^n it recovers, and W1 into Yp) and, without U^n+1
+  // from the caller, stage 2
   set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
   reset_bits_kernel<<<1, 32, 0, s>>>(h->tsi_bits, 1, h->counters, 4);
   CUDA_TRY(cudaGetLastError());
-  h->launches += 3;
+  h->launches += 2;
   BrickDesc d1 = make_desc(h, U_n, nullptr, nullptr, nullptr, feat, nullptr, h->dt_slot, 0.5,
                            nullptr);
+  d1.wn = W0;
   CUDA_TRY(launch_stage(MODE_STAGE1, false, hllc, grav, d1, nullptr, h->items, h->n_items,
                         h->counters, h->ph, s));
   h->launches += 1;

@@ -87,8 +87,8 @@ struct BrickDesc {
   double weight;         // Runge-Kutta weight of the stage (fluence)
   unsigned long long* tsi_bits;  // max inverse CFL time, ordered bits
   const int* skip;       // device flag: nonzero = do nothing (finished evolve)
-  double* wn;            // stage 2: primitives N, V1, V2, V3, E of the new state, compact
-                         // (or null)
+  double* wn;            // compact primitives N, V1, V2, V3, E (or null): stage 2, of
+                         // the new state; stage 1, of its input
   int tile_y;            // host side: tile rows of the work list (0 = kTileY)
   // chart bricks: the brick across each face ([axis][inner, outer]) as an
   // index into `links`, the descriptors of this stage for every brick of the
@@ -986,6 +986,13 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             Kc[4] = Kc[4] - N * (V1 * 0.0 + V2 * 0.0 + V3 * a) * dt;
           }
           if (MODE == MODE_STAGE1) {
+            if (B.wn) {
+              B.wn[cidx] = N;
+              B.wn[B.nP + cidx] = V1;
+              B.wn[2 * B.nP + cidx] = V2;
+              B.wn[3 * B.nP + cidx] = V3;
+              B.wn[4 * B.nP + cidx] = E;
+            }
             Cons u;
             {
               Cons raw;
