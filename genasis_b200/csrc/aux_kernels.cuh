@@ -152,33 +152,44 @@ __global__ void ghost_refresh_kernel(Box b, Phys ph, double* __restrict__ U) {
     ghost_refresh_value(b, ph, U, v);
 }
 
-// The same, visiting only the ghost shell: the two z ghost planes at each
-// end, then the y ghost rows and the x ghost columns of the proper planes.
-__global__ void ghost_refresh_shell_kernel(Box b, Phys ph, double* __restrict__ U) {
+// The ghost-layout coordinates of the u-th value (u < nV - nP) of the ghost
+// shell: the two z ghost planes at each end, then the y ghost rows and the x
+// ghost columns of the proper planes.
+__device__ __forceinline__ void shell_cell(const Box& b, long long u, long long& i, long long& j,
+                                           long long& k) {
   const long long m0 = b.m[0], m1 = b.m[1], m2 = b.m[2];
   const long long n1 = b.n[1], n2 = b.n[2];
-  const long long gz = 4 * m0 * m1, gy = 4 * m0 * n2, gx = 4 * n1 * n2;
-  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < gz + gy + gx;
-       u += (long long)gridDim.x * blockDim.x) {
-    long long i, j, k;
-    if (u < gz) {  // planes k = 0, 1, m2 - 2, m2 - 1
-      const long long s = u / (m0 * m1), r = u - s * m0 * m1;
-      k = (s < 2) ? s : m2 - 4 + s;
-      j = r / m0;
-      i = r - j * m0;
-    } else if (u < gz + gy) {  // rows j = 0, 1, m1 - 2, m1 - 1 of planes 2 .. m2 - 3
-      const long long w = u - gz, s = w / (m0 * n2), r = w - s * m0 * n2;
-      j = (s < 2) ? s : m1 - 4 + s;
-      k = 2 + r / m0;
-      i = r - (k - 2) * m0;
-    } else {  // columns i = 0, 1, m0 - 2, m0 - 1 of rows 2 .. m1 - 3
-      const long long w = u - gz - gy, s = w / (n1 * n2), r = w - s * n1 * n2;
-      i = (s < 2) ? s : m0 - 4 + s;
-      k = 2 + r / n1;
-      j = 2 + (r - (k - 2) * n1);
-    }
-    ghost_refresh_value(b, ph, U, i + m0 * (j + m1 * k));
+  const long long gz = 4 * m0 * m1, gy = 4 * m0 * n2;
+  if (u < gz) {  // planes k = 0, 1, m2 - 2, m2 - 1
+    const long long s = u / (m0 * m1), r = u - s * m0 * m1;
+    k = (s < 2) ? s : m2 - 4 + s;
+    j = r / m0;
+    i = r - j * m0;
+  } else if (u < gz + gy) {  // rows j = 0, 1, m1 - 2, m1 - 1 of planes 2 .. m2 - 3
+    const long long w = u - gz, s = w / (m0 * n2), r = w - s * m0 * n2;
+    j = (s < 2) ? s : m1 - 4 + s;
+    k = 2 + r / m0;
+    i = r - (k - 2) * m0;
+  } else {  // columns i = 0, 1, m0 - 2, m0 - 1 of rows 2 .. m1 - 3
+    const long long w = u - gz - gy, s = w / (n1 * n2), r = w - s * n1 * n2;
+    i = (s < 2) ? s : m0 - 4 + s;
+    k = 2 + r / n1;
+    j = 2 + (r - (k - 2) * n1);
   }
+}
+
+// Its ghost-layout index.
+__device__ __forceinline__ long long shell_value(const Box& b, long long u) {
+  long long i, j, k;
+  shell_cell(b, u, i, j, k);
+  return i + (long long)b.m[0] * (j + (long long)b.m[1] * k);
+}
+
+// The same, visiting only the ghost shell.
+__global__ void ghost_refresh_shell_kernel(Box b, Phys ph, double* __restrict__ U) {
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < b.nV - b.nP;
+       u += (long long)gridDim.x * blockDim.x)
+    ghost_refresh_value(b, ph, U, shell_value(b, u));
 }
 
 // The same over the values [v0, v1) only (whole planes of a z slab).
@@ -212,13 +223,21 @@ __device__ __forceinline__ int find_brick(const BatchBrick* bb, int n, long long
   return lo;
 }
 
+// The ghost shells of every brick of a batch, one thread per shell value
+// (the shells are laid end to end: brick b's starts at v_off - c_off).
 __global__ void batch_ghost_refresh_kernel(const BatchBrick* __restrict__ bb, int n,
                                            long long total, Phys ph) {
   for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
        x += (long long)gridDim.x * blockDim.x) {
-    const int b = find_brick(bb, n, x, false);
-    if (bb[b].skip && *bb[b].skip) continue;
-    ghost_refresh_value(bb[b].box, ph, bb[b].U, x - bb[b].v_off);
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (bb[mid].v_off - bb[mid].c_off <= x) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchBrick& B = bb[lo];
+    if (B.skip && *B.skip) continue;
+    ghost_refresh_value(B.box, ph, B.U, shell_value(B.box, x - (B.v_off - B.c_off)));
   }
 }
 

@@ -215,9 +215,8 @@ __global__ void __launch_bounds__(kDetThreads, 3)
 // exchanged increments keep it equal to that cell); every other ghost keeps
 // its conserved values through the floors of ComputeFromConserved.
 // The ghost values of every brick, one thread per value of the bricks' ghost
-// shells (s_off: prefix sums of nV - nP over the bricks; the shell of a brick
-// is its two z ghost planes at each end, the y ghost rows and the x ghost
-// columns of its proper planes).
+// shells (laid end to end: brick b's starts at v_off - c_off; shell_cell
+// orders a shell).
 __device__ __forceinline__ int chart_find_shell(const ChartBrick* cb, int n, long long x) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
@@ -236,27 +235,9 @@ __global__ void chart_ghost_refresh_kernel(const ChartBrick* __restrict__ cb, in
     const int b = chart_find_shell(cb, n, x);
     const ChartBrick& B = cb[b];
     const long long u = x - (B.v_off - B.c_off), nV = B.box.nV;
-    const long long m0 = B.box.m[0], m1 = B.box.m[1], m2 = B.box.m[2];
-    const long long n1 = B.box.n[1], n2 = B.box.n[2];
-    const long long gz = 4 * m0 * m1, gy = 4 * m0 * n2;
     long long i, j, k;
-    if (u < gz) {  // planes k = 0, 1, m2 - 2, m2 - 1
-      const long long s = u / (m0 * m1), r = u - s * m0 * m1;
-      k = (s < 2) ? s : m2 - 4 + s;
-      j = r / m0;
-      i = r - j * m0;
-    } else if (u < gz + gy) {  // rows j = 0, 1, m1 - 2, m1 - 1 of the proper planes
-      const long long w = u - gz, s = w / (m0 * n2), r = w - s * m0 * n2;
-      j = (s < 2) ? s : m1 - 4 + s;
-      k = 2 + r / m0;
-      i = r - (k - 2) * m0;
-    } else {  // columns i = 0, 1, m0 - 2, m0 - 1 of the proper rows
-      const long long w = u - gz - gy, s = w / (n1 * n2), r = w - s * n1 * n2;
-      i = (s < 2) ? s : m0 - 4 + s;
-      k = 2 + r / n1;
-      j = 2 + (r - (k - 2) * n1);
-    }
-    const long long v = i + m0 * (j + m1 * k);
+    shell_cell(B.box, u, i, j, k);
+    const long long v = i + (long long)B.box.m[0] * (j + (long long)B.box.m[1] * k);
     int p[3] = {(int)i - 2, (int)j - 2, (int)k - 2};
     if (chart_reachable(B, p)) {
       int c[3] = {p[0], p[1], p[2]};

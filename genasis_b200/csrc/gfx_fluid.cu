@@ -653,8 +653,9 @@ int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, const BrickDesc* d1, bo
                         B->counters, B->ph, s));
   CUDA_TRY(launch_stage(MODE_STAGE2, true, B->hllc, false, none, B->d2, B->items, B->n_items,
                         B->counters + 1, B->ph, s));
-  batch_ghost_refresh_kernel<<<grid_for(B->total_v, blk), blk, 0, s>>>(B->bb, B->n,
-                                                                       B->total_v, B->ph);
+  const long long shells = B->total_v - B->total_c;
+  batch_ghost_refresh_kernel<<<grid_for(shells, blk), blk, 0, s>>>(B->bb, B->n, shells,
+                                                                   B->ph);
   advance_clock_kernel<<<grid_for(B->n, blk), blk, 0, s>>>(B->clocks, B->n);
   finalize_dt_kernel<<<grid_for(B->n, blk), blk, 0, s>>>(B->ph, B->tsi_bits, B->clocks, B->n, 1);
   CUDA_TRY(cudaGetLastError());
