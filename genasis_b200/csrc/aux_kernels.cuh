@@ -205,7 +205,6 @@ __global__ void ghost_refresh_range_kernel(Box b, Phys ph, double* __restrict__ 
 struct BatchBrick {
   Box box;
   double* U;
-  uint8_t* sb;
   uint8_t* df;
   const int* skip;
   long long v_off;  // prefix sum of nV
@@ -239,79 +238,6 @@ __global__ void batch_ghost_refresh_kernel(const BatchBrick* __restrict__ bb, in
     if (B.skip && *B.skip) continue;
     ghost_refresh_value(B.box, ph, B.U, shell_value(B.box, x - (B.v_off - B.c_off)));
   }
-}
-
-// Pressure and normal velocity of proper cell (i, j, k) of the state.
-__device__ __forceinline__ void cell_p_v(const Box& b, const Phys& ph, const double* U,
-                                         const double* Pst, int i, int j, int k, double& P,
-                                         double v[3]) {
-  Prim w;
-  if (Pst) {
-    const long long c = i + (long long)b.n[0] * (j + (long long)b.n[1] * k);
-    w.N = Pst[c];
-    w.V1 = Pst[b.nP + c];
-    w.V2 = Pst[2 * b.nP + c];
-    w.V3 = Pst[3 * b.nP + c];
-    w.E = Pst[4 * b.nP + c];
-  } else {
-    const long long o = (i + 2) + (long long)b.m[0] * ((j + 2) + (long long)b.m[1] * (k + 2));
-    Cons u{U[o], U[b.nV + o], U[2 * b.nV + o], U[3 * b.nV + o], U[4 * b.nV + o]};
-    cons_to_prim_exact(u, w, ph.nmin);
-  }
-  P = ph.gm1 * w.E;
-  v[0] = w.V1;
-  v[1] = w.V2;
-  v[2] = w.V3;
-}
-
-// DetectShocks_CSL_Kernel (FluidFeatures_P__Kernel.f90:12-186) for the proper
-// cells: bit e of sb[c] = shock along e at c (compared with c - e_e).
-__device__ __forceinline__ void detect_shock_cell(const Box& b, const Phys& ph, const double* U,
-                                                  const double* Pst, uint8_t* sb, long long c) {
-  int i, j, k;
-  decode3(c, b.n[0], b.n[1], i, j, k);
-  double P0, v0[3];
-  cell_p_v(b, ph, U, Pst, i, j, k, P0, v0);
-  uint8_t bits = 0;
-  const int t[3] = {i, j, k};
-#pragma unroll
-  for (int e = 0; e < 3; ++e) {
-    if (t[e] < 1) continue;
-    double P1, v1[3];
-    cell_p_v(b, ph, U, Pst, i - (e == 0), j - (e == 1), k - (e == 2), P1, v1);
-    if (shock_between(P0, P1, v0[e] - v1[e], ph.shock_threshold)) bits |= (uint8_t)(1u << e);
-  }
-  sb[c] = bits;
-}
-
-// DIFFUSIVE_FLUX_I flags after ClearBoundary_CSL_Kernel (FluidFeatures_P__Kernel.f90:
-// 189-313) on a single brick: only cells at least two cells inside every face
-// keep flags, and DF_d(x) is set by a shock along e != d at x, x + e_e, x - e_d
-// or x + e_e - e_d (the positions DetectShocks_CSL_Kernel writes).
-__device__ __forceinline__ void detect_flags_cell(const Box& b, const uint8_t* sb, uint8_t* df,
-                                                  long long c) {
-  int t[3];
-  decode3(c, b.n[0], b.n[1], t[0], t[1], t[2]);
-  uint8_t bits = 0;
-  bool interior = true;
-#pragma unroll
-  for (int d = 0; d < 3; ++d)
-    if (t[d] < 1 || t[d] > b.n[d] - 2) interior = false;
-  if (interior) {
-    const long long st[3] = {1, b.n[0], (long long)b.n[0] * b.n[1]};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-#pragma unroll
-      for (int e = 0; e < 3; ++e) {
-        if (e == d) continue;
-        const uint8_t m = (uint8_t)(1u << e);
-        if ((sb[c] & m) || (sb[c + st[e]] & m) || (sb[c - st[d]] & m) ||
-            (sb[c + st[e] - st[d]] & m))
-          bits |= (uint8_t)(1u << d);
-      }
-    }
-  }
-  df[c] = bits;
 }
 
 // Tiles of the feature detection over the planes [k0, k1): 32 x 8 cells of a
@@ -359,11 +285,17 @@ struct DetectBrick {
   }
 };
 
-// Shock bits (detect_shock_cell) and DIFFUSIVE_FLUX_I flags (detect_flags_cell)
-// of the proper cells of planes [k0, k1) of a box of n0 x n1 x n2 cells in one
-// pass, from the state that `src` reads (a brick, or a chart of bricks by
-// its global coordinates; raw values: E, V1, V2, V3 with PST, else D, S1,
-// S2, S3, G).  For every plane kk each thread recovers pressure and
+// Shock bits and DIFFUSIVE_FLUX_I flags of the proper cells of a tile of a box
+// of n0 x n1 x n2 cells in one pass: DetectShocks_CSL_Kernel
+// (FluidFeatures_P__Kernel.f90:12-186) sets bit e of a cell for a shock along
+// e between it and the cell before it along e; after ClearBoundary_CSL_Kernel
+// (:189-313) only cells not next to a face keep flags, and
+// flag d is set by a shock along e != d at x, x + e_e, x - e_d or
+// x + e_e - e_d (the positions DetectShocks_CSL_Kernel writes).  The state is
+// the one that `src` reads (a brick, or a chart of bricks by its global
+// coordinates; raw values: E, V1, V2, V3 with PST, else D, S1, S2, S3, G).
+// The tile of this block: columns i0 .. i0 + 31, rows j0 .. j0 + 7, planes
+// [kb, ke) (at most kDetKZ).  For every plane kk each thread recovers pressure and
 // velocities of its halo-tile cell (its loads for plane kk + 1 are issued
 // before the CTA synchronises), forms the cell's shock bits from the -x and
 // -y neighbours in shared memory and the -z neighbour kept in registers, and
@@ -372,18 +304,15 @@ struct DetectBrick {
 // only.  A bit that no flag reads (x at the left halo column, y at the bottom
 // halo row, z at the first plane) is left zero, and so is every bit outside
 // the box, which only cells without flags would read.  Reads the state of
-// planes k0 - 1 to k1 (those that exist); writes the flags of planes
-// [k0, k1).
+// planes kb - 1 to ke (those that exist); writes the flags of planes
+// [kb, ke).
 template <bool PST, class Src>
 __device__ __forceinline__ void detect_tile(const Src& src, const Phys& ph, int n0, int n1,
-                                            int n2, int k0, int k1) {
+                                            int n2, int i0, int j0, int kb, int ke) {
   constexpr int RX = kDetRX, NR = kDetNR;
   __shared__ double sP[NR], sV1[NR], sV2[NR];
   __shared__ uint8_t sS[3][NR];
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * kDetTX, j0 = blockIdx.y * kDetTY;
-  const int kb = k0 + blockIdx.z * kDetKZ;
-  const int ke = min(kb + kDetKZ, k1);
   const double thr = ph.shock_threshold;
   // the halo-tile cell of this thread
   const int rx = tid % RX, ry = tid / RX;
@@ -474,27 +403,28 @@ __global__ void __launch_bounds__(kDetThreads, 3)
                            const double* __restrict__ Pst, uint8_t* __restrict__ df, int k0,
                            int k1) {
   const DetectBrick<PST> src(b, U, Pst, df);
-  detect_tile<PST>(src, ph, b.n[0], b.n[1], b.n[2], k0, k1);
+  const int kb = k0 + blockIdx.z * kDetKZ;
+  detect_tile<PST>(src, ph, b.n[0], b.n[1], b.n[2], blockIdx.x * kDetTX, blockIdx.y * kDetTY, kb,
+                   min(kb + kDetKZ, k1));
 }
 
-__global__ void batch_detect_shock_kernel(const BatchBrick* __restrict__ bb, int n,
-                                          long long total, Phys ph) {
-  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
-       x += (long long)gridDim.x * blockDim.x) {
-    const int b = find_brick(bb, n, x, true);
-    if (bb[b].skip && *bb[b].skip) continue;
-    detect_shock_cell(bb[b].box, ph, bb[b].U, nullptr, bb[b].sb, x - bb[b].c_off);
-  }
-}
+// A tile of the features of a batch: brick, and the tile's first column, row
+// and plane.
+struct DetItem {
+  int brick, i0, j0, k0;
+};
 
-__global__ void batch_detect_flags_kernel(const BatchBrick* __restrict__ bb, int n,
-                                          long long total) {
-  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total;
-       x += (long long)gridDim.x * blockDim.x) {
-    const int b = find_brick(bb, n, x, true);
-    if (bb[b].skip && *bb[b].skip) continue;
-    detect_flags_cell(bb[b].box, bb[b].sb, bb[b].df, x - bb[b].c_off);
-  }
+// The features of every brick of a batch from the conserved states, one
+// block per tile of the work list (detect_tile on the tile's brick).
+__global__ void __launch_bounds__(kDetThreads, 3)
+    batch_detect_features_kernel(const BatchBrick* __restrict__ bb,
+                                 const DetItem* __restrict__ items, Phys ph) {
+  const DetItem it = items[blockIdx.x];
+  const BatchBrick& B = bb[it.brick];
+  if (B.skip && *B.skip) return;
+  const DetectBrick<false> src(B.box, B.U, nullptr, B.df);
+  detect_tile<false>(src, ph, B.box.n[0], B.box.n[1], B.box.n[2], it.i0, it.j0, it.k0,
+                     min(it.k0 + kDetKZ, B.box.n[2]));
 }
 
 // Per-cell inverse CFL time of the state, reduced to one maximum

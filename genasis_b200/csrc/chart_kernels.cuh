@@ -207,7 +207,9 @@ __global__ void __launch_bounds__(kDetThreads, 3)
                                  Phys ph, const int* skip) {
   if (skip && *skip) return;
   const DetectChart<PST> src{cb, nbx, nby, cb[0].box.n[0], cb[0].box.n[1], cb[0].box.n[2]};
-  detect_tile<PST>(src, ph, nbx * src.bn0, nby * src.bn1, nbz * src.bn2, 0, nbz * src.bn2);
+  const int n2 = nbz * src.bn2, kb = blockIdx.z * kDetKZ;
+  detect_tile<PST>(src, ph, nbx * src.bn0, nby * src.bn1, n2, blockIdx.x * kDetTX,
+                   blockIdx.y * kDetTY, kb, min(kb + kDetKZ, n2));
 }
 
 // Ghost values at the end of a step: an exchange-reachable ghost takes the

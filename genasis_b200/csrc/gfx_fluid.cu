@@ -171,7 +171,6 @@ struct gfx_fluid {
   double* H = nullptr;
   double* Pst = nullptr;
   uint8_t* df = nullptr;
-  uint8_t* sb = nullptr;
   unsigned long long* tsi_bits = nullptr;  // [1]
   int* counters = nullptr;                 // [4]
   Clock* clock = nullptr;                  // evolve clock
@@ -615,6 +614,8 @@ struct gfx_fluid_batch {
   BrickDesc* d2 = nullptr;   // stage 2, per brick
   WorkItem* items = nullptr;
   int n_items = 0;
+  DetItem* det_items = nullptr;  // tiles of the features (HLLC)
+  int n_det_items = 0;
   BatchBrick* bb = nullptr;
   long long total_v = 0, total_c = 0;
   unsigned long long* tsi_bits = nullptr;  // [n]
@@ -639,12 +640,10 @@ int enqueue_batch_cycle(gfx_fluid_batch* B, bool detect, const BrickDesc* d1, bo
   CUDA_TRY(cudaGetLastError());
   B->launches += 1;
   if (B->hllc && detect) {
-    batch_detect_shock_kernel<<<grid_for(B->total_c, blk), blk, 0, s>>>(B->bb, B->n,
-                                                                        B->total_c, B->ph);
-    batch_detect_flags_kernel<<<grid_for(B->total_c, blk), blk, 0, s>>>(B->bb, B->n,
-                                                                        B->total_c);
+    batch_detect_features_kernel<<<B->n_det_items, kDetThreads, 0, s>>>(B->bb, B->det_items,
+                                                                        B->ph);
     CUDA_TRY(cudaGetLastError());
-    B->launches += 2;
+    B->launches += 1;
   }
   BrickDesc none;
   memset(&none, 0, sizeof(none));
@@ -962,7 +961,7 @@ int create_handle(const gfx_fluid_config* cfg, const HostAxis* axes, gfx_fluid**
   if (cudaMalloc(&h->Yp, 5 * nP * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&h->H, 5 * nP * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&h->Pst, 5 * nP * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->df, nP) != cudaSuccess || cudaMalloc(&h->sb, nP) != cudaSuccess ||
+      cudaMalloc(&h->df, nP) != cudaSuccess ||
       cudaMalloc(&h->tsi_bits, 2 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&h->counters, 4 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&h->clock, 2 * sizeof(Clock)) != cudaSuccess ||
@@ -995,7 +994,6 @@ int gfx_fluid_destroy(gfx_fluid* h) {
   cudaFree(h->H);
   cudaFree(h->Pst);
   cudaFree(h->df);
-  cudaFree(h->sb);
   cudaFree(h->tsi_bits);
   cudaFree(h->counters);
   cudaFree(h->clock);
@@ -1410,9 +1408,13 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
   std::vector<BatchBrick> bb(n);
   std::vector<WorkItem> items;
   std::vector<long long> work;
+  std::vector<DetItem> det;
   for (int b = 0; b < n; ++b) {
     gfx_fluid* h = handles[b];
     const uint8_t* df = B->hllc ? h->df : nullptr;
+    for (int z = 0; z < h->box.n[2]; z += kDetKZ)
+      for (int y = 0; y < h->box.n[1]; y += kDetTY)
+        for (int x = 0; x < h->box.n[0]; x += kDetTX) det.push_back({b, x, y, z});
     const double* dt = &B->clocks[b].dt;
     const int* skip = &B->clocks[b].done;
     d1[b] = make_desc(h, U[b], nullptr, nullptr, nullptr, df, nullptr, dt, 0.5, skip);
@@ -1423,7 +1425,6 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
     d1[b].tsi_bits = d1p[b].tsi_bits = d1w[b].tsi_bits = d2[b].tsi_bits = B->tsi_bits + b;
     bb[b].box = h->box;
     bb[b].U = U[b];
-    bb[b].sb = h->sb;
     bb[b].df = h->df;
     bb[b].skip = skip;
     bb[b].v_off = B->total_v;
@@ -1452,6 +1453,14 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
   B->n_items = (int)sorted.size();
   if (cudaMalloc(&B->items, sorted.size() * sizeof(WorkItem)) != cudaSuccess)
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch work items"));
+  if (B->hllc) {
+    B->n_det_items = (int)det.size();
+    if (cudaMalloc(&B->det_items, det.size() * sizeof(DetItem)) != cudaSuccess)
+      return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch feature tiles"));
+    if (cudaMemcpy(B->det_items, det.data(), det.size() * sizeof(DetItem),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return cleanup(fail(GFX_ERR_CUDA, "copy batch feature tiles"));
+  }
   if (cudaMemcpy(B->d1, d1.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
       cudaMemcpy(B->d1p, d1p.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
       cudaMemcpy(B->d1w, d1w.data(), n * sizeof(BrickDesc), cudaMemcpyHostToDevice) ||
@@ -1484,6 +1493,7 @@ int gfx_fluid_batch_destroy(gfx_fluid_batch* B) {
   cudaFree(B->d2);
   cudaFree(B->bb);
   cudaFree(B->items);
+  cudaFree(B->det_items);
   delete B;
   return GFX_OK;
 }
