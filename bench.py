@@ -236,16 +236,16 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def fp64_peak():
+def fp64_peak(reps=10):
     """The device's FP64 rate (FLOP/s, a fused multiply-add counting two):
     genasis_b200/libgfx_probe.so times chains of fused multiply-adds on every
-    SM, best of 10 launches."""
+    SM, best of `reps` launches (about 0.55 ms each on a B200)."""
     import ctypes
 
     try:
         probe = ctypes.CDLL(os.path.join(ROOT, "genasis_b200", "libgfx_probe.so"))
         f, ms = ctypes.c_double(), ctypes.c_double()
-        if probe.gfx_probe_fp64(10, ctypes.byref(f), ctypes.byref(ms)) == 0:
+        if probe.gfx_probe_fp64(int(reps), ctypes.byref(f), ctypes.byref(ms)) == 0:
             return f.value
     except OSError:
         pass
@@ -290,14 +290,20 @@ def pipe_use(kernel):
 def _timed_evolve(box, steps, warmup, local, world):
     """Warm-up cycles (they also capture the cycle graph), then `steps` cycles
     of gfx_fluid_evolve timed with CUDA events on the launching stream between
-    barriers, with the clocks sampled meanwhile.  The sampler starts before
-    the warm-up, so that the device is busy up to the timed region (no idle
-    gap for the clocks to drop in, and nvidia-smi's start-up stays outside)."""
+    barriers, with the clocks sampled meanwhile.  The sampler starts first;
+    then the FP64 probe of the roofline runs (about 0.2 s of full load), so
+    that the device is at its running clock, not ramping up from idle, when
+    the warm-up cycles and the timed region follow without a gap.  The events
+    are the ones gfx_fluid_evolve_timed records just before its first and
+    after its last launch (a host delay before the call's first launch, or
+    before it returns, would otherwise count as device time); events around
+    the call are kept beside them as "ms_call"."""
     import torch
 
     stream = torch.cuda.current_stream()
     sampler = ClockSampler(local)
     sampler.start()
+    fp64 = fp64_peak(reps=400)
     t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
     torch.cuda.synchronize()
     launches0 = box.kernel_launches()
@@ -306,13 +312,14 @@ def _timed_evolve(box, steps, warmup, local, world):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=steps)
+    t_sim, cyc2, ms = box.evolve_timed(1e30, t_sim, cyc, max_cycles=steps)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop()
-    return {"ms": ev0.elapsed_time(ev1), "steps": cyc2 - cyc, "t_sim": t_sim, "cycle": cyc2,
-            "launches": box.kernel_launches() - launches0, "clocks": clocks}
+    return {"ms": ms, "ms_call": ev0.elapsed_time(ev1), "steps": cyc2 - cyc, "t_sim": t_sim,
+            "cycle": cyc2, "launches": box.kernel_launches() - launches0, "clocks": clocks,
+            "fp64": fp64}
 
 
 def _sine_box(args, cfg, prim, variant):
@@ -446,7 +453,8 @@ def _stage_timing(box, cfg, cyc, steps, fp64_rate=None):
                         "peak_tflops": fp64_rate / 1e12 if fp64_rate else None,
                         "frac": rate / fp64_rate if fp64_rate else None,
                         "peak_source": "measured by genasis_b200/libgfx_probe.so (chains of "
-                                       "fused multiply-adds, best of 10)",
+                                       "fused multiply-adds, best of 400 launches run "
+                                       "right before the warm-up cycles)",
                         "counts_source": "profiles/stage_fp64.json (ncu thread instructions "
                                          "dadd + dmul + 2 dfma, %s)" % counts.get("case", "")}
     return dt, avg, dom, roof
@@ -465,12 +473,13 @@ def run_ours(args):
     t = _timed_evolve(box, args.steps, args.warmup, local, world)
     ms, steps_done, t_sim, cyc2 = t["ms"], t["steps"], t["t_sim"], t["cycle"]
     ms_max = max_over_ranks(ms, world)
+    ms_call_max = max_over_ranks(t["ms_call"], world)
     value = replica_rate(cells, steps_done, ms, world)
     # L1 density error against the exact translated profile at the end of the
     # timed region (before the extra steps below move the state on)
     l1 = _sine_l1(box, cfg, t_sim)
 
-    rate64 = fp64_peak()
+    rate64 = t["fp64"] or fp64_peak()
     dt, avg, dom, roofline = _stage_timing(box, cfg, cyc2, args.steps, rate64)
     roofline["step_hbm_frac"] = STEP_BYTES * value / world / 1e9 / roofline["peak"]
     roofline["ncu_pipes"] = pipe_use(dom)
@@ -585,7 +594,11 @@ def run_ours(args):
                            6 * (args.n + 4) ** 3 * 8 / 1e6),
                        "l1_density_error": l1, "sim_time": t_sim,
                        "full_crossing": crossing,
-                       "tuning": _tuning_of(args, cfg)},
+                       "tuning": _tuning_of(args, cfg),
+                       "timing": "CUDA events on the launching stream, recorded by "
+                                 "gfx_fluid_evolve_timed just before its first and after its "
+                                 "last launch; ms_per_step_call: events around the call"},
+            "ms_per_step_call": ms_call_max / steps_done,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

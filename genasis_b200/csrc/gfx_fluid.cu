@@ -176,6 +176,7 @@ struct gfx_fluid {
   Clock* clock = nullptr;                  // evolve clock
   Clock* clock_host = nullptr;             // [2] pinned copies read between chunks
   cudaEvent_t chunk_ev[2] = {};            // after each copy
+  cudaEvent_t evolve_ev[2] = {};           // gfx_fluid_evolve_timed: around its work
   double* dt_slot = nullptr;               // dt of gfx_fluid_step
   WorkItem* items = nullptr;
   int n_items = 0;
@@ -1015,8 +1016,10 @@ int gfx_fluid_destroy(gfx_fluid* h) {
     if (h->ev_out[j]) cudaEventDestroy(h->ev_out[j]);
   }
   if (h->ev_end) cudaEventDestroy(h->ev_end);
-  for (int j = 0; j < 2; ++j)
+  for (int j = 0; j < 2; ++j) {
     if (h->chunk_ev[j]) cudaEventDestroy(h->chunk_ev[j]);
+    if (h->evolve_ev[j]) cudaEventDestroy(h->evolve_ev[j]);
+  }
   if (h->clock_host) cudaFreeHost(h->clock_host);
   if (h->copy_in) cudaStreamDestroy(h->copy_in);
   if (h->copy_out) cudaStreamDestroy(h->copy_out);
@@ -1216,12 +1219,18 @@ int gfx_fluid_timestep(gfx_fluid* h, const double* U, int i_cycle, double* dt_ho
   return GFX_OK;
 }
 
-int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double finish_time,
-                     int n_cycles_max, double* time_out, int* i_cycle_out, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// The evolve loop of gfx_fluid_evolve; ev (may be null): two events, recorded
+// on the stream before the first of its device work and after the last.
+int evolve_impl(gfx_fluid* h, double* U, double time, int i_cycle, double finish_time,
+                int n_cycles_max, double* time_out, int* i_cycle_out, cudaStream_t s,
+                cudaEvent_t* ev) {
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_evolve")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (n_cycles_max < 0) return fail(GFX_ERR_ARGUMENT, "n_cycles_max < 0");
-  cudaStream_t s = (cudaStream_t)stream;
   Clock c;
   memset(&c, 0, sizeof(c));
   c.time = time;
@@ -1230,6 +1239,7 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
   c.max_cycle = (int)std::min<long long>(0x7fffffffLL, (long long)i_cycle + n_cycles_max);
   c.done = !(c.time < c.finish && c.cycle < c.max_cycle);
   Clock* dc = h->clock;
+  if (ev) CUDA_TRY(cudaEventRecord(ev[0], s));
   CUDA_TRY(cudaMemcpyAsync(dc, &c, sizeof(c), cudaMemcpyHostToDevice, s));
   if (!c.done) {
     // initial dt from the state (ComputeNewTime before the first cycle)
@@ -1311,10 +1321,37 @@ int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double f
       slot ^= 1;
     }
   }
+  if (ev) CUDA_TRY(cudaEventRecord(ev[1], s));
   CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   if (time_out) *time_out = c.time;
   if (i_cycle_out) *i_cycle_out = c.cycle;
+  return GFX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfx_fluid_evolve(gfx_fluid* h, double* U, double time, int i_cycle, double finish_time,
+                     int n_cycles_max, double* time_out, int* i_cycle_out, void* stream) {
+  return evolve_impl(h, U, time, i_cycle, finish_time, n_cycles_max, time_out, i_cycle_out,
+                     (cudaStream_t)stream, nullptr);
+}
+
+int gfx_fluid_evolve_timed(gfx_fluid* h, double* U, double time, int i_cycle,
+                           double finish_time, int n_cycles_max, double* time_out,
+                           int* i_cycle_out, double* ms_out, void* stream) {
+  if (!h || !ms_out) return fail(GFX_ERR_ARGUMENT, "NULL argument");
+  if (!h->evolve_ev[0]) {
+    for (int j = 0; j < 2; ++j) CUDA_TRY(cudaEventCreate(&h->evolve_ev[j]));
+  }
+  int rc = evolve_impl(h, U, time, i_cycle, finish_time, n_cycles_max, time_out, i_cycle_out,
+                       (cudaStream_t)stream, h->evolve_ev);
+  if (rc) return rc;
+  float ms = 0.0f;
+  CUDA_TRY(cudaEventElapsedTime(&ms, h->evolve_ev[0], h->evolve_ev[1]));
+  *ms_out = ms;
   return GFX_OK;
 }
 

@@ -211,6 +211,18 @@ class FluidBox:
                  _stream())
         return t.value, c.value
 
+    def evolve_timed(self, finish_time, time=0.0, i_cycle=0, max_cycles=2**31 - 1):
+        """evolve, and the device milliseconds of its work (CUDA events the
+        library records just before its first and after its last launch):
+        returns (time, cycle, ms)."""
+        t = ctypes.c_double()
+        c = ctypes.c_int()
+        ms = ctypes.c_double()
+        self.call("gfx_fluid_evolve_timed", self.h, _ptr(self.U), float(time), int(i_cycle),
+                  float(finish_time), int(max_cycles), ctypes.byref(t), ctypes.byref(c),
+                  ctypes.byref(ms), _stream())
+        return t.value, c.value, ms.value
+
 
 class Step_RK2_C_ASC:
     """Step_RK_C_ASC_Template % Compute (Step_RK_C_ASC__Template.f90:504-542)

@@ -51,6 +51,8 @@ SIGNATURES = {
     "gfx_fluid_step_host": [P, P, D, P],
     "gfx_fluid_timestep": [P, P, I, ctypes.POINTER(D), P],
     "gfx_fluid_evolve": [P, P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I), P],
+    "gfx_fluid_evolve_timed": [P, P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I),
+                               ctypes.POINTER(D), P],
     "gfx_fluid_step_timed": [P, P, D, P, P, P],
     "gfx_fluid_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
     "gfx_fluid_batch_create": [I, P, P, ctypes.POINTER(P)],

@@ -172,6 +172,17 @@ int gfx_fluid_evolve(gfx_fluid *h, double *U_dev, double time, int i_cycle,
                      double finish_time, int n_cycles_max, double *time_out,
                      int *i_cycle_out, void *stream);
 
+/* gfx_fluid_evolve that also gives the device milliseconds of its work in
+ * ms_out: CUDA events recorded on the stream just before its first device
+ * operation and just after its last (the reference's Evolve timer,
+ * Integrator_Template.f90:291-346, on the device).  The call returns after
+ * the work completes, like gfx_fluid_evolve, but a host delay before its
+ * first launch or before the return stays out of ms_out; the results are
+ * those of gfx_fluid_evolve bit for bit. */
+int gfx_fluid_evolve_timed(gfx_fluid *h, double *U_dev, double time, int i_cycle,
+                           double finish_time, int n_cycles_max, double *time_out,
+                           int *i_cycle_out, double *ms_out, void *stream);
+
 /* gfx_fluid_step with a CUDA event recorded around each launch (the
  * reference's per-phase timers, StorageDivergence_Form.f90:45-74): ms_out[4]
  * receives the device milliseconds of features, stage 1, stage 2 and the

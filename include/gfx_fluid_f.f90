@@ -60,7 +60,7 @@ module GFX_Fluid_C
     gfx_fluid_clear_features, gfx_fluid_get_features, gfx_fluid_increment, &
     gfx_fluid_fluence_face_size, gfx_fluid_step, gfx_fluid_step_sources, &
     gfx_fluid_step_host, &
-    gfx_fluid_timestep, gfx_fluid_evolve, gfx_fluid_step_timed, &
+    gfx_fluid_timestep, gfx_fluid_evolve, gfx_fluid_evolve_timed, gfx_fluid_step_timed, &
     gfx_fluid_kernel_launches, gfx_fluid_step_adjoint, gfx_fluid_step_branches, &
     gfx_fluid_set_tuning, gfx_fluid_batch_create, gfx_fluid_batch_destroy, &
     gfx_fluid_batch_set_clocks, gfx_fluid_batch_evolve, &
@@ -201,6 +201,18 @@ module GFX_Fluid_C
       real ( c_double ), intent ( out ) :: TimeOut
       integer ( c_int ), intent ( out ) :: iCycleOut
     end function gfx_fluid_evolve
+
+    integer ( c_int ) function gfx_fluid_evolve_timed &
+      ( Handle, Conserved_dev, Time, iCycle, FinishTime, nCyclesMax, TimeOut, &
+        iCycleOut, DeviceMilliseconds, Stream ) &
+      bind ( c, name = 'gfx_fluid_evolve_timed' )
+      import
+      type ( c_ptr ), value :: Handle, Conserved_dev, Stream
+      real ( c_double ), value :: Time, FinishTime
+      integer ( c_int ), value :: iCycle, nCyclesMax
+      real ( c_double ), intent ( out ) :: TimeOut, DeviceMilliseconds
+      integer ( c_int ), intent ( out ) :: iCycleOut
+    end function gfx_fluid_evolve_timed
 
     integer ( c_int ) function gfx_fluid_step_timed &
       ( Handle, Conserved_dev, TimeStep, Fluence_dev, Milliseconds, Stream ) &
