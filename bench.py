@@ -236,16 +236,18 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def fp64_peak(reps=10):
+def fp64_peak(reps=10, iters=4096):
     """The device's FP64 rate (FLOP/s, a fused multiply-add counting two):
     genasis_b200/libgfx_probe.so times chains of fused multiply-adds on every
-    SM, best of `reps` launches (about 0.55 ms each on a B200)."""
+    SM, best of `reps` launches of `iters` steps per chain (4096 steps take
+    about 0.55 ms on a B200)."""
     import ctypes
 
     try:
         probe = ctypes.CDLL(os.path.join(ROOT, "genasis_b200", "libgfx_probe.so"))
         f, ms = ctypes.c_double(), ctypes.c_double()
-        if probe.gfx_probe_fp64(int(reps), ctypes.byref(f), ctypes.byref(ms)) == 0:
+        if probe.gfx_probe_fp64_chains(int(reps), int(iters), ctypes.byref(f),
+                                       ctypes.byref(ms)) == 0:
             return f.value
     except OSError:
         pass
@@ -303,7 +305,7 @@ def _timed_evolve(box, steps, warmup, local, world):
     stream = torch.cuda.current_stream()
     sampler = ClockSampler(local)
     sampler.start()
-    fp64 = fp64_peak(reps=400)
+    fp64 = fp64_peak(reps=20, iters=20 * 4096)
     t_sim, cyc = box.evolve(1e30, 0.0, 0, max_cycles=max(warmup, 3))
     torch.cuda.synchronize()
     launches0 = box.kernel_launches()
@@ -453,8 +455,8 @@ def _stage_timing(box, cfg, cyc, steps, fp64_rate=None):
                         "peak_tflops": fp64_rate / 1e12 if fp64_rate else None,
                         "frac": rate / fp64_rate if fp64_rate else None,
                         "peak_source": "measured by genasis_b200/libgfx_probe.so (chains of "
-                                       "fused multiply-adds, best of 400 launches run "
-                                       "right before the warm-up cycles)",
+                                       "fused multiply-adds, best of 20 launches of about "
+                                       "11 ms run right before the warm-up cycles)",
                         "counts_source": "profiles/stage_fp64.json (ncu thread instructions "
                                          "dadd + dmul + 2 dfma, %s)" % counts.get("case", "")}
     return dt, avg, dom, roof

@@ -41,6 +41,24 @@ def test_every_declared_symbol_is_exported_and_bound(variant):
     assert set(names) == set(lib.exported_symbols())
 
 
+def test_fp64_probe_exports_and_refuses_bad_arguments():
+    """libgfx_probe.so, the bench's FP64 rate probe, is built beside the
+    library and checks its arguments before any CUDA call."""
+    from genasis_b200 import build_ext
+
+    build_ext.build()
+    so = ctypes.CDLL(os.path.join(ROOT, "genasis_b200", "libgfx_probe.so"))
+    f, ms = ctypes.c_double(), ctypes.c_double()
+    fn = so.gfx_probe_fp64_chains
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                   ctypes.POINTER(ctypes.c_double)]
+    assert fn(0, 4096, ctypes.byref(f), ctypes.byref(ms)) == -1
+    assert fn(1, 0, ctypes.byref(f), ctypes.byref(ms)) == -1
+    assert fn(1, 4096, None, ctypes.byref(ms)) == -1
+    assert hasattr(so, "gfx_probe_fp64")
+
+
 def test_config_struct_layout_matches_header_defaults():
     c = GfxConfig()
     lib.call("gfx_fluid_config_default", ctypes.byref(c))

@@ -61,3 +61,21 @@ def test_timed_evolve_equals_the_evolve():
     assert 0.0 < ms <= e0.elapsed_time(e1)
     a.close()
     b.close()
+
+
+def test_fp64_probe_rate_is_independent_of_the_chain_length():
+    """The bench's FP64 probe: short and long launches give the same rate
+    (within 20 %), in the range of a B200's FP64 pipes."""
+    import ctypes
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    so = ctypes.CDLL(os.path.join(root, "genasis_b200", "libgfx_probe.so"))
+    rates = []
+    for reps, iters in ((5, 4096), (2, 4 * 4096)):
+        f, ms = ctypes.c_double(), ctypes.c_double()
+        assert so.gfx_probe_fp64_chains(reps, iters, ctypes.byref(f), ctypes.byref(ms)) == 0
+        assert ms.value > 0.0
+        rates.append(f.value)
+    assert 1e12 < rates[0] < 1e14
+    assert abs(rates[1] / rates[0] - 1.0) < 0.2
