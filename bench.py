@@ -179,6 +179,19 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def sum_over_ranks(x, world):
+    """The sum of x over the ranks (counts of the whole job)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return type(x)(t.item())
+
+
 def replica_rate(cells, steps, ms_per_rank, world):
     """Whole-job cell-updates/s of independent replicas: every rank's cells
     over the slowest rank's time."""
@@ -626,22 +639,32 @@ def _tuning_of(args, cfg):
     return {"z_chunk": e.get("z_chunk"), "tile": "32x%s" % e.get("tile_rows")}
 
 
-def bricks_result(steps=50, warmup=3, n_bricks=512, variant="exact"):
+def bricks_result(steps=50, warmup=3, n_bricks=512, variant="exact", world=1, rank=0):
     """512 independent bricks, edges U{16..96} per axis (seeded), seeded
     two-state Riemann problems, outflow, PLM + HLL, RK2, CFL 0.8: K cycles of
     the batched path (one persistent launch per stage, one graph per cycle)
     against K cycles of each brick's own single-brick path, brick after brick,
-    each timed with CUDA events."""
+    each timed with CUDA events.  With world > 1 ranks (one per GPU) the
+    bricks are split over the ranks (genasis_b200.batch.shard_bricks), each
+    rank advances its own with no data exchange, and the times are the
+    slowest rank's."""
     import torch
 
     from genasis_b200 import problems
-    from genasis_b200.batch import FluidBatch
+    from genasis_b200.batch import FluidBatch, shard_bricks
 
-    torch.cuda.set_device(0)
-    bricks = problems.random_bricks(count=n_bricks, seed=20261203, riemann_solver="HLL")
-    cfgs = [c for c, _ in bricks]
-    prims = [p for _, p in bricks]
-    cells = sum(c.n_proper for c in cfgs)
+    if world == 1:
+        torch.cuda.set_device(0)
+    all_cfgs = [c for c, _ in problems.random_bricks(count=n_bricks, seed=20261203,
+                                                      riemann_solver="HLL", only=set())]
+    mine = shard_bricks(all_cfgs, world, rank)
+    bricks = problems.random_bricks(count=n_bricks, seed=20261203, riemann_solver="HLL",
+                                    only=set(mine))
+    cfgs = [bricks[i][0] for i in mine]
+    prims = [bricks[i][1] for i in mine]
+    del bricks
+    cells = sum(c.n_proper for c in all_cfgs)
+    cells_mine = sum(c.n_proper for c in cfgs)
     batch = FluidBatch(cfgs, variant=variant)
     K = steps
     # the pencil length of the batch's work items: autotuned (cached per GPU
@@ -658,6 +681,7 @@ def bricks_result(steps=50, warmup=3, n_bricks=512, variant="exact"):
     batch.set_primitives(prims)
     batch.set_clocks(0.0, 0)
     torch.cuda.synchronize()
+    barrier(world)
     l0 = batch.kernel_launches()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     e[0].record()
@@ -674,6 +698,7 @@ def bricks_result(steps=50, warmup=3, n_bricks=512, variant="exact"):
     for b, p in zip(batch.boxes, prims):
         b.compute_from_primitive(p)
     torch.cuda.synchronize()
+    barrier(world)
     l1 = sum(b.kernel_launches() for b in batch.boxes)
     e[2].record()
     for b in batch.boxes:
@@ -683,14 +708,25 @@ def bricks_result(steps=50, warmup=3, n_bricks=512, variant="exact"):
     t_plain = e[2].elapsed_time(e[3]) / 1000.0
     launches_plain = sum(b.kernel_launches() for b in batch.boxes) - l1
     same = all(torch.equal(a, b.U) for a, b in zip(U_batch, batch.boxes))
+    # the job's figures: the slowest rank's times, every rank's launches, and
+    # the batch equal to the loop on every rank (the same steps on all ranks)
+    t_batch = max_over_ranks(t_batch, world)
+    t_plain = max_over_ranks(t_plain, world)
+    launches_batch = sum_over_ranks(launches_batch, world)
+    launches_plain = sum_over_ranks(launches_plain, world)
+    same = max_over_ranks(0.0 if same else 1.0, world) == 0.0
     line = {
         "metric": "FP64 cell-updates/s (batched bricks)", "value": cells * K / t_batch,
-        "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(warmup, 3),
-        "ms_per_step": 1000.0 * t_batch / K, "higher_is_better": True, "scaling": "weak",
+        "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(warmup, 3),
+        "ms_per_step": 1000.0 * t_batch / K, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "bricks_%d" % n_bricks, "cells": cells, "riemann": "HLL",
                    "boundary": "outflow", "cfl": 0.8, "edges": "U{16..96}", "seed": 20261203,
                    "library": variant,
+                   "parallelism": ("bricks split over %d ranks by proper cells, no data "
+                                   "exchange" % world) if world > 1 else "single",
+                   "cells_this_rank": cells_mine, "bricks_this_rank": len(mine),
                    "plain_loop": "each brick's own gfx_fluid_evolve (a graph per cycle), "
                                  "brick after brick"},
         "plain_loop": {"value": cells * K / t_plain, "ms_per_step": 1000.0 * t_plain / K,
@@ -1230,7 +1266,15 @@ def main():
         return
     n = args.n if args.n != 256 else 128
     if args.workload == "bricks":
-        line = bricks_result(args.steps, args.warmup, args.bricks, args.variant)
+        world, rank, _ = dist_init()
+        line = bricks_result(args.steps, args.warmup, args.bricks, args.variant, world, rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
     elif args.workload == "adjoint":
         line = adjoint_result(n, args.directions, args.warmup, not args.no_cpu_baseline,
                               args.variant)

@@ -21,6 +21,7 @@ kept in a JSON cache keyed by the GPU's name and a bucket of the problem
 the brick count and the sizes' digest).  The shipped cache, tuning/<GPU>.json,
 was measured on B200s; set GFX_TUNING_CACHE to use another file.
 """
+import fcntl
 import hashlib
 import json
 import os
@@ -41,8 +42,8 @@ def gpu_name():
 
 
 def cache_path():
-    return os.environ.get("GFX_TUNING_CACHE",
-                          os.path.join(_HERE, "tuning", gpu_name() + ".json"))
+    path = os.environ.get("GFX_TUNING_CACHE")
+    return path if path else os.path.join(_HERE, "tuning", gpu_name() + ".json")
 
 
 def load_cache():
@@ -53,13 +54,24 @@ def load_cache():
         return {}
 
 
-def save_cache(cache):
+def save_entry(key, entry):
+    """Adds one entry to the cache file.  Ranks that tune at once on one host
+    (a batch split over GPUs, each rank with its own bricks) each add their
+    own key: the file is read, merged and replaced under an exclusive lock on
+    a lock file beside it, through a temporary file of this process."""
     path = cache_path()
     os.makedirs(os.path.dirname(path), exist_ok=True)
-    tmp = path + ".tmp"
-    with open(tmp, "w") as f:
-        json.dump(cache, f, indent=1, sort_keys=True)
-    os.replace(tmp, path)
+    with open(path + ".lock", "a") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            cache = load_cache()
+            cache[key] = entry
+            tmp = "%s.%d.tmp" % (path, os.getpid())
+            with open(tmp, "w") as f:
+                json.dump(cache, f, indent=1, sort_keys=True)
+            os.replace(tmp, path)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
 
 
 def _variant_suffix(variant):
@@ -143,7 +155,7 @@ def tuned_box(cfg, retune=False, adjoint=True, variant=None):
     key = brick_key(cfg, variant)
     if retune or "tile_rows" not in cache.get(key, {}):
         cache[key] = tune_brick(cfg, adjoint=adjoint, variant=variant)
-        save_cache(cache)
+        save_entry(key, cache[key])
     box = FluidBox(cfg, variant=variant)
     e = cache[key]
     box.set_tuning(e["z_chunk"], e["adjoint_segment"], e["tile_rows"])
@@ -175,7 +187,7 @@ def tune_batch(batch, prims, cycles=3, retune=False):
     best = min(ms, key=ms.get)
     best_r, best_z = (int(v) for v in best.split("x"))
     cache[key] = {"z_chunk": best_z, "tile_rows": best_r, "ms": ms}
-    save_cache(cache)
+    save_entry(key, cache[key])
     batch.set_pencil_length(best_z, best_r)
     batch.set_primitives(prims)
     batch.set_clocks(0.0, 0)

@@ -84,3 +84,23 @@ class FluidBatch:
             self.close()
         except Exception:  # noqa: BLE001 -- interpreter shutdown
             pass
+
+
+def shard_bricks(configs, world, rank):
+    """The bricks that rank `rank` of `world` advances when a set of
+    independent bricks is split over GPUs, one rank per GPU, as the
+    reference gives each brick to its own program or rank.  The bricks are
+    taken in decreasing order of proper cells (ties by index), and each goes
+    to the rank with the fewest cells so far (ties to the lower rank).  Every
+    rank computes the same split from the same list, so the split needs no
+    collective.  The indices come back in increasing order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank %r of a world of %r" % (rank, world))
+    cells = [int(c.n_proper) for c in configs]
+    load = [0] * world
+    owner = [0] * len(cells)
+    for i in sorted(range(len(cells)), key=lambda j: (-cells[j], j)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += cells[i]
+    return [i for i in range(len(cells)) if owner[i] == rank]

@@ -145,14 +145,17 @@ def rayleigh_taylor(shape=(384, 384, 768), seed=20261206, g=0.1, riemann_solver=
 
 
 def random_bricks(count=512, seed=20261203, lo=16, hi=96, riemann_solver="HLL",
-                  courant=0.8, n_ramp_cycles=1):
+                  courant=0.8, n_ramp_cycles=1, only=None):
     """Independent bricks with seeded sizes and two-state Riemann problems:
     per-axis edges U{lo..hi}; (rho, p) log-uniform in [0.1, 10]; velocity
     components U[-1, 1]; a diaphragm through a uniform point of the unit cube
-    with a normal uniform on the sphere."""
+    with a normal uniform on the sphere.  only: the indices whose primitive
+    arrays are built (the others come as (config, None)); the draws are the
+    same whatever it holds, so a rank of a sharded run gets its bricks exactly
+    as the whole set has them."""
     rng = np.random.default_rng(seed)
     out = []
-    for _ in range(count):
+    for i in range(count):
         n = tuple(int(v) for v in rng.integers(lo, hi + 1, size=3))
         cfg = FluidConfig(n_cells=n, boundary=(("OUTFLOW", "OUTFLOW"),) * 3,
                           riemann_solver=riemann_solver, courant_factor=courant,
@@ -163,7 +166,9 @@ def random_bricks(count=512, seed=20261203, lo=16, hi=96, riemann_solver="HLL",
         point = rng.uniform(0.0, 1.0, size=3)
         normal = rng.normal(size=3)
         normal = normal / np.linalg.norm(normal)
-        prim = riemann(cfg, rho_l, p_l, v_l, rho_r, p_r, v_r, point, normal)
+        prim = None
+        if only is None or i in only:
+            prim = riemann(cfg, rho_l, p_l, v_l, rho_r, p_r, v_r, point, normal)
         out.append((cfg, prim))
     return out
 
