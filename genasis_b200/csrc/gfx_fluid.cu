@@ -154,6 +154,73 @@ int num_sms() {
   return g_num_sms[dev];
 }
 
+// The cycles of an evolve after its first, replayed from the cycle's graph
+// in chunks of kChunkCycles with up to kChunksInFlight chunks ahead of the
+// host.  After enqueuing chunk j the host waits for the clock copied after
+// chunk j - (kChunksInFlight - 1), so the device keeps the chunks between
+// queued: a host thread that is off its core for less than their device time
+// (a CPU quota, a busy host) leaves no gap on the device.  The events block
+// instead of spinning, leaving the host's cores to others while the host
+// waits.  Chunks enqueued after the finish run as no-ops (the kernels test
+// the clock's done flag).
+constexpr int kChunksInFlight = 4;
+constexpr int kChunkCycles = 8;
+
+struct ChunkRing {
+  Clock* host = nullptr;                  // [kChunksInFlight] pinned copies of the clock
+  cudaEvent_t ev[kChunksInFlight] = {};   // after each copy
+};
+
+int ring_init(ChunkRing& R) {
+  if (R.host) return GFX_OK;
+  for (int j = 0; j < kChunksInFlight; ++j) {
+    if (R.ev[j]) continue;
+    const cudaError_t e =
+        cudaEventCreateWithFlags(&R.ev[j], cudaEventDisableTiming | cudaEventBlockingSync);
+    if (e != cudaSuccess) {
+      R.ev[j] = nullptr;
+      return fail(GFX_ERR_CUDA, "event of the evolve clock: %s", cudaGetErrorString(e));
+    }
+  }
+  if (cudaMallocHost(&R.host, kChunksInFlight * sizeof(Clock)) != cudaSuccess) {
+    R.host = nullptr;
+    return fail(GFX_ERR_NO_MEMORY, "cudaMallocHost of the evolve clock");
+  }
+  return GFX_OK;
+}
+
+void ring_free(ChunkRing& R) {
+  for (int j = 0; j < kChunksInFlight; ++j)
+    if (R.ev[j]) cudaEventDestroy(R.ev[j]);
+  if (R.host) cudaFreeHost(R.host);
+  R = ChunkRing{};
+}
+
+// Replays `graph` on s from cycle done_cycles to n_cycles_max (the evolve's
+// first cycle ran eagerly), reading the device clock dc between chunks, and
+// adds the kernels it launches to *launches.
+int ring_run(ChunkRing& R, cudaGraphExec_t graph, long long graph_kernels, long long* launches,
+             const Clock* dc, int done_cycles, int n_cycles_max, cudaStream_t s) {
+  long long j = 0;  // chunks enqueued
+  while (done_cycles < n_cycles_max) {
+    const int slot = (int)(j % kChunksInFlight);
+    const int nrep = std::min(kChunkCycles, n_cycles_max - done_cycles);
+    for (int r = 0; r < nrep; ++r) CUDA_TRY(cudaGraphLaunch(graph, s));
+    *launches += (long long)nrep * graph_kernels;
+    done_cycles += nrep;
+    CUDA_TRY(cudaMemcpyAsync(R.host + slot, dc, sizeof(Clock), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(R.ev[slot], s));
+    const long long w = j - (kChunksInFlight - 1);  // the chunk the host waits for
+    ++j;
+    if (w >= 0) {
+      const int ws = (int)(w % kChunksInFlight);
+      CUDA_TRY(cudaEventSynchronize(R.ev[ws]));
+      if (R.host[ws].done) break;
+    }
+  }
+  return GFX_OK;
+}
+
 }  // namespace
 
 // z slabs of the pipelined gfx_fluid_step_host
@@ -174,8 +241,7 @@ struct gfx_fluid {
   unsigned long long* tsi_bits = nullptr;  // [1]
   int* counters = nullptr;                 // [4]
   Clock* clock = nullptr;                  // evolve clock
-  Clock* clock_host = nullptr;             // [2] pinned copies read between chunks
-  cudaEvent_t chunk_ev[2] = {};            // after each copy
+  ChunkRing ring;                          // the evolve's clock copies between chunks
   cudaEvent_t evolve_ev[2] = {};           // gfx_fluid_evolve_timed: around its work
   double* dt_slot = nullptr;               // dt of gfx_fluid_step
   WorkItem* items = nullptr;
@@ -1016,11 +1082,9 @@ int gfx_fluid_destroy(gfx_fluid* h) {
     if (h->ev_out[j]) cudaEventDestroy(h->ev_out[j]);
   }
   if (h->ev_end) cudaEventDestroy(h->ev_end);
-  for (int j = 0; j < 2; ++j) {
-    if (h->chunk_ev[j]) cudaEventDestroy(h->chunk_ev[j]);
+  for (int j = 0; j < 2; ++j)
     if (h->evolve_ev[j]) cudaEventDestroy(h->evolve_ev[j]);
-  }
-  if (h->clock_host) cudaFreeHost(h->clock_host);
+  ring_free(h->ring);
   if (h->copy_in) cudaStreamDestroy(h->copy_in);
   if (h->copy_out) cudaStreamDestroy(h->copy_out);
   if (h->host_stream) cudaStreamDestroy(h->host_stream);
@@ -1289,37 +1353,11 @@ int evolve_impl(gfx_fluid* h, double* U, double time, int i_cycle, double finish
         return fail(GFX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
       h->graph_U = U;
     }
-    // chunks of cycles, two in flight: after enqueuing chunk j the host
-    // waits for the clock read after chunk j - 1, so the device runs chunk j
-    // while the host decides (a host thread that is slow to wake leaves no
-    // gap on the device).  A chunk enqueued after the finish runs as no-ops
-    // (the kernels test the clock's done flag).
-    if (!h->clock_host) {
-      if (cudaMallocHost(&h->clock_host, 2 * sizeof(Clock)) != cudaSuccess) {
-        h->clock_host = nullptr;
-        return fail(GFX_ERR_NO_MEMORY, "cudaMallocHost of the evolve clock");
-      }
-      for (int j = 0; j < 2; ++j)
-        CUDA_TRY(cudaEventCreateWithFlags(&h->chunk_ev[j], cudaEventDisableTiming));
-    }
-    int done_cycles = 1, slot = 0;
-    bool pending = false;
-    const int chunk = 8;
-    while (done_cycles < n_cycles_max) {
-      const int nrep = std::min(chunk, n_cycles_max - done_cycles);
-      for (int r = 0; r < nrep; ++r) CUDA_TRY(cudaGraphLaunch(h->graph, s));
-      h->launches += (long long)nrep * h->graph_kernels;
-      done_cycles += nrep;
-      CUDA_TRY(cudaMemcpyAsync(h->clock_host + slot, dc, sizeof(Clock), cudaMemcpyDeviceToHost,
-                               s));
-      CUDA_TRY(cudaEventRecord(h->chunk_ev[slot], s));
-      if (pending) {
-        CUDA_TRY(cudaEventSynchronize(h->chunk_ev[slot ^ 1]));
-        if (h->clock_host[slot ^ 1].done) break;
-      }
-      pending = true;
-      slot ^= 1;
-    }
+    // the remaining cycles in chunks, several in flight (ChunkRing)
+    if (int rc3 = ring_init(h->ring)) return rc3;
+    if (int rc3 = ring_run(h->ring, h->graph, h->graph_kernels, &h->launches, dc, 1,
+                           n_cycles_max, s))
+      return rc3;
   }
   if (ev) CUDA_TRY(cudaEventRecord(ev[1], s));
   CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
@@ -2283,8 +2321,7 @@ struct gfx_fluid_chart {
   unsigned long long* tsi_bits = nullptr;  // [1]
   Clock* clock = nullptr;                  // [2]: the chart's clock, a scratch clock
   int* counters = nullptr;                 // [4]
-  Clock* clock_host = nullptr;             // [2] pinned
-  cudaEvent_t chunk_ev[2] = {};
+  ChunkRing ring;                          // the evolve's clock copies between chunks
   int features = FEAT_ZERO;
   bool prims_pending = false;  // the kept primitives are the state (after from_primitive)
   bool wn_valid = false;       // the primitives the last stage 2 stored are the state's
@@ -2518,9 +2555,7 @@ int gfx_fluid_chart_destroy(gfx_fluid_chart* C) {
   cudaFree(C->tsi_bits);
   cudaFree(C->clock);
   cudaFree(C->counters);
-  for (int j = 0; j < 2; ++j)
-    if (C->chunk_ev[j]) cudaEventDestroy(C->chunk_ev[j]);
-  if (C->clock_host) cudaFreeHost(C->clock_host);
+  ring_free(C->ring);
   delete C;
   return GFX_OK;
 }
@@ -2738,33 +2773,11 @@ int gfx_fluid_chart_evolve(gfx_fluid_chart* C, double time, int i_cycle, double 
       if (ce != cudaSuccess)
         return fail(GFX_ERR_CUDA, "chart graph instantiate: %s", cudaGetErrorString(ce));
     }
-    if (!C->clock_host) {
-      if (cudaMallocHost(&C->clock_host, 2 * sizeof(Clock)) != cudaSuccess) {
-        C->clock_host = nullptr;
-        return fail(GFX_ERR_NO_MEMORY, "cudaMallocHost of the chart clock");
-      }
-      for (int j = 0; j < 2; ++j)
-        CUDA_TRY(cudaEventCreateWithFlags(&C->chunk_ev[j], cudaEventDisableTiming));
-    }
-    // chunks of cycles, two in flight (as gfx_fluid_evolve)
-    int done_cycles = 1, slot = 0;
-    bool pending = false;
-    const int chunk = 8;
-    while (done_cycles < n_cycles_max) {
-      const int nrep = std::min(chunk, n_cycles_max - done_cycles);
-      for (int r = 0; r < nrep; ++r) CUDA_TRY(cudaGraphLaunch(C->graph, s));
-      C->launches += (long long)nrep * C->graph_kernels;
-      done_cycles += nrep;
-      CUDA_TRY(cudaMemcpyAsync(C->clock_host + slot, dc, sizeof(Clock), cudaMemcpyDeviceToHost,
-                               s));
-      CUDA_TRY(cudaEventRecord(C->chunk_ev[slot], s));
-      if (pending) {
-        CUDA_TRY(cudaEventSynchronize(C->chunk_ev[slot ^ 1]));
-        if (C->clock_host[slot ^ 1].done) break;
-      }
-      pending = true;
-      slot ^= 1;
-    }
+    // the remaining cycles in chunks, several in flight (ChunkRing)
+    if (int rc3 = ring_init(C->ring)) return rc3;
+    if (int rc3 = ring_run(C->ring, C->graph, C->graph_kernels, &C->launches, dc, 1,
+                           n_cycles_max, s))
+      return rc3;
   }
   CUDA_TRY(cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));

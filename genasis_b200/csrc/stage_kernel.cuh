@@ -940,7 +940,34 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             (gx + 2) + (long long)B.m[0] * ((gy + 2) + (long long)B.m[1] * (k + 2));
         const long long cidx = gx + (long long)n0 * (gy + (long long)n1 * k);
         // dU += dT (A_I F_I(i) - A_I F_I(i+1)) / V per direction
-        // (IncrementDivergence_FV__Kernel.f90:729-748), all quotients at once
+        // (IncrementDivergence_FV__Kernel.f90:729-748)
+#if GFX_FAST_MATH
+        // the speed build: dT A_d / V once per direction, times the
+        // direction's flux difference, the three terms summed with fused
+        // multiply-adds (a few ulps of the increment from the reference's
+        // order of operations, which the exact build keeps)
+        double Kc[NF];
+        {
+          const double cx = dt * ax * rvol, cy = dt * ay * rvol, cz = dt * az * rvol;
+#pragma unroll
+          for (int u = 0; u < NF; ++u) {
+            const double fx = fxs[(u * TY + ty) * (TX + 1) + tx] -
+                              fxs[(u * TY + ty) * (TX + 1) + tx + 1];
+            const double fy = fys[(u * (TY + 1) + ty) * TX + tx] -
+                              fys[(u * (TY + 1) + ty + 1) * TX + tx];
+            const double fz = zfs[u * NT + tid] - zfn[u];
+            Kc[u] = cx * fx + cy * fy + cz * fz;
+          }
+          if (MODE == MODE_INCREMENT) {
+#pragma unroll
+            for (int u = 0; u < NF; ++u) {
+              double* kp = B.K + (long long)u * B.nV + gidx;
+              *kp = *kp + Kc[u];
+            }
+          }
+        }
+#else
+        // all quotients at once
         double nx_[NF], ny_[NF], nz_[NF], qx[NF], qy[NF], qz[NF];
         bool ok = true;
 #pragma unroll
@@ -974,6 +1001,7 @@ __global__ void __launch_bounds__(TX * TYt, tile_min_ctas(TYt))
             Kc[u] = qx[u] + qy[u] + qz[u];
           }
         }
+#endif
         if (MODE != MODE_INCREMENT) {
           const double N = full[c_off], V1 = full[FS + c_off], V2 = full[2 * FS + c_off],
                        V3 = full[3 * FS + c_off], E = full[4 * FS + c_off];
