@@ -35,10 +35,11 @@ extern "C" {
 
 // Best of `reps` launches of `iters` steps per chain: FP64 operations per
 // second (a fused multiply-add counts two) into *flops, the launch's
-// milliseconds into *ms.  4096 steps take about 0.55 ms on a B200.  0 on
+// milliseconds into *ms.  4096 steps take about 0.55 ms on a B200; a launch
+// is held under about half a second (iters <= 2^22), reps to 10000.  0 on
 // success, -1 on a bad argument, -2 on a CUDA error.
 int gfx_probe_fp64_chains(int reps, int iters, double* flops, double* ms) {
-  if (reps < 1 || iters < 1 || !flops || !ms) return -1;
+  if (reps < 1 || reps > 10000 || iters < 1 || iters > (1 << 22) || !flops || !ms) return -1;
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -2;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -2;

@@ -154,6 +154,17 @@ int num_sms() {
   return g_num_sms[dev];
 }
 
+// cudaMalloc that leaves *p null when it fails (and clears the error it
+// records), so that a handle whose lazy allocation failed allocates again on
+// its next call instead of keeping a pointer it does not own.
+template <class T>
+bool dev_alloc(T** p, size_t bytes) {
+  if (cudaMalloc(p, bytes) == cudaSuccess) return true;
+  *p = nullptr;
+  cudaGetLastError();
+  return false;
+}
+
 // The cycles of an evolve after its first, replayed from the cycle's graph
 // in chunks of kChunkCycles with up to kChunksInFlight chunks ahead of the
 // host.  After enqueuing chunk j the host waits for the clock copied after
@@ -782,7 +793,7 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
     cudaFree(h->host_items);
     h->host_items = nullptr;
     h->host_chunk = 0;
-    if (cudaMalloc(&h->host_items, items.size() * sizeof(WorkItem)) != cudaSuccess)
+    if (!dev_alloc(&h->host_items, items.size() * sizeof(WorkItem)))
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc slab work items");
     CUDA_TRY(cudaMemcpy(h->host_items, items.data(), items.size() * sizeof(WorkItem),
                         cudaMemcpyHostToDevice));
@@ -808,8 +819,7 @@ int step_host_pipelined(gfx_fluid* h, double* U_host, double dt, double* fluence
     if (!h->ev_out[j]) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_out[j], cudaEventDisableTiming));
   }
   if (!h->ev_end) CUDA_TRY(cudaEventCreateWithFlags(&h->ev_end, cudaEventDisableTiming));
-  if (!h->slab_counters &&
-      cudaMalloc(&h->slab_counters, 2 * kMaxSlabs * sizeof(int)) != cudaSuccess)
+  if (!h->slab_counters && !dev_alloc(&h->slab_counters, 2 * kMaxSlabs * sizeof(int)))
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc slab counters");
   cudaStream_t sc = h->host_stream, si = h->copy_in, so = h->copy_out;
   double* U = h->U_stage;
@@ -1213,7 +1223,7 @@ int gfx_fluid_step_sources(gfx_fluid* h, double* U, double dt, double* fluence,
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_sources")) return rc0;
   if (!h || !U || !sources) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
-  if (!h->Ksrc && cudaMalloc(&h->Ksrc, 6 * (size_t)h->box.nV * sizeof(double)) != cudaSuccess)
+  if (!h->Ksrc && !dev_alloc(&h->Ksrc, 6 * (size_t)h->box.nV * sizeof(double)))
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc sources scratch");
   cudaStream_t s = (cudaStream_t)stream;
   set_scalar_kernel<<<1, 1, 0, s>>>(h->dt_slot, dt);
@@ -1234,10 +1244,8 @@ int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence
   if (!h || !U_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   const size_t bytes = 6 * (size_t)h->box.nV * sizeof(double);
   if (!h->host_stream) CUDA_TRY(cudaStreamCreateWithFlags(&h->host_stream, cudaStreamNonBlocking));
-  if (!h->U_stage) {
-    if (cudaMalloc(&h->U_stage, bytes + 36 * h->face_size * sizeof(double)) != cudaSuccess)
-      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc host-step staging");
-  }
+  if (!h->U_stage && !dev_alloc(&h->U_stage, bytes + 36 * h->face_size * sizeof(double)))
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc host-step staging");
   int prc = step_host_pipelined(h, U_host, dt, fluence_host);
   if (prc != GFX_ERR_UNSUPPORTED) return prc;
   cudaStream_t s = h->host_stream;
@@ -1691,8 +1699,7 @@ int gfx_fluid_batch_kernel_launches(const gfx_fluid_batch* B, long long* count) 
 int gfx_fluid_check_state(gfx_fluid* h, const double* U, void* stream) {
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
-  if (!h->state_counts &&
-      cudaMalloc(&h->state_counts, 2 * sizeof(unsigned long long)) != cudaSuccess)
+  if (!h->state_counts && !dev_alloc(&h->state_counts, 2 * sizeof(unsigned long long)))
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc state counters");
   CUDA_TRY(cudaMemsetAsync(h->state_counts, 0, 2 * sizeof(unsigned long long), s));
   check_state_kernel<<<grid_for(h->box.nP, 256), 256, 0, s>>>(h->box, h->ph, U,
@@ -1723,7 +1730,7 @@ int gfx_fluid_totals(gfx_fluid* h, const double* U, double* totals, void* stream
   cudaStream_t s = (cudaStream_t)stream;
   const int blocks = 4 * num_sms();
   const long long chunk = (h->box.nP + blocks - 1) / blocks;
-  if (!h->partials && cudaMalloc(&h->partials, 6 * blocks * sizeof(double)) != cudaSuccess)
+  if (!h->partials && !dev_alloc(&h->partials, 6 * blocks * sizeof(double)))
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc tally partials");
   totals_kernel<<<blocks, 256, 0, s>>>(h->box, U, h->dgeo[0], h->dgeo[1], h->dgeo[2], chunk,
                                        h->partials);
@@ -2146,16 +2153,14 @@ int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const dou
   if (b.nP >= (1LL << 31))
     return fail(GFX_ERR_UNSUPPORTED, "adjoint: %lld proper cells (at most 2^31 - 1)", b.nP);
   const size_t nP = (size_t)b.nP, nV = (size_t)b.nV;
-  if (!h->adj) {
-    if (cudaMalloc(&h->adj, 20 * nP * sizeof(double)) != cudaSuccess)
-      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
-    if (cudaMalloc(&h->adj_flags, nP) != cudaSuccess)
-      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
-  }
-  if (!U_np1 && !h->adj_U) {
-    if (cudaMalloc(&h->adj_U, 6 * nV * sizeof(double)) != cudaSuccess)
-      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint state");
-  }
+  // each buffer on its own: a failed allocation leaves its pointer null and
+  // the next call tries it again
+  if (!h->adj && !dev_alloc(&h->adj, 20 * nP * sizeof(double)))
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
+  if (!h->adj_flags && !dev_alloc(&h->adj_flags, nP))
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
+  if (!U_np1 && !h->adj_U && !dev_alloc(&h->adj_U, 6 * nV * sizeof(double)))
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint state");
   double* W0 = h->adj;
   double* lamZ = W0 + 5 * nP;
   double* lamW = lamZ + 5 * nP;

@@ -55,6 +55,7 @@ def test_fp64_probe_exports_and_refuses_bad_arguments():
                    ctypes.POINTER(ctypes.c_double)]
     assert fn(0, 4096, ctypes.byref(f), ctypes.byref(ms)) == -1
     assert fn(1, 0, ctypes.byref(f), ctypes.byref(ms)) == -1
+    assert fn(1, (1 << 22) + 1, ctypes.byref(f), ctypes.byref(ms)) == -1
     assert fn(1, 4096, None, ctypes.byref(ms)) == -1
     assert hasattr(so, "gfx_probe_fp64")
 
