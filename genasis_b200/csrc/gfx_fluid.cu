@@ -1007,7 +1007,7 @@ int create_handle(const gfx_fluid_config* cfg, const HostAxis* axes, gfx_fluid**
   // geometry arena: 9 tables per axis, then the PG_N parabolic ones, each m + 1 long
   size_t geo_len = 0;
   for (int d = 0; d < 3; ++d) geo_len += (9 + PG_N) * (size_t)(b.m[d] + 1);
-  if (cudaMalloc(&h->geo, geo_len * sizeof(double)) != cudaSuccess)
+  if (!dev_alloc(&h->geo, geo_len * sizeof(double)))
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc geometry"));
   {
     std::vector<double> host(geo_len, 0.0);
@@ -1035,21 +1035,21 @@ int create_handle(const gfx_fluid_config* cfg, const HostAxis* axes, gfx_fluid**
       return cleanup(fail(GFX_ERR_CUDA, "copy geometry tables"));
   }
   const size_t nP = (size_t)b.nP;
-  if (cudaMalloc(&h->Yp, 5 * nP * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->H, 5 * nP * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->Pst, 5 * nP * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->df, nP) != cudaSuccess ||
-      cudaMalloc(&h->tsi_bits, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&h->counters, 4 * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&h->clock, 2 * sizeof(Clock)) != cudaSuccess ||
-      cudaMalloc(&h->dt_slot, sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->wn, 5 * nP * sizeof(double)) != cudaSuccess)
+  if (!dev_alloc(&h->Yp, 5 * nP * sizeof(double)) ||
+      !dev_alloc(&h->H, 5 * nP * sizeof(double)) ||
+      !dev_alloc(&h->Pst, 5 * nP * sizeof(double)) ||
+      !dev_alloc(&h->df, nP) ||
+      !dev_alloc(&h->tsi_bits, 2 * sizeof(unsigned long long)) ||
+      !dev_alloc(&h->counters, 4 * sizeof(int)) ||
+      !dev_alloc(&h->clock, 2 * sizeof(Clock)) ||
+      !dev_alloc(&h->dt_slot, sizeof(double)) ||
+      !dev_alloc(&h->wn, 5 * nP * sizeof(double)))
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc of the stage scratch (%zu cells)", nP));
   if (cudaMemset(h->df, 0, nP) != cudaSuccess)
     return cleanup(fail(GFX_ERR_CUDA, "clear features"));
   std::vector<WorkItem> items = make_items(b.n, 0);
   h->n_items = (int)items.size();
-  if (cudaMalloc(&h->items, items.size() * sizeof(WorkItem)) != cudaSuccess)
+  if (!dev_alloc(&h->items, items.size() * sizeof(WorkItem)))
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc work items"));
   if (cudaMemcpy(h->items, items.data(), items.size() * sizeof(WorkItem),
                  cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1478,14 +1478,14 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
   B->U.assign(U, U + n);
   B->ph = handles[0]->ph;
   B->hllc = c0.riemann_solver == GFX_RIEMANN_HLLC;
-  if (cudaMalloc(&B->tsi_bits, n * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&B->clocks, n * sizeof(Clock)) != cudaSuccess ||
-      cudaMalloc(&B->counters, 4 * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&B->d1, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&B->d1p, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&B->d1w, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&B->d2, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&B->bb, n * sizeof(BatchBrick)) != cudaSuccess)
+  if (!dev_alloc(&B->tsi_bits, n * sizeof(unsigned long long)) ||
+      !dev_alloc(&B->clocks, n * sizeof(Clock)) ||
+      !dev_alloc(&B->counters, 4 * sizeof(int)) ||
+      !dev_alloc(&B->d1, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&B->d1p, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&B->d1w, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&B->d2, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&B->bb, n * sizeof(BatchBrick)))
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch tables"));
   std::vector<BrickDesc> d1(n), d1p(n), d1w(n), d2(n);
   std::vector<BatchBrick> bb(n);
@@ -1534,11 +1534,11 @@ int gfx_fluid_batch_create(int n, gfx_fluid* const* handles, double* const* U,
   std::vector<WorkItem> sorted(items.size());
   for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
   B->n_items = (int)sorted.size();
-  if (cudaMalloc(&B->items, sorted.size() * sizeof(WorkItem)) != cudaSuccess)
+  if (!dev_alloc(&B->items, sorted.size() * sizeof(WorkItem)))
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch work items"));
   if (B->hllc) {
     B->n_det_items = (int)det.size();
-    if (cudaMalloc(&B->det_items, det.size() * sizeof(DetItem)) != cudaSuccess)
+    if (!dev_alloc(&B->det_items, det.size() * sizeof(DetItem)))
       return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc batch feature tiles"));
     if (cudaMemcpy(B->det_items, det.data(), det.size() * sizeof(DetItem),
                    cudaMemcpyHostToDevice) != cudaSuccess)
@@ -2234,13 +2234,13 @@ int gfx_fluid_step_branches(gfx_fluid* h, const double* U_n, double dt, int dete
     return fail(GFX_ERR_UNSUPPORTED, "branch signature: %lld proper cells", b.nP);
   const size_t nP = (size_t)b.nP;
   if (!h->adj) {
-    if (cudaMalloc(&h->adj, 20 * nP * sizeof(double)) != cudaSuccess)
+    if (!dev_alloc(&h->adj, 20 * nP * sizeof(double)))
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
-    if (cudaMalloc(&h->adj_flags, nP) != cudaSuccess)
+    if (!dev_alloc(&h->adj_flags, nP))
       return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
   }
   if (!h->branch_buf &&
-      cudaMalloc(&h->branch_buf, (2 + BR_KINDS) * sizeof(unsigned long long)) != cudaSuccess)
+      !dev_alloc(&h->branch_buf, (2 + BR_KINDS) * sizeof(unsigned long long)))
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc branch signature");
   double* W0 = h->adj;
   uint8_t* df = h->adj_flags;
@@ -2529,15 +2529,15 @@ int gfx_fluid_chart_create(const gfx_fluid_config* cfg, const int n_bricks[3],
   for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
   C->n_items = (int)sorted.size();
   const size_t n = (size_t)C->n;
-  if (cudaMalloc(&C->d1, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&C->d1p, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&C->d1w, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&C->d2, n * sizeof(BrickDesc)) != cudaSuccess ||
-      cudaMalloc(&C->cb, n * sizeof(ChartBrick)) != cudaSuccess ||
-      cudaMalloc(&C->items, sorted.size() * sizeof(WorkItem)) != cudaSuccess ||
-      cudaMalloc(&C->tsi_bits, sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&C->clock, 2 * sizeof(Clock)) != cudaSuccess ||
-      cudaMalloc(&C->counters, 4 * sizeof(int)) != cudaSuccess)
+  if (!dev_alloc(&C->d1, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&C->d1p, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&C->d1w, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&C->d2, n * sizeof(BrickDesc)) ||
+      !dev_alloc(&C->cb, n * sizeof(ChartBrick)) ||
+      !dev_alloc(&C->items, sorted.size() * sizeof(WorkItem)) ||
+      !dev_alloc(&C->tsi_bits, sizeof(unsigned long long)) ||
+      !dev_alloc(&C->clock, 2 * sizeof(Clock)) ||
+      !dev_alloc(&C->counters, 4 * sizeof(int)))
     return cleanup(fail(GFX_ERR_NO_MEMORY, "cudaMalloc chart tables"));
   if (cudaMemcpy(C->items, sorted.data(), sorted.size() * sizeof(WorkItem),
                  cudaMemcpyHostToDevice) != cudaSuccess ||
