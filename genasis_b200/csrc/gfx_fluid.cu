@@ -154,11 +154,19 @@ int num_sms() {
   return g_num_sms[dev];
 }
 
+// gfx_fluid_debug_fail_allocation: the allocations of this thread still to
+// pass before the one that fails (-1: none fails)
+thread_local int g_fail_alloc = -1;
+
 // cudaMalloc that leaves *p null when it fails (and clears the error it
 // records), so that a handle whose lazy allocation failed allocates again on
 // its next call instead of keeping a pointer it does not own.
 template <class T>
 bool dev_alloc(T** p, size_t bytes) {
+  if (g_fail_alloc >= 0 && g_fail_alloc-- == 0) {
+    *p = nullptr;
+    return false;
+  }
   if (cudaMalloc(p, bytes) == cudaSuccess) return true;
   *p = nullptr;
   cudaGetLastError();
@@ -1790,6 +1798,11 @@ int gfx_fluid_last_error(char* buf, size_t len) {
   return GFX_OK;
 }
 
+int gfx_fluid_debug_fail_allocation(int nth) {
+  g_fail_alloc = nth < 0 ? -1 : nth;
+  return GFX_OK;
+}
+
 }  // extern "C"
 
 // ---- One RK2 step that allocates nothing ----------------------------------
@@ -2233,12 +2246,11 @@ int gfx_fluid_step_branches(gfx_fluid* h, const double* U_n, double dt, int dete
   if (b.nP >= (1LL << 31))
     return fail(GFX_ERR_UNSUPPORTED, "branch signature: %lld proper cells", b.nP);
   const size_t nP = (size_t)b.nP;
-  if (!h->adj) {
-    if (!dev_alloc(&h->adj, 20 * nP * sizeof(double)))
-      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
-    if (!dev_alloc(&h->adj_flags, nP))
-      return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
-  }
+  // each buffer on its own (as in gfx_fluid_step_adjoint)
+  if (!h->adj && !dev_alloc(&h->adj, 20 * nP * sizeof(double)))
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint workspace (%zu cells)", nP);
+  if (!h->adj_flags && !dev_alloc(&h->adj_flags, nP))
+    return fail(GFX_ERR_NO_MEMORY, "cudaMalloc adjoint flags");
   if (!h->branch_buf &&
       !dev_alloc(&h->branch_buf, (2 + BR_KINDS) * sizeof(unsigned long long)))
     return fail(GFX_ERR_NO_MEMORY, "cudaMalloc branch signature");

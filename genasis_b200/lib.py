@@ -80,6 +80,7 @@ SIGNATURES = {
     "gfx_fluid_chart_evolve": [P, D, I, D, I, ctypes.POINTER(D), ctypes.POINTER(I), P],
     "gfx_fluid_chart_kernel_launches": [P, ctypes.POINTER(ctypes.c_longlong)],
     "gfx_fluid_last_error": [ctypes.c_char_p, SZ],
+    "gfx_fluid_debug_fail_allocation": [I],
 }
 
 _libs = {}

@@ -371,6 +371,15 @@ int gfx_fluid_set_tuning(gfx_fluid *h, int z_chunk, int adjoint_segment, int til
 
 int gfx_fluid_last_error(char *buf, size_t len);
 
+/* Fault injection for tests, on the host: the nth device allocation that the
+ * library makes on the calling thread from now on (0 = the next one) fails as
+ * if the device were out of memory, once; a negative nth turns it off.  The
+ * call that meets it returns GFX_ERR_NO_MEMORY, frees what it had allocated
+ * (a create) or keeps the buffers it had (a handle's lazily allocated
+ * workspaces), and the next call allocates again.  The reference aborts on
+ * an allocation failure and has no counterpart. */
+int gfx_fluid_debug_fail_allocation(int nth);
+
 #ifdef __cplusplus
 }
 #endif

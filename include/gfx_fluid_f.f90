@@ -70,7 +70,8 @@ module GFX_Fluid_C
     gfx_fluid_chart_n_bricks, gfx_fluid_chart_brick, gfx_fluid_chart_bind, &
     gfx_fluid_chart_from_primitive, gfx_fluid_chart_set_conserved, &
     gfx_fluid_chart_timestep, gfx_fluid_chart_step, gfx_fluid_chart_evolve, &
-    gfx_fluid_chart_kernel_launches, gfx_fluid_last_error
+    gfx_fluid_chart_kernel_launches, gfx_fluid_last_error, &
+    gfx_fluid_debug_fail_allocation
 
   interface
 
@@ -423,6 +424,12 @@ module GFX_Fluid_C
       character ( kind = c_char ), intent ( out ) :: Buffer ( * )
       integer ( c_size_t ), value :: Length
     end function gfx_fluid_last_error
+
+    integer ( c_int ) function gfx_fluid_debug_fail_allocation ( nth ) &
+      bind ( c, name = 'gfx_fluid_debug_fail_allocation' )
+      import
+      integer ( c_int ), value :: nth
+    end function gfx_fluid_debug_fail_allocation
 
   end interface
 
