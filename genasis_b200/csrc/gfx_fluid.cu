@@ -6,6 +6,7 @@
 // state Y and the partial solution U + K1/2, both without ghosts), the shock
 // feature bits and a device-side clock for the evolve loop.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -26,6 +27,17 @@ using namespace gfx;
 namespace {
 
 thread_local std::string g_last_error;
+
+// A named range of the calling thread for profilers (NVTX, header-only;
+// without a tool attached a push is a call to a no-op).  The names are the
+// reference's routines, so a profile of the library's launches reads by the
+// reference's phases.
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -652,6 +664,7 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
     CUDA_TRY(cudaMemsetAsync(fluence, 0, sizeof(double) * 36 * h->face_size, s));
   if (ev) CUDA_TRY(cudaEventRecord(ev[0], s));
   if (hllc && detect) {
+    Range r("FluidFeatures_P % Detect");
     int rc = from_wn ? run_features_wn(h, U, s) : run_features(h, U, nullptr, s);
     if (rc) return rc;
   }
@@ -664,8 +677,11 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
     if (rc) return rc;
   }
   BrickDesc d1 = make_desc(h, U, nullptr, nullptr, P1, df, fluence, dt_ptr, 0.5, skip);
-  CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, hllc, grav, d1, nullptr, h->items, h->n_items,
-                        h->counters, h->ph, s));
+  {
+    Range r("Step_RK_C_ASC % ComputeStage 1");
+    CUDA_TRY(launch_stage(MODE_STAGE1, in_prim, hllc, grav, d1, nullptr, h->items, h->n_items,
+                          h->counters, h->ph, s));
+  }
   if (ev) CUDA_TRY(cudaEventRecord(ev[2], s));
   if (sources) {
     int rc = enqueue_sources(h, U, h->Yp, true, df, dt_ptr, 1, sources, h->counters + 3, s);
@@ -673,8 +689,11 @@ int enqueue_step(gfx_fluid* h, double* U, const double* dt_ptr, const int* skip,
   }
   BrickDesc d2 = make_desc(h, U, U, nullptr, h->Yp, df, fluence, dt_ptr, 0.5, skip);
   d2.wn = h->wn;
-  CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
-                        h->counters + 1, h->ph, s));
+  {
+    Range r("Step_RK_C_ASC % ComputeStage 2");
+    CUDA_TRY(launch_stage(MODE_STAGE2, true, hllc, grav, d2, nullptr, h->items, h->n_items,
+                          h->counters + 1, h->ph, s));
+  }
   if (ev) CUDA_TRY(cudaEventRecord(ev[3], s));
   const int blk = 256;
   const Box& bx = h->box;
@@ -1132,6 +1151,7 @@ int gfx_fluid_geometry(const gfx_fluid* h, int axis, double* c, double* wl, doub
 }
 
 int gfx_fluid_from_primitive(gfx_fluid* h, const double* prim, double* U, void* stream) {
+  Range range_("Fluid_P_I % ComputeFromPrimitive");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_from_primitive")) return rc0;
   if (!h || !prim || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1187,6 +1207,7 @@ int gfx_fluid_get_features(gfx_fluid* h, uint8_t* flags, void* stream) {
 
 int gfx_fluid_increment(gfx_fluid* h, const double* U, double* K, double dt, double weight,
                         double* fluence, void* stream) {
+  Range range_("IncrementDivergence_FV % Compute");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_increment")) return rc0;
   if (!h || !U || !K) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1209,6 +1230,7 @@ int gfx_fluid_increment(gfx_fluid* h, const double* U, double* K, double dt, dou
 }
 
 int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* stream) {
+  Range range_("Step_RK_C_ASC % Compute");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
@@ -1228,6 +1250,7 @@ int gfx_fluid_step(gfx_fluid* h, double* U, double dt, double* fluence, void* st
 
 int gfx_fluid_step_sources(gfx_fluid* h, double* U, double dt, double* fluence,
                            double* sources, void* stream) {
+  Range range_("Step_RK_C_ASC % Compute (Sources records)");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_sources")) return rc0;
   if (!h || !U || !sources) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
@@ -1248,6 +1271,7 @@ int gfx_fluid_step_sources(gfx_fluid* h, double* U, double dt, double* fluence,
 }
 
 int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence_host) {
+  Range range_("Step_RK_C_ASC % Compute (host state)");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_host")) return rc0;
   if (!h || !U_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   const size_t bytes = 6 * (size_t)h->box.nV * sizeof(double);
@@ -1273,6 +1297,7 @@ int gfx_fluid_step_host(gfx_fluid* h, double* U_host, double dt, double* fluence
 
 int gfx_fluid_timestep(gfx_fluid* h, const double* U, int i_cycle, double* dt_host,
                        void* stream) {
+  Range range_("Integrator_C_PS % ComputeTimeStepLocal");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_timestep")) return rc0;
   if (!h || !U || !dt_host) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1308,6 +1333,7 @@ namespace {
 int evolve_impl(gfx_fluid* h, double* U, double time, int i_cycle, double finish_time,
                 int n_cycles_max, double* time_out, int* i_cycle_out, cudaStream_t s,
                 cudaEvent_t* ev) {
+  Range range_("Integrator % Evolve");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_evolve")) return rc0;
   if (!h || !U) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (n_cycles_max < 0) return fail(GFX_ERR_ARGUMENT, "n_cycles_max < 0");
@@ -1615,6 +1641,7 @@ __global__ void batch_arm_clocks_kernel(Clock* clk, int n, double finish, int n_
 }
 
 int gfx_fluid_batch_evolve(gfx_fluid_batch* B, double finish_time, int n_cycles, void* stream) {
+  Range range_("Integrator % Evolve (batched bricks)");
   if (!B || n_cycles < 0) return fail(GFX_ERR_ARGUMENT, "bad batch evolve arguments");
   if (n_cycles == 0) return GFX_OK;
   cudaStream_t s = (cudaStream_t)stream;
@@ -2155,6 +2182,7 @@ extern "C" {
 int gfx_fluid_step_adjoint(gfx_fluid* h, const double* U_n, double dt, const double* lam_np1,
                            double* lam_n, const double* U_np1, int detect_features,
                            void* stream) {
+  Range range_("Step_RK_C_ASC % Compute (adjoint)");
   if (int rc0 = refuse_chart_brick(h, "gfx_fluid_step_adjoint")) return rc0;
   if (!h || !U_n || !lam_np1 || !lam_n) return fail(GFX_ERR_ARGUMENT, "NULL argument");
   if (lam_n == lam_np1) return fail(GFX_ERR_ARGUMENT, "lam_n must not alias lam_np1");
@@ -2709,6 +2737,7 @@ int gfx_fluid_chart_timestep(gfx_fluid_chart* C, int i_cycle, double* dt_host, v
 }
 
 int gfx_fluid_chart_step(gfx_fluid_chart* C, double dt, double* const* fluence, void* stream) {
+  Range range_("Step_RK_C_ASC % Compute (chart)");
   if (!C) return fail(GFX_ERR_ARGUMENT, "NULL chart");
   if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(GFX_ERR_ARGUMENT, "dt = %g", dt);
@@ -2743,6 +2772,7 @@ int gfx_fluid_chart_step(gfx_fluid_chart* C, double dt, double* const* fluence, 
 
 int gfx_fluid_chart_evolve(gfx_fluid_chart* C, double time, int i_cycle, double finish_time,
                            int n_cycles_max, double* time_out, int* i_cycle_out, void* stream) {
+  Range range_("Integrator % Evolve (chart)");
   if (!C) return fail(GFX_ERR_ARGUMENT, "NULL chart");
   if (C->U.empty()) return fail(GFX_ERR_ARGUMENT, "chart: bind the bricks' states first");
   if (n_cycles_max < 0) return fail(GFX_ERR_ARGUMENT, "n_cycles_max < 0");
