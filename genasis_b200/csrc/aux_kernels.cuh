@@ -272,13 +272,15 @@ struct DetectBrick {
     F[3] = F[2] + fs;
     F[4] = F[3] + fs;  // G (U only)
   }
-  __device__ __forceinline__ void load(int i, int j, int k, double* raw) const {
+  // starts the copies of the raw values of cell (i, j, k) into dst, dst +
+  // stride, ... (cp.async)
+  __device__ __forceinline__ void load_async(int i, int j, int k, double* dst, int stride) const {
     const int o = (i + gh) + pitch * (j + gh) + plane * (k + gh);
-    raw[0] = F[0][o];
-    raw[1] = F[1][o];
-    raw[2] = F[2][o];
-    raw[3] = F[3][o];
-    if (!PST) raw[4] = F[4][o];
+    cp_async8(dst, F[0] + o);
+    cp_async8(dst + stride, F[1] + o);
+    cp_async8(dst + 2 * stride, F[2] + o);
+    cp_async8(dst + 3 * stride, F[3] + o);
+    if (!PST) cp_async8(dst + 4 * stride, F[4] + o);
   }
   __device__ __forceinline__ uint8_t* flags(int i, int j, int k) const {
     return df + (i + n0 * (j + n1 * k));
@@ -296,8 +298,10 @@ struct DetectBrick {
 // coordinates; raw values: E, V1, V2, V3 with PST, else D, S1, S2, S3, G).
 // The tile of this block: columns i0 .. i0 + 31, rows j0 .. j0 + 7, planes
 // [kb, ke) (at most kDetKZ).  For every plane kk each thread recovers pressure and
-// velocities of its halo-tile cell (its loads for plane kk + 1 are issued
-// before the CTA synchronises), forms the cell's shock bits from the -x and
+// velocities of its halo-tile cell (the values of planes kk + 1 .. kk + D - 1
+// are on their way meanwhile: asynchronous copies into a ring of D planes in
+// shared memory, each thread reading back only its own copies, so that the
+// ring needs no barrier of its own), forms the cell's shock bits from the -x and
 // -y neighbours in shared memory and the -z neighbour kept in registers, and
 // the CTA keeps three planes of bits in a ring; the flags of plane kk - 1
 // (threads 0-255, one per tile cell) then read bits of planes kk - 2 to kk
@@ -309,9 +313,13 @@ struct DetectBrick {
 template <bool PST, class Src>
 __device__ __forceinline__ void detect_tile(const Src& src, const Phys& ph, int n0, int n1,
                                             int n2, int i0, int j0, int kb, int ke) {
-  constexpr int RX = kDetRX, NR = kDetNR;
+  constexpr int RX = kDetRX, NR = kDetNR, NT = kDetThreads;
+  // planes in flight: three of the four primitive fields; two of the five
+  // conserved ones (the static shared memory stays under 48 KB)
+  constexpr int NRAW = PST ? 4 : 5, D = PST ? 3 : 2;
   __shared__ double sP[NR], sV1[NR], sV2[NR];
   __shared__ uint8_t sS[3][NR];
+  __shared__ double sRaw[D][NRAW][NT];
   const int tid = threadIdx.x;
   const double thr = ph.shock_threshold;
   // the halo-tile cell of this thread
@@ -319,11 +327,14 @@ __device__ __forceinline__ void detect_tile(const Src& src, const Phys& ph, int 
   const int gi = i0 - 1 + rx, gj = j0 - 1 + ry;
   const bool ok = tid < NR && gi >= 0 && gj >= 0 && gi < n0 && gj < n1;
   const bool has_xm = rx >= 1 && gi >= 1, has_ym = ry >= 1 && gj >= 1;
-  double raw[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  auto fetch = [&](int kk) {
-    if (ok && kk >= 0 && kk < n2) src.load(gi, gj, kk, raw);
+  // plane kk into ring slot `slot`: one group of copies per plane, empty
+  // where there is nothing to read, so that the groups count planes
+  auto fetch = [&](int kk, int slot) {
+    if (ok && kk >= 0 && kk < n2 && kk <= ke) src.load_async(gi, gj, kk, &sRaw[slot][0][tid], NT);
+    cp_async_commit();
   };
-  fetch(kb - 1);
+#pragma unroll
+  for (int q = 0; q < D - 1; ++q) fetch(kb - 1 + q, q);
   double Pz = 0.0, Vz = 0.0;  // the plane below
   // the output cell of this thread (threads 0-255)
   const int ox = tid % kDetTX, oy = tid / kDetTX;
@@ -332,17 +343,22 @@ __device__ __forceinline__ void detect_tile(const Src& src, const Phys& ph, int 
   const bool inner_xy = i >= 1 && j >= 1 && i <= n0 - 2 && j <= n1 - 2;
   // the ring slots of planes kk, kk - 1 and kk - 2
   uint8_t *s_new = sS[0], *s_cur = sS[2], *s_old = sS[1];
-  for (int kk = kb - 1; kk <= ke; ++kk) {
+  for (int kk = kb - 1, slot = 0; kk <= ke; ++kk, slot = (slot + 1 == D) ? 0 : slot + 1) {
+    // plane kk + D - 1 into the slot of plane kk - 1 (read back in the last
+    // round); then plane kk, the oldest of the D groups in flight, has landed
+    fetch(kk + D - 1, slot == 0 ? D - 1 : slot - 1);
+    cp_async_wait_group<D - 1>();
     const bool live = ok && kk >= 0 && kk < n2;
     double P = 0.0, V1 = 0.0, V2 = 0.0, V3 = 0.0;
     if (live) {
+      const double* raw = &sRaw[slot][0][tid];
       if (PST) {
         P = ph.gm1 * raw[0];
-        V1 = raw[1];
-        V2 = raw[2];
-        V3 = raw[3];
+        V1 = raw[NT];
+        V2 = raw[2 * NT];
+        V3 = raw[3 * NT];
       } else {
-        Cons u{raw[0], raw[1], raw[2], raw[3], raw[4]};
+        Cons u{raw[0], raw[NT], raw[2 * NT], raw[3 * NT], raw[4 * NT]};
         Prim w;
         cons_to_prim_exact(u, w, ph.nmin);
         P = ph.gm1 * w.E;
@@ -351,7 +367,6 @@ __device__ __forceinline__ void detect_tile(const Src& src, const Phys& ph, int 
         V3 = w.V3;
       }
     }
-    if (kk < ke) fetch(kk + 1);
     if (tid < NR) {
       sP[tid] = P;
       sV1[tid] = V1;

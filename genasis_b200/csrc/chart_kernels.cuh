@@ -167,20 +167,22 @@ struct DetectChart {
     lk = k - bz * bn2;
     return cb[bx + nbx * (by + nby * bz)];
   }
-  __device__ __forceinline__ void load(int i, int j, int k, double* raw) const {
+  // starts the copies of the raw values of cell (i, j, k) into dst, dst +
+  // stride, ... (cp.async)
+  __device__ __forceinline__ void load_async(int i, int j, int k, double* dst, int stride) const {
     int li, lj, lk;
     const ChartBrick& B = brick(i, j, k, li, lj, lk);
     if (PST) {
       const long long nP = B.box.nP, o = li + (long long)bn0 * (lj + (long long)bn1 * lk);
-      raw[0] = B.wn[4 * nP + o];
-      raw[1] = B.wn[nP + o];
-      raw[2] = B.wn[2 * nP + o];
-      raw[3] = B.wn[3 * nP + o];
+      cp_async8(dst, B.wn + 4 * nP + o);
+      cp_async8(dst + stride, B.wn + nP + o);
+      cp_async8(dst + 2 * stride, B.wn + 2 * nP + o);
+      cp_async8(dst + 3 * stride, B.wn + 3 * nP + o);
     } else {
       const int c[3] = {li, lj, lk};
       const long long nV = B.box.nV, o = ghost_index(B.box, c);
 #pragma unroll
-      for (int q = 0; q < 5; ++q) raw[q] = B.U[q * nV + o];
+      for (int q = 0; q < 5; ++q) cp_async8(dst + q * stride, B.U + q * nV + o);
     }
   }
   __device__ __forceinline__ uint8_t* flags(int i, int j, int k) const {

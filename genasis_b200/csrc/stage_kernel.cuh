@@ -254,6 +254,12 @@ __device__ __forceinline__ void cp_async_commit() {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
+// Waits until at most N of this thread's committed groups of copies are
+// still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Starts the asynchronous copy of the input values of cell (gx, gy, gz)
 // (possibly ghosts) into 5 shared slots at stride `stride`: the stored
