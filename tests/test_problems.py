@@ -107,3 +107,22 @@ def test_random_bricks_follow_the_seeded_draws():
         for d in range(3):
             assert np.array_equal(prim[1 + d], np.where(left, v_l[d], v_r[d]))
         assert 0.1 <= min(rho_l, rho_r) and max(rho_l, rho_r) <= 10.0
+
+
+def test_l1_error_is_the_plane_wave_norm_over_proper_cells():
+    """sum |N - N_exact| / sum |N_exact| over the proper cells only: ghost
+    values do not enter; the exact profile is the initial one translated by
+    v t."""
+    cfg, prim = problems.sine_wave(8)
+    exact = problems.sine_density(cfg, t=0.25)
+    rho = exact.copy()
+    p = cfg.proper
+    rho[p] += 1e-3
+    ghost = np.ones(cfg.shape, dtype=bool)
+    ghost[p] = False
+    rho[ghost] += 7.0  # ghosts are left out of the norm
+    expected = 1e-3 * rho[p].size / np.abs(exact[p]).sum()
+    assert problems.l1_error(rho, exact, cfg) == pytest.approx(expected, rel=1e-12)
+    X, Y, Z = _grid(cfg)
+    shifted = 1.0 + 0.5 * np.sin(2.0 * math.pi * ((X - 0.25) + (Y - 0.25) + (Z - 0.25)))
+    assert np.array_equal(exact, shifted)
