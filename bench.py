@@ -92,11 +92,14 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region,
+    every 20 ms, with each sample's time, so that the samples that fall in
+    the timed window can be told apart from those around it."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
@@ -109,13 +112,15 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:  # noqa: BLE001
             self.proc = None
         time.sleep(0.3)
 
-    def stop(self):
+    def stop(self, window=None):
+        """The summary of the samples; window = (t0, t1), host wall-clock
+        seconds around the timed region, adds the samples inside it."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.15)
@@ -124,21 +129,51 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:  # noqa: BLE001
             self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        with open(self.path) as f:
+            lines = f.readlines()
         os.unlink(self.path)
+        return self.summarize(lines, window)
+
+    @classmethod
+    def summarize(cls, lines, window=None):
+        """Median and maximum SM clock and the throttle reasons seen (any
+        sample), and, for the samples whose time falls in window, their count
+        and lowest SM clock."""
+        import datetime
+
+        rows = []
+        for line in lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 10:
+                rows.append(parts)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [x for x in (num(r[2]) for r in rows) if x is not None]
+        mx = [x for x in (num(r[3]) for r in rows) if x is not None]
+        reasons = sorted({cls.REASONS[i] for r in rows for i in range(4) if r[6 + i] == "Active"})
+        out = {"sm_mhz": statistics.median(sm) if sm else None,
+               "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+               "samples": len(rows), "interval_ms": 20}
+        if window is not None:
+            t0, t1 = window
+            inside = []
+            for r in rows:
+                try:
+                    t = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    continue
+                if t0 <= t <= t1 and num(r[2]) is not None:
+                    inside.append(num(r[2]))
+            out["timed_samples"] = len(inside)
+            out["timed_sm_mhz_min"] = min(inside) if inside else None
+        return out
 
 
 def dist_init():
@@ -326,12 +361,14 @@ def _timed_evolve(box, steps, warmup, local, world):
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
     ev0.record(stream)
     t_sim, cyc2, ms = box.evolve_timed(1e30, t_sim, cyc, max_cycles=steps)
     ev1.record(stream)
     torch.cuda.synchronize()
+    w1 = time.time()
     barrier(world)
-    clocks = sampler.stop()
+    clocks = sampler.stop(window=(w0, w1))
     return {"ms": ms, "ms_call": ev0.elapsed_time(ev1), "steps": cyc2 - cyc, "t_sim": t_sim,
             "cycle": cyc2, "launches": box.kernel_launches() - launches0, "clocks": clocks,
             "fp64": fp64}
