@@ -361,3 +361,32 @@ def test_parabolic_keeps_sod_close_to_the_exact_solution():
     x = problems.axis_geometry(n, 0.0, 1.0)[0][2:-2]
     rho = o.conserved()[0][cfg.proper][2, 2, :]
     assert np.abs(rho - _exact_sod_density(x, t)).mean() < 0.02
+
+
+@pytest.mark.parametrize("rs", ["HLLC", "HLL"])
+def test_hllc_keeps_a_stationary_contact_and_hll_spreads_it(rs):
+    """A density jump at rest under a uniform pressure (a contact).  HLLC's
+    centre wave is the contact itself: the centre speed AC = SN / MD is 0
+    exactly (SN = p_L - p_R = 0), so every face carries (0, p, 0, 0, 0) and
+    the steps leave D, S and G unchanged bit for bit (no shock flags arise:
+    the pressure is uniform).  HLL has no centre wave: its mass flux at the
+    jump, -AP AM (D_R - D_L) / (AP + AM), spreads the contact."""
+    cfg = FluidConfig(n_cells=(16, 6, 6), boundary=(("OUTFLOW", "OUTFLOW"),) * 3,
+                      riemann_solver=rs, courant_factor=0.8, n_ramp_cycles=1)
+    prim = problems.riemann(cfg, 1.0, 1.0, (0.0, 0.0, 0.0), 0.5, 1.0, (0.0, 0.0, 0.0),
+                            (0.5, 0.0, 0.0), (1.0, 0.0, 0.0))
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    p = (slice(0, 5),) + cfg.proper
+    U0 = o.conserved()[p].copy()
+    if rs == "HLLC":
+        for i in range(3):
+            o.step(o.timestep(i))
+        assert np.array_equal(o.conserved()[p], U0)
+        assert not o.features().any()
+    else:
+        o.step(o.timestep(0))
+        changed = np.argwhere(o.conserved()[p][0] != U0[0])
+        # the jump lies between x cells 7 and 8; each of the two stages
+        # carries the change one cell further on either side
+        assert sorted(set(int(x) for x in changed[:, 2])) == [6, 7, 8, 9]
