@@ -452,3 +452,31 @@ def test_reflecting_walls_keep_the_mass_in(rs):
         assert float(np.abs(fl[0, :4]).max()) <= 1e-10
     m1 = o.conserved()[0][p].sum()
     assert abs(m1 - m0) <= 1e-13 * m0
+
+
+def test_gravity_source_on_a_uniform_gas_at_rest():
+    """A uniform gas at rest under the uniform acceleration a along z
+    (ApplyGravity_F, ApplyGravity_F__Command.f90:124-264, with the gradient
+    (0, 0, a)): every flux divergence vanishes, so one RK2 step is the source
+    alone.  Stage 1 gives K_S3 = -N a dt and no energy term (V = 0); stage 2,
+    on Y with V3 = -a dt, gives K_S3 = -N a dt again and K_G = -N (V3 a) dt.
+    So S3 = -N a dt and G = G0 + N a^2 dt^2 / 2: the work of gravity is the
+    kinetic energy gained."""
+    a, rho, p0 = 0.1, 1.5, 1.0
+    cfg = FluidConfig(n_cells=(8, 8, 8), boundary=(("PERIODIC", "PERIODIC"),) * 3,
+                      riemann_solver="HLLC", courant_factor=0.8, n_ramp_cycles=1,
+                      uniform_acceleration=a)
+    prim = np.zeros((5,) + cfg.shape)
+    prim[0] = rho
+    prim[4] = p0 / (cfg.adiabatic_index - 1.0)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    p = (slice(None),) + cfg.proper
+    U0 = o.conserved()[p].copy()
+    dt = o.timestep(0)
+    o.step(dt)
+    U1 = o.conserved()[p]
+    assert np.array_equal(U1[0], U0[0])
+    assert np.all(U1[1] == 0.0) and np.all(U1[2] == 0.0)
+    assert np.allclose(U1[3], -rho * a * dt, rtol=1e-14, atol=0.0)
+    assert np.allclose(U1[4] - U0[4], 0.5 * rho * a * a * dt * dt, rtol=1e-9, atol=0.0)
