@@ -293,6 +293,28 @@ def test_time_step_ramp():
     assert full == cfg.courant_factor * (1.0 / tsi)
 
 
+def test_time_step_of_a_uniform_flow():
+    """ComputeTimeStepKernel_CSL (Integrator_C_PS__Kernel.f90:122-142) on a
+    uniform state: the inverse CFL time is sum_d max(FEP_d, -FEM_d) / dX_d
+    with FEP_d = V_d + CS, FEM_d = V_d - CS and CS = sqrt(gamma P / N), and the
+    step is CourantFactor over it."""
+    rho, p0, v = 1.3, 0.7, (0.4, -0.25, 0.0)
+    n = (8, 10, 12)
+    cfg = FluidConfig(n_cells=n, boundary=(("PERIODIC", "PERIODIC"),) * 3, courant_factor=0.8,
+                      n_ramp_cycles=1)
+    prim = np.zeros((5,) + cfg.shape)
+    prim[0] = rho
+    for d in range(3):
+        prim[1 + d] = v[d]
+    prim[4] = p0 / (cfg.adiabatic_index - 1.0)
+    o = Oracle(cfg)
+    o.set_primitive(prim)
+    cs = math.sqrt(cfg.adiabatic_index * p0 / rho)
+    tsi = sum(max(v[d] + cs, -(v[d] - cs)) * n[d] for d in range(3))
+    assert o.inverse_timestep() == pytest.approx(tsi, rel=1e-13)
+    assert o.timestep(0) == pytest.approx(0.8 / tsi, rel=1e-13)
+
+
 # ---- PARABOLIC reconstruction (IncrementDivergence_FV__Kernel.f90:296-596) ----
 
 def test_parabolic_reconstructs_a_linear_profile_exactly():
