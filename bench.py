@@ -936,11 +936,12 @@ def rt_result(steps=200, warmup=3, adjoint_steps=10, variant="exact"):
     sampler.start()
     l0 = box.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
     e0.record()
     t_sim, cyc2 = box.evolve(1e30, t_sim, cyc, max_cycles=steps)
     e1.record()
     torch.cuda.synchronize()
-    clocks = sampler.stop()
+    clocks = sampler.stop(window=(w0, time.time()))
     launches = box.kernel_launches() - l0
     ms = e0.elapsed_time(e1)
     n_done = cyc2 - cyc
